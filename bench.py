@@ -1,0 +1,383 @@
+"""Benchmark of the PDHG path on B200.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2] [--impl ours|reference]
+
+A step is one solve of the workload to 1e-6 relative KKT (the metric of the
+reference's PDHG path is time to tolerance).  Workloads (seeded synthetic
+instances of include/nir_lpgen.h; the reference publishes no dataset):
+
+  c2  ZIPF 200,000 x 500,000, ~5M nonzeros, mixed precision (default)
+  c1  RANDOM_EQ 2,000 x 5,000, 40,000 nonzeros
+  c5  BADLY_SCALED 50,000 x 120,000, ~1M nonzeros
+
+`value` is the time to tolerance with the LP already resident in HBM
+(handle created before the timed region); `e2e` is the same metric through
+the one-shot C ABI (nir_pdhg_solve_lp) from host arrays, host->device copy,
+transpose and device->host copy of x and y included.  `roofline` covers the
+dominant kernel (the fused A'y SpMV + primal update) timed with CUDA events
+on the engine's stream during a solve.  `cpu_baseline` times the
+reference's own PdhgSolver::solve (compiled from source into oracle/_ref) on
+a bounded sample of the same workload.
+
+With --gpus N > 1 (torchrun), every rank solves its own replica (the path
+does not shard a single LP) and the time is the max over
+ranks.  --impl reference runs the reference's CPU PDHG on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "time to 1e-6 rel KKT: learned-warm/mixed vs plain PDHG on B200; SpMV GB/s"
+L2_BYTES = 126 * 2 ** 20
+
+WORKLOADS = {
+    "c2": dict(kind=2, seed=1, kw={}, label="zipf_200000x500000_nnz5M", precision=1),
+    "c1": dict(kind=1, seed=1, kw={}, label="random_eq_2000x5000_nnz40000", precision=1),
+    "c5": dict(kind=5, seed=1, kw={}, label="badly_scaled_50000x120000_nnz1M", precision=1),
+}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def committed_traffic(kernel_tag: str):
+    """Per-launch DRAM bytes of the fused kernel from the committed ncu
+    summary (profiles/*.md line `traffic_bytes_per_launch[<tag>]: N`)."""
+    pdir = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(pdir):
+        return None
+    pat = re.compile(r"traffic_bytes_per_launch\[" + re.escape(kernel_tag) + r"\]:\s*([0-9.eE+]+)")
+    for fn in sorted(os.listdir(pdir)):
+        if fn.endswith((".md", ".txt")):
+            with open(os.path.join(pdir, fn)) as f:
+                m = pat.search(f.read())
+            if m:
+                return float(m.group(1))
+    return None
+
+
+def committed_ref_iterations(label: str):
+    pdir = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(pdir):
+        return None, None
+    pat = re.compile(r"reference_iterations_to_tol\[" + re.escape(label) + r"\]:\s*([0-9]+)(\s*lower_bound)?")
+    for fn in sorted(os.listdir(pdir)):
+        if fn.endswith((".md", ".txt")):
+            with open(os.path.join(pdir, fn)) as f:
+                m = pat.search(f.read())
+            if m:
+                return int(m.group(1)), bool(m.group(2))
+    return None, None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def fused_primal_bytes(lp, nblk):
+    """Algorithmic bytes of one launch of the fused A'y SpMV + primal update
+    in FP32: index+value per nonzero, row pointers and row-block starts, y read
+    once, x/c/l/u/x0 read and x/xbar written once."""
+    n, m, nnz = lp.ncol, lp.nrow, lp.nnz
+    return 8 * nnz + 4 * (n + 1) + 4 * (nblk + 1) + 4 * m + 4 * 5 * n + 4 * 2 * n
+
+
+def fused_dual_bytes(lp, nblk):
+    n, m, nnz = lp.ncol, lp.nrow, lp.nnz
+    return 8 * nnz + 4 * (m + 1) + 4 * (nblk + 1) + 4 * n + 4 * 4 * m + 4 * 1 * m
+
+
+def spmv_bytes(lp, transpose, word):
+    """Algorithmic bytes of a plain CSR SpMV (SURVEY's formula)."""
+    R, Cc = (lp.ncol, lp.nrow) if transpose else (lp.nrow, lp.ncol)
+    iw = 4
+    return (iw + word) * lp.nnz + 4 * (R + 1) + word * Cc + word * R
+
+
+def dist_setup(gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return rank, world, local
+
+
+def allmax(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(v)], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    import torch
+
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def run_ours(args, rank, world, local):
+    import numpy as np
+    import torch
+
+    from nirnaya_b200 import lp as L
+    from nirnaya_b200 import pdhg
+
+    wl = WORKLOADS[args.workload]
+    lp = L.generate(wl["kind"], wl["seed"], **wl["kw"])
+    params = pdhg.default_params(precision=wl["precision"], tol=1e-6, max_iters=args.max_iters)
+    eng = pdhg.Engine(lp, local)
+    flush = torch.empty(2 * L2_BYTES, dtype=torch.uint8, device=f"cuda:{local}")
+    launches = 0
+    infos = []
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        eng.solve(params)
+    barrier(world)
+    with ClockSampler(local) as clk:
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record()
+        for _ in range(args.steps):
+            flush.fill_(1)  # every solve starts with a cold L2
+            x, y, info = eng.solve(params)
+            launches += info.kernel_launches
+            infos.append(info.as_dict())
+        b.record()
+        torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / args.steps
+    ms = allmax(ms, world)
+    # end-to-end through the one-shot C ABI with host arrays
+    e2e_s = []
+    for _ in range(max(1, min(args.steps, 3))):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        x = np.zeros(lp.ncol)
+        y = np.zeros(lp.nrow)
+        info = pdhg.Info()
+        import ctypes as C
+
+        pdhg.lib().nir_pdhg_solve_lp(C.byref(lp.view()), local, C.byref(params), pdhg.POLL_FN(0), None,
+                                     x.ctypes.data_as(C.POINTER(C.c_double)), y.ctypes.data_as(C.POINTER(C.c_double)),
+                                     C.byref(info))
+        e2e_s.append(time.perf_counter() - t0)
+        launches_e2e = info.kernel_launches
+    e2e = allmax(statistics.median(e2e_s), world)
+    # dominant kernel, timed live with CUDA events on the engine's stream
+    eng.set_profiling(True)
+    flush.fill_(1)
+    eng.solve(params)
+    kt = eng.kernel_times()
+    eng.set_profiling(False)
+    lay = eng.layout()
+    # plain SpMV of A' in FP32 with a cold L2 (the SpMV GB/s of the metric)
+    spmv_t_us = eng.time_spmv(True, 2, reps=20, flush_l2=True)
+    spmv_a_us = eng.time_spmv(False, 2, reps=20, flush_l2=True)
+    eng.close()
+    return dict(lp=lp, ms=ms, infos=infos, launches=launches, e2e=e2e, kt=kt, lay=lay, clocks=clk.summary(),
+                spmv_t_us=spmv_t_us, spmv_a_us=spmv_a_us, launches_e2e=launches_e2e)
+
+
+def cpu_baseline(lp, label, seconds=15.0, threads=None):
+    """The reference's PdhgSolver::solve (oracle/_ref) on this host for a
+    bounded wall time: iterations per second, then time to tolerance from the
+    reference algorithm's iteration count on this instance when known."""
+    from oracle import ffi
+
+    if not ffi.ref_available():
+        return None
+    threads = threads or os.cpu_count() or 1
+    t0 = time.perf_counter()
+    x, y, st, obj, it = ffi.ref_pdhg(lp, threads=threads, simplex_iter_limit=10 ** 9, time_limit=seconds)
+    dt = time.perf_counter() - t0
+    it_s = it / dt
+    n_ref, lower = committed_ref_iterations(label)
+    value = (n_ref / it_s) if n_ref else None
+    return dict(value=value, unit="s", cores=threads, kind="reference",
+                sample=f"PdhgSolver::solve for {seconds:.0f} s wall ({it} iterations, {it_s:.1f} it/s, threads={threads}); "
+                       f"time = iterations the reference algorithm needs on this instance "
+                       f"({n_ref if n_ref else 'unknown'}{' lower bound' if lower else ''}) / it/s",
+                iterations_per_s=it_s, lower_bound=bool(lower))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--max-iters", type=int, default=1000000)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    args = ap.parse_args()
+    rank, world, local = dist_setup(args.gpus)
+    wl = WORKLOADS[args.workload]
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        from nirnaya_b200 import lp as L
+
+        lp = L.generate(wl["kind"], wl["seed"], **wl["kw"])
+        vals = []
+        for _ in range(args.warmup):
+            pass
+        res = None
+        for _ in range(args.steps):
+            res = cpu_baseline(lp, wl["label"], seconds=max(1.0, args.cpu_seconds / max(1, args.steps)))
+            if res is None:
+                print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_nirnaya.so was not built "
+                                  "from the reference sources"}))
+                return
+            vals.append(res["value"])
+        v = res["value"]
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": None if v is None else 1000 * v,
+                "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded generator, include/nir_lpgen.h)",
+                "config": {"workload": wl["label"], "tol": 1e-6, "threads": res["cores"]},
+                "cpu_baseline": res,
+                "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    r = run_ours(args, rank, world, local)
+    if rank != 0:
+        return
+    lp, infos = r["lp"], r["infos"]
+    last = infos[-1]
+    peak, peak_kind = peaks()
+    kt, lay = r["kt"], r["lay"]
+    ach_bytes = fused_primal_bytes(lp, lay.blocks_at)
+    achieved = ach_bytes / (kt.primal_us * 1e-6) / 1e9 if kt.primal_us > 0 else None
+    traffic = committed_traffic(f"fused_primal_f32:{wl['label']}")
+    cpu = cpu_baseline(lp, wl["label"], seconds=args.cpu_seconds)
+    line = {
+        "metric": METRIC,
+        "value": r["ms"] / 1000.0,
+        "unit": "s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": r["ms"],
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32+f64",
+        "data": "synthetic (seeded generator, include/nir_lpgen.h)",
+        "config": {"workload": wl["label"], "m": lp.nrow, "n": lp.ncol, "nnz": lp.nnz, "tol": 1e-6,
+                   "algorithm": "pdlp (restarted reflected Halpern PDHG)", "precision": "mixed (fp32 + fp64 polish)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single gpu",
+                   "l2": "flushed (2x L2 write) before every solve; inside a solve the working set stays resident"},
+        "status": last["status"],
+        "iterations": last["iterations"],
+        "iterations_fp64": last["iterations_fp64"],
+        "rel_kkt": last["rel_kkt"],
+        "objective": last["objective"],
+        "setup_s": last["setup_seconds"],
+        "e2e": {"value": r["e2e"], "unit": "s", "h2d_bytes_per_step": lp.host_bytes(),
+                "d2h_bytes_per_step": 8 * (lp.ncol + lp.nrow)},
+        "gpu_launches": r["launches"],
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                     "kernel": "k_primal<float> (fused A'y CSR-adaptive SpMV + primal update)",
+                     "algorithmic_bytes_per_launch": ach_bytes, "launch_us": kt.primal_us,
+                     "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+                     "dual_kernel_us": kt.dual_us, "dual_algorithmic_bytes": fused_dual_bytes(lp, lay.blocks_a),
+                     "iteration_us": kt.iter_us,
+                     "spmv_fp32_cold_At_GBs": spmv_bytes(lp, True, 4) / (r["spmv_t_us"] * 1e-6) / 1e9,
+                     "spmv_fp32_cold_A_GBs": spmv_bytes(lp, False, 4) / (r["spmv_a_us"] * 1e-6) / 1e9},
+        "cpu_baseline": cpu,
+        "clocks": r["clocks"],
+    }
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,184 @@
+/*
+ * nir_pdhg.h -- C ABI of the B200 PDHG / PDLP engine (libnir_pdhg.so).
+ *
+ * This is the boundary a caller of the reference's PDHG path binds.  It
+ * replaces, one for one:
+ *
+ *   sov::PdhgSolver::solve(const Model&, const Options&, const Deadline&)
+ *       src/gpu/pdhg_solver.hpp:25-107         -> nir_pdhg_solve_lp, or
+ *                                                 nir_pdhg_create + nir_pdhg_solve
+ *   sov::PdhgResult {status, objective, x, y, iterations}
+ *       src/gpu/pdhg_solver.hpp:14-20          -> status return, x_out, y_out,
+ *                                                 nir_pdhg_info
+ *   sov::Deadline::expired() (stop flag, wall clock, work counter)
+ *       src/core/timer.hpp:41-46, polled every 256 iterations at
+ *       src/gpu/pdhg_solver.hpp:63            -> the poll callback, called on
+ *                                                 the host between launch chunks
+ *   sov::Options::simplex_iter_limit -> max_iters
+ *       src/gpu/pdhg_solver.hpp:60             -> nir_pdhg_params.max_iters
+ *   sov::Status (src/core/status.hpp:7-24)     -> NIR_STATUS_* (same values)
+ *
+ * The LP comes in the reference's layout (nir_lp.h).  All pointers in
+ * the signatures are host pointers owned by the caller; device memory is
+ * owned by the handle.  No C++ exception crosses this boundary: every entry
+ * point returns a status and sets a thread-local message
+ * (nir_pdhg_last_error), as src/driver/c_api.cpp:56-59, :136-139 do.
+ *
+ * There is no CPU fallback: without a usable CUDA device nir_pdhg_create
+ * fails with NIR_STATUS_INTERNAL_ERROR.
+ */
+#ifndef NIR_PDHG_H
+#define NIR_PDHG_H
+
+#include <stdint.h>
+#include "nir_lp.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* sov::Status values (src/core/status.hpp:7-24). */
+enum {
+    NIR_STATUS_OPTIMAL = 0,
+    NIR_STATUS_TIME_LIMIT = 4,
+    NIR_STATUS_ITERATION_LIMIT = 6,
+    NIR_STATUS_INTERRUPTED = 10,
+    NIR_STATUS_NUMERICAL_TROUBLE = 11,
+    NIR_STATUS_INPUT_ERROR = 12,
+    NIR_STATUS_INTERNAL_ERROR = 14
+};
+
+/* Algorithms.
+ *  REFERENCE  the reference loop itself (src/gpu/pdhg_solver.hpp:33-105) in
+ *             FP64, reproduced bit for bit: same power iteration, fixed
+ *             steps 0.85/||A||, box-midpoint start, its absolute row-violation
+ *             stop test every 32 iterations, and the same iteration count.
+ *             Unlike the reference it reports NIR_STATUS_ITERATION_LIMIT
+ *             (not Optimal) when max_iters is reached without the stop test.
+ *  PDHG       the same unrestarted iteration on the fast kernels, stopping on
+ *             the relative KKT error (precision selectable).
+ *  PDLP       diagonal preconditioning (Ruiz + Pock-Chambolle), reflected
+ *             Halpern PDHG with fixed-point-residual restarts, adaptive primal
+ *             weight, relative-KKT stop; mixed precision by default. */
+enum { NIR_ALGO_REFERENCE = 0, NIR_ALGO_PDHG = 1, NIR_ALGO_PDLP = 2 };
+
+/* Precision of matrix, iterates and SpMV.  KKT residuals, restart
+ * criterion, primal weight and objective are always FP64.  MIXED = FP32
+ * iterations followed by an FP64 polish phase when FP32 stalls. */
+enum { NIR_PREC_FP64 = 0, NIR_PREC_MIXED = 1, NIR_PREC_FP32 = 2 };
+
+typedef struct nir_pdhg_params {
+    int32_t algorithm;            /* NIR_ALGO_*                                  (PDLP)  */
+    int32_t precision;            /* NIR_PREC_*                                  (MIXED) */
+    double tol;                   /* relative KKT target                         (1e-6)  */
+    double feas_tol;              /* also require max_i viol_i/(1+|b_i|) <= this (0=off) */
+    int64_t max_iters;            /* iteration cap                               (1e6)   */
+    double time_limit;            /* seconds of solve time; <= 0 = none          (0)     */
+    int32_t check_every;          /* iterations per restart/KKT check            (64)    */
+    int32_t ruiz_iters;           /* Ruiz l-inf equilibration passes             (10)    */
+    int32_t pock_chambolle;       /* 1 = one Pock-Chambolle (alpha=1) pass        (1)     */
+    double reflection;            /* Halpern reflection rho in [0,1]             (1.0)   */
+    double restart_sufficient;    /* restart if r <= this * r_anchor             (0.2)   */
+    double restart_necessary;     /* ... or r <= this * r_anchor and r grew      (0.8)   */
+    double restart_artificial;    /* ... or inner iterations >= this * total     (0.36)  */
+    double primal_weight_smoothing; /* theta of the log-space weight update      (0.5)   */
+    double step_factor;           /* eta = step_factor / ||A||_2 estimate        (0.998) */
+    int32_t power_iters;          /* power-iteration rounds for ||A||_2          (64)    */
+    int32_t polish_stall_checks;  /* MIXED: FP64 polish after this many checks
+                                     without a 0.8x improvement of the best KKT   (6)    */
+    double polish_switch_kkt;     /* MIXED: ... or as soon as KKT <= this        (0)     */
+    int32_t spmv_block_nnz;       /* nonzeros per CSR-adaptive row block; 0=auto (0)     */
+    int32_t use_graphs;           /* capture launch chunks in CUDA graphs        (1)     */
+    int32_t verbose;              /* 1 = one line per check on stderr            (0)     */
+    const double* x_init;         /* warm start in original space, ncol, or NULL          */
+    const double* y_init;         /* warm start duals, nrow, or NULL                      */
+    double omega_init;            /* warm-start primal weight; <= 0 = default             */
+} nir_pdhg_params;
+
+typedef struct nir_pdhg_info {
+    int32_t status;               /* NIR_STATUS_*                                        */
+    int32_t restarts;
+    int64_t iterations;           /* all iterations (FP32 + FP64)                        */
+    int64_t iterations_fp64;      /* of which in FP64 (polish, or all for FP64)          */
+    double objective;             /* c'x + offset in double-double (eval_objective)      */
+    double rel_kkt, rel_primal, rel_dual, rel_gap;  /* at the returned point, FP64       */
+    double max_rel_row_viol;      /* max_i viol_i / (1 + |b_i|) at the returned point    */
+    double primal_weight, step_size;
+    double setup_seconds;         /* preconditioning, norm estimate, graph capture       */
+    double solve_seconds;         /* iterations until the returned point                 */
+    double time_to_fp64_seconds;  /* when the FP64 polish began (MIXED), else 0          */
+    int32_t kernel_launches;      /* engine kernels launched by this solve               */
+} nir_pdhg_info;
+
+typedef struct nir_pdhg nir_pdhg;
+
+/* Fills *p with the defaults shown above. */
+int nir_pdhg_default_params(nir_pdhg_params* p);
+
+/* Copies the LP to `device`, builds CSR(A) and CSR(A^T) there.
+ * Errors: NIR_STATUS_INPUT_ERROR (malformed LP), NIR_STATUS_INTERNAL_ERROR
+ * (no device / out of device memory). */
+int nir_pdhg_create(const nir_lp_view* lp, int device, nir_pdhg** out);
+
+/* Replaces cost, column and row bounds of an existing handle (same
+ * matrix); NULL leaves an array unchanged.  Used by families of LPs that
+ * share A (warm-start training). */
+int nir_pdhg_update_vectors(nir_pdhg* h, const double* cost, const double* collo, const double* colup,
+                            const double* rowlo, const double* rowup);
+
+/* Solves.  poll(ctx) is called on the host between launch chunks (at least
+ * every 256 iterations); a nonzero return stops the solve with
+ * NIR_STATUS_TIME_LIMIT, like Deadline::expired().  x_out (ncol) and y_out
+ * (nrow) may be NULL.  y follows the reference's sign convention
+ * (y += sigma*(clamp(Ax - y/sigma) - Ax): y > 0 where a row's lower bound
+ * binds).  Returns info->status. */
+int nir_pdhg_solve(nir_pdhg* h, const nir_pdhg_params* p, int (*poll)(void* ctx), void* poll_ctx,
+                   double* x_out, double* y_out, nir_pdhg_info* info);
+
+/* create + solve + free in one call (what the drop-in PdhgSolver uses). */
+int nir_pdhg_solve_lp(const nir_lp_view* lp, int device, const nir_pdhg_params* p, int (*poll)(void* ctx),
+                      void* poll_ctx, double* x_out, double* y_out, nir_pdhg_info* info);
+
+void nir_pdhg_free(nir_pdhg* h);
+const char* nir_pdhg_last_error(void);
+
+/* --- kernel-level entry points (parity tests and the benchmark) --- */
+
+/* One SpMV with the handle's unscaled matrix, host in/out.
+ * transpose=0: y = A x (x: ncol, y: nrow); 1: y = A' x.
+ * kernel: 0 = reference-order sequential FP64 (bit-identical to
+ * CscMatrix::spmv / spmv_transpose), 1 = CSR-adaptive FP64,
+ * 2 = CSR-adaptive FP32 (values and x rounded to FP32, FP32 accumulation). */
+int nir_pdhg_spmv(nir_pdhg* h, int transpose, int kernel, const double* x, double* y);
+
+/* Times `reps` back-to-back launches of one SpMV kind on device-resident
+ * data (optionally flushing L2 before each) and reports the mean duration
+ * in microseconds measured with CUDA events on the launching stream. */
+int nir_pdhg_time_spmv(nir_pdhg* h, int transpose, int kernel, int reps, int flush_l2, double* usec);
+
+typedef struct nir_pdhg_kernel_time {
+    double primal_us;   /* mean duration of the fused A'y + primal-update kernel */
+    double dual_us;     /* mean duration of the fused A x + dual-update kernel   */
+    double iter_us;     /* mean wall time of one iteration inside the graphs     */
+    int64_t samples;
+} nir_pdhg_kernel_time;
+
+/* Event timing of the hot kernels during the last solve (when enabled by
+ * nir_pdhg_set_profiling before the solve). */
+int nir_pdhg_set_profiling(nir_pdhg* h, int on);
+int nir_pdhg_kernel_times(nir_pdhg* h, nir_pdhg_kernel_time* out);
+
+/* Matrix and layout facts: nnz, rows, row blocks of each orientation. */
+typedef struct nir_pdhg_layout {
+    int32_t nrow, ncol;
+    int64_t nnz;
+    int32_t blocks_a, blocks_at;        /* CSR-adaptive row blocks of A and A' */
+    int32_t block_nnz;                  /* row-block capacity in nonzeros      */
+    int64_t device_bytes;               /* device memory held by the handle    */
+} nir_pdhg_layout;
+int nir_pdhg_get_layout(nir_pdhg* h, nir_pdhg_layout* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

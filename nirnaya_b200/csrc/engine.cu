@@ -1,0 +1,1311 @@
+// Host side of the B200 PDHG engine and its C ABI (include/nir_pdhg.h).
+//
+// One handle = one LP resident on one GPU: CSR(A) and CSR(A') (the CSC of
+// A read as rows), original and scaled FP64 values, FP32 values, and every
+// vector the iteration touches.  A solve runs launch chunks of K
+// iterations (each chunk ends with the FP64 KKT evaluation, the restart /
+// primal-weight controller and a status snapshot to host-mapped memory),
+// captured once into CUDA graphs and replayed with a few chunks in flight.
+// The host only reads the snapshots, polls the caller's deadline and
+// decides when to switch from FP32 to the FP64 polish.
+
+#include <cub/device/device_radix_sort.cuh>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "dev_common.cuh"
+#include "k_adaptive.cuh"
+#include "k_reference.cuh"
+#include "k_setup.cuh"
+#include "nir_pdhg.h"
+
+namespace {
+
+thread_local std::string g_err;
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+#define NIR_CUDA(call)                                                                                  \
+    do {                                                                                                \
+        cudaError_t e_ = (call);                                                                        \
+        if (e_ != cudaSuccess)                                                                          \
+            throw CudaError(std::string(#call) + ": " + cudaGetErrorString(e_) + " (" __FILE__ ":" +    \
+                            std::to_string(__LINE__) + ")");                                            \
+    } while (0)
+
+#define NIR_LAUNCHED() NIR_CUDA(cudaGetLastError())
+
+inline unsigned grid_for(long long n, int b = nir::kBlock) {
+    long long g = (n + b - 1) / b;
+    return unsigned(g < 1 ? 1 : g);
+}
+
+double now_sec() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// ---- double-double accumulation for the objective (Dekker / Knuth
+// error-free transformations; the reference's Model::eval_objective,
+// src/model/model.hpp:73-98, evaluates c'x + offset the same way).
+struct DD {
+    double hi = 0.0, lo = 0.0;
+};
+inline void two_sum(double a, double b, double& s, double& e) {
+    s = a + b;
+    double bb = s - a;
+    e = (a - (s - bb)) + (b - bb);
+}
+inline void quick_two_sum(double a, double b, double& s, double& e) {
+    s = a + b;
+    e = b - (s - a);
+}
+inline DD dd_add(DD a, DD b) {
+    double s1, s2, t1, t2;
+    two_sum(a.hi, b.hi, s1, s2);
+    two_sum(a.lo, b.lo, t1, t2);
+    s2 += t1;
+    quick_two_sum(s1, s2, s1, s2);
+    s2 += t2;
+    DD r;
+    quick_two_sum(s1, s2, r.hi, r.lo);
+    return r;
+}
+inline DD dd_add_prod(DD a, double x, double y) {
+    DD p;
+    p.hi = x * y;
+    p.lo = std::fma(x, y, -p.hi);
+    return dd_add(a, p);
+}
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace
+
+// ---------------------------------------------------------------- handle
+
+struct Orient {
+    int rows = 0, cols = 0;
+    long long nnz = 0;
+    int* rp = nullptr;
+    int* ci = nullptr;
+    double* v_orig = nullptr;
+    double* v64 = nullptr;
+    float* v32 = nullptr;
+    float* v32_orig = nullptr;  // for the FP32 SpMV test entry point
+    std::vector<int> h_rp;
+    int cap = 0;
+    int nblk = 0;
+    int* blk = nullptr;
+};
+
+struct Snapshot {
+    nir::HostSnap* ring = nullptr;  // host-mapped
+    long long* d_seq = nullptr;
+};
+
+struct ChunkGraph {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    int key = -1;
+};
+
+struct nir_pdhg {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int m = 0, n = 0;
+    long long nnz = 0;
+    double offset = 0.0;
+    Orient A, At;
+    // original vectors on the device (bounds sanitised to +-inf)
+    double *c = nullptr, *l = nullptr, *u = nullptr, *rl = nullptr, *ru = nullptr;
+    std::vector<double> h_c, h_l, h_u, h_rl, h_ru;
+    // scaling and scaled vectors
+    double *dr = nullptr, *dc = nullptr;
+    double *c64 = nullptr, *l64 = nullptr, *u64 = nullptr, *rl64 = nullptr, *ru64 = nullptr;
+    float *c32 = nullptr, *l32 = nullptr, *u32 = nullptr, *rl32 = nullptr, *ru32 = nullptr;
+    // iterates
+    double *x64 = nullptr, *xb64 = nullptr, *x064 = nullptr, *xp64 = nullptr;
+    double *y64 = nullptr, *y064 = nullptr, *yp64 = nullptr;
+    float *x32 = nullptr, *xb32 = nullptr, *x032 = nullptr, *xp32 = nullptr;
+    float *y32 = nullptr, *y032 = nullptr, *yp32 = nullptr;
+    double *tmp_n = nullptr, *tmp_m = nullptr, *out_x = nullptr, *out_y = nullptr;
+    float *tmp_n32 = nullptr, *tmp_m32 = nullptr;
+    double* part = nullptr;
+    size_t part_len = 0;
+    double* hist = nullptr;
+    nir::DevState* st = nullptr;
+    Snapshot snap;
+    unsigned char* flush = nullptr;
+    size_t flush_bytes = 0;
+    std::vector<DevBuf> bufs;
+    long long device_bytes = 0;
+    ChunkGraph graphs[3];
+    bool profiling = false;
+    nir_pdhg_kernel_time ktime{};
+    int launches = 0;
+
+    template <typename T>
+    T* alloc(size_t count) {
+        void* p = nullptr;
+        size_t bytes = std::max<size_t>(1, count) * sizeof(T);
+        NIR_CUDA(cudaMalloc(&p, bytes));
+        bufs.push_back({p, bytes});
+        device_bytes += (long long)bytes;
+        return static_cast<T*>(p);
+    }
+
+    ~nir_pdhg() {
+        if (device >= 0) cudaSetDevice(device);
+        if (stream) cudaStreamSynchronize(stream);
+        for (auto& g : graphs) {
+            if (g.ge) cudaGraphExecDestroy(g.ge);
+            if (g.g) cudaGraphDestroy(g.g);
+        }
+        for (auto& b : bufs) cudaFree(b.p);
+        if (snap.ring) cudaFreeHost(snap.ring);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+// Copies ordered on the handle's (non-blocking) stream, then waited for.
+void h2d(nir_pdhg* h, void* dst, const void* src, size_t bytes) {
+    NIR_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->stream));
+    NIR_CUDA(cudaStreamSynchronize(h->stream));
+}
+void d2h(nir_pdhg* h, void* dst, const void* src, size_t bytes) {
+    NIR_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, h->stream));
+    NIR_CUDA(cudaStreamSynchronize(h->stream));
+}
+
+// CSR-adaptive row blocks: consecutive rows packed while their nonzeros
+// fit in `cap`; a longer row gets a block of its own.
+std::vector<int> build_row_blocks(const std::vector<int>& rp, int cap) {
+    std::vector<int> blk{0};
+    const int rows = int(rp.size()) - 1;
+    if (rows <= 0) return {0, 0};
+    int s = 0;
+    while (s < rows) {
+        int r = s + 1;
+        if (rp[s + 1] - rp[s] <= cap) {
+            while (r < rows && rp[r + 1] - rp[s] <= cap && r - s < cap) ++r;
+        }
+        blk.push_back(r);
+        s = r;
+    }
+    return blk;
+}
+
+void set_blocks(nir_pdhg* h, Orient& o, int cap) {
+    if (o.cap == cap && o.blk) return;
+    std::vector<int> b = build_row_blocks(o.h_rp, cap);
+    o.nblk = int(b.size()) - 1;
+    o.blk = h->alloc<int>(b.size());
+    h2d(h, o.blk, b.data(), b.size() * sizeof(int));
+    o.cap = cap;
+}
+
+int auto_cap(long long nnz, int rows) {
+    (void)rows;
+    (void)nnz;
+    return 2048;
+}
+
+void validate_lp(const nir_lp_view* lp) {
+    if (!lp) throw std::invalid_argument("null LP");
+    if (lp->nrow < 0 || lp->ncol < 0) throw std::invalid_argument("negative dimension");
+    if (!lp->col_start || (lp->nnz > 0 && (!lp->row_index || !lp->value)))
+        throw std::invalid_argument("missing matrix arrays");
+    if ((lp->ncol > 0 && (!lp->cost || !lp->collo || !lp->colup)) || (lp->nrow > 0 && (!lp->rowlo || !lp->rowup)))
+        throw std::invalid_argument("missing vector arrays");
+    if (lp->col_start[0] != 0 || lp->col_start[lp->ncol] != lp->nnz) throw std::invalid_argument("column starts");
+    if (lp->nnz >= (1LL << 31) - 1) throw std::invalid_argument("more than 2^31-2 nonzeros");
+    for (int j = 0; j < lp->ncol; ++j)
+        if (lp->col_start[j + 1] < lp->col_start[j]) throw std::invalid_argument("column starts not nondecreasing");
+    for (long long k = 0; k < lp->nnz; ++k) {
+        if (lp->row_index[k] < 0 || lp->row_index[k] >= lp->nrow) throw std::invalid_argument("row index out of range");
+        if (!std::isfinite(lp->value[k])) throw std::invalid_argument("non-finite matrix entry");
+    }
+    for (int j = 0; j < lp->ncol; ++j)
+        if (!std::isfinite(lp->cost[j])) throw std::invalid_argument("non-finite cost");
+}
+
+void upload_vectors(nir_pdhg* h, const double* cost, const double* collo, const double* colup, const double* rowlo,
+                    const double* rowup) {
+    const int n = h->n, m = h->m;
+    auto sanitize = [](double b, bool lower) {
+        bool f = std::isfinite(b) && std::fabs(b) < 1e20;
+        return f ? b : (lower ? -INFINITY : INFINITY);
+    };
+    if (cost) h->h_c.assign(cost, cost + n);
+    if (collo) {
+        h->h_l.resize(n);
+        for (int j = 0; j < n; ++j) h->h_l[j] = sanitize(collo[j], true);
+    }
+    if (colup) {
+        h->h_u.resize(n);
+        for (int j = 0; j < n; ++j) h->h_u[j] = sanitize(colup[j], false);
+    }
+    if (rowlo) {
+        h->h_rl.resize(m);
+        for (int i = 0; i < m; ++i) h->h_rl[i] = sanitize(rowlo[i], true);
+    }
+    if (rowup) {
+        h->h_ru.resize(m);
+        for (int i = 0; i < m; ++i) h->h_ru[i] = sanitize(rowup[i], false);
+    }
+    auto up = [&](double* d, const std::vector<double>& v) {
+        if (!v.empty()) NIR_CUDA(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    };
+    if (cost) up(h->c, h->h_c);
+    if (collo) up(h->l, h->h_l);
+    if (colup) up(h->u, h->h_u);
+    if (rowlo) up(h->rl, h->h_rl);
+    if (rowup) up(h->ru, h->h_ru);
+    NIR_CUDA(cudaStreamSynchronize(h->stream));
+}
+
+void create_impl(nir_pdhg* h, const nir_lp_view* lp, int device) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0)
+        throw CudaError("no CUDA device available (the PDHG engine has no CPU fallback)");
+    if (device < 0 || device >= ndev) throw std::invalid_argument("device ordinal out of range");
+    h->device = device;
+    NIR_CUDA(cudaSetDevice(device));
+    NIR_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    const int m = lp->nrow, n = lp->ncol;
+    const long long nnz = lp->nnz;
+    h->m = m;
+    h->n = n;
+    h->nnz = nnz;
+    h->offset = lp->obj_offset;
+    cudaStream_t s = h->stream;
+
+    // A' = CSC of A read as rows.
+    Orient& T = h->At;
+    T.rows = n;
+    T.cols = m;
+    T.nnz = nnz;
+    T.rp = h->alloc<int>(n + 1);
+    T.ci = h->alloc<int>(nnz);
+    T.v_orig = h->alloc<double>(nnz);
+    T.v64 = h->alloc<double>(nnz);
+    T.v32 = h->alloc<float>(nnz);
+    long long* d_start = h->alloc<long long>(n + 1);
+    NIR_CUDA(cudaMemcpyAsync(d_start, lp->col_start, (n + 1) * sizeof(long long), cudaMemcpyHostToDevice, s));
+    NIR_CUDA(cudaMemcpyAsync(T.ci, lp->row_index, nnz * sizeof(int), cudaMemcpyHostToDevice, s));
+    NIR_CUDA(cudaMemcpyAsync(T.v_orig, lp->value, nnz * sizeof(double), cudaMemcpyHostToDevice, s));
+    nir::k_offsets_to_int<<<grid_for(n + 1), nir::kBlock, 0, s>>>(n + 1, d_start, T.rp);
+    NIR_LAUNCHED();
+    T.h_rp.resize(n + 1);
+    for (int j = 0; j <= n; ++j) T.h_rp[j] = int(lp->col_start[j]);
+
+    // A: stable radix sort of the CSC entries by row keeps each row's
+    // entries in ascending column order (the reference's scatter order).
+    Orient& R = h->A;
+    R.rows = m;
+    R.cols = n;
+    R.nnz = nnz;
+    R.rp = h->alloc<int>(m + 1);
+    R.ci = h->alloc<int>(nnz);
+    R.v_orig = h->alloc<double>(nnz);
+    R.v64 = h->alloc<double>(nnz);
+    R.v32 = h->alloc<float>(nnz);
+    {
+        int* col_of = h->alloc<int>(nnz);
+        int* ids = h->alloc<int>(nnz);
+        int* perm = h->alloc<int>(nnz);
+        int* keys_out = h->alloc<int>(nnz);
+        nir::k_expand_cols<<<grid_for(n), nir::kBlock, 0, s>>>(n, d_start, col_of);
+        NIR_LAUNCHED();
+        nir::k_iota<<<grid_for(nnz), nir::kBlock, 0, s>>>(nnz, ids);
+        NIR_LAUNCHED();
+        int end_bit = 1;
+        while ((1LL << end_bit) <= (long long)m) ++end_bit;
+        size_t tmp_bytes = 0;
+        NIR_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, T.ci, keys_out, ids, perm, (int)nnz, 0, end_bit, s));
+        void* tmp = h->alloc<unsigned char>(tmp_bytes);
+        NIR_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, T.ci, keys_out, ids, perm, (int)nnz, 0, end_bit, s));
+        nir::k_row_ptr_from_sorted<<<grid_for(m + 1), nir::kBlock, 0, s>>>(m, nnz, keys_out, R.rp);
+        NIR_LAUNCHED();
+        nir::k_gather_csr<<<grid_for(nnz), nir::kBlock, 0, s>>>(nnz, perm, col_of, T.v_orig, R.ci, R.v_orig);
+        NIR_LAUNCHED();
+        R.h_rp.resize(m + 1);
+        NIR_CUDA(cudaMemcpyAsync(R.h_rp.data(), R.rp, (m + 1) * sizeof(int), cudaMemcpyDeviceToHost, s));
+        NIR_CUDA(cudaStreamSynchronize(s));
+        // scratch of the transpose is released right away
+        for (void* p : {(void*)col_of, (void*)ids, (void*)perm, (void*)keys_out, tmp, (void*)d_start}) {
+            for (auto it = h->bufs.begin(); it != h->bufs.end(); ++it)
+                if (it->p == p) {
+                    h->device_bytes -= (long long)it->bytes;
+                    cudaFree(it->p);
+                    h->bufs.erase(it);
+                    break;
+                }
+        }
+    }
+
+    // vectors
+    h->c = h->alloc<double>(n);
+    h->l = h->alloc<double>(n);
+    h->u = h->alloc<double>(n);
+    h->rl = h->alloc<double>(m);
+    h->ru = h->alloc<double>(m);
+    upload_vectors(h, lp->cost, lp->collo, lp->colup, lp->rowlo, lp->rowup);
+    h->dr = h->alloc<double>(m);
+    h->dc = h->alloc<double>(n);
+    h->c64 = h->alloc<double>(n);
+    h->l64 = h->alloc<double>(n);
+    h->u64 = h->alloc<double>(n);
+    h->rl64 = h->alloc<double>(m);
+    h->ru64 = h->alloc<double>(m);
+    h->c32 = h->alloc<float>(n);
+    h->l32 = h->alloc<float>(n);
+    h->u32 = h->alloc<float>(n);
+    h->rl32 = h->alloc<float>(m);
+    h->ru32 = h->alloc<float>(m);
+    h->x64 = h->alloc<double>(n);
+    h->xb64 = h->alloc<double>(n);
+    h->x064 = h->alloc<double>(n);
+    h->xp64 = h->alloc<double>(n);
+    h->y64 = h->alloc<double>(m);
+    h->y064 = h->alloc<double>(m);
+    h->yp64 = h->alloc<double>(m);
+    h->x32 = h->alloc<float>(n);
+    h->xb32 = h->alloc<float>(n);
+    h->x032 = h->alloc<float>(n);
+    h->xp32 = h->alloc<float>(n);
+    h->y32 = h->alloc<float>(m);
+    h->y032 = h->alloc<float>(m);
+    h->yp32 = h->alloc<float>(m);
+    h->tmp_n = h->alloc<double>(n);
+    h->tmp_m = h->alloc<double>(m);
+    h->tmp_n32 = h->alloc<float>(n);
+    h->tmp_m32 = h->alloc<float>(m);
+    h->out_x = h->alloc<double>(n);
+    h->out_y = h->alloc<double>(m);
+    h->st = h->alloc<nir::DevState>(1);
+    h->hist = h->alloc<double>(8 * nir::kHist);
+    h->snap.d_seq = h->alloc<long long>(1);
+    NIR_CUDA(cudaMemsetAsync(h->snap.d_seq, 0, sizeof(long long), s));
+    NIR_CUDA(cudaHostAlloc((void**)&h->snap.ring, sizeof(nir::HostSnap) * nir::kSnapRing, cudaHostAllocMapped));
+    std::memset(h->snap.ring, 0, sizeof(nir::HostSnap) * nir::kSnapRing);
+    NIR_CUDA(cudaStreamSynchronize(s));
+}
+
+// Partial-sum area large enough for any kernel of this handle.
+void ensure_partials(nir_pdhg* h) {
+    size_t need = 4 * size_t(std::max(h->A.nblk, 1)) + 4 * size_t(std::max(h->At.nblk, 1)) +
+                  2 * size_t(std::max(h->A.nblk, 1)) + 2 * size_t(std::max(h->At.nblk, 1)) +
+                  size_t(grid_for(std::max(h->m, h->n))) + 16;
+    if (h->part && h->part_len >= need) return;
+    h->part = h->alloc<double>(need);
+    h->part_len = need;
+}
+
+struct PartLayout {
+    double *P, *D, *KR, *KC, *misc;
+};
+
+PartLayout part_layout(nir_pdhg* h) {
+    PartLayout L;
+    L.P = h->part;
+    L.D = L.P + 2 * std::max(h->At.nblk, 1);
+    L.KR = L.D + 2 * std::max(h->A.nblk, 1);
+    L.KC = L.KR + 4 * std::max(h->A.nblk, 1);
+    L.misc = L.KC + 4 * std::max(h->At.nblk, 1);
+    return L;
+}
+
+// ---------------------------------------------------------------- precision views
+
+template <typename T>
+struct View;
+
+template <>
+struct View<float> {
+    static const float* valA(nir_pdhg* h) { return h->A.v32; }
+    static const float* valAt(nir_pdhg* h) { return h->At.v32; }
+    static float* x(nir_pdhg* h) { return h->x32; }
+    static float* xb(nir_pdhg* h) { return h->xb32; }
+    static float* x0(nir_pdhg* h) { return h->x032; }
+    static float* xp(nir_pdhg* h) { return h->xp32; }
+    static float* y(nir_pdhg* h) { return h->y32; }
+    static float* y0(nir_pdhg* h) { return h->y032; }
+    static float* yp(nir_pdhg* h) { return h->yp32; }
+    static const float* c(nir_pdhg* h) { return h->c32; }
+    static const float* l(nir_pdhg* h) { return h->l32; }
+    static const float* u(nir_pdhg* h) { return h->u32; }
+    static const float* rl(nir_pdhg* h) { return h->rl32; }
+    static const float* ru(nir_pdhg* h) { return h->ru32; }
+};
+
+template <>
+struct View<double> {
+    static const double* valA(nir_pdhg* h) { return h->A.v64; }
+    static const double* valAt(nir_pdhg* h) { return h->At.v64; }
+    static double* x(nir_pdhg* h) { return h->x64; }
+    static double* xb(nir_pdhg* h) { return h->xb64; }
+    static double* x0(nir_pdhg* h) { return h->x064; }
+    static double* xp(nir_pdhg* h) { return h->xp64; }
+    static double* y(nir_pdhg* h) { return h->y64; }
+    static double* y0(nir_pdhg* h) { return h->y064; }
+    static double* yp(nir_pdhg* h) { return h->yp64; }
+    static const double* c(nir_pdhg* h) { return h->c64; }
+    static const double* l(nir_pdhg* h) { return h->l64; }
+    static const double* u(nir_pdhg* h) { return h->u64; }
+    static const double* rl(nir_pdhg* h) { return h->rl64; }
+    static const double* ru(nir_pdhg* h) { return h->ru64; }
+};
+
+struct SolveCfg {
+    nir_pdhg_params p;
+    int K = 64;
+    int halpern = 1;
+    int restarts = 1;
+    int mixed = 0;
+    double bnorm = 0.0, cnorm = 0.0;
+};
+
+// Optional event timing of the first iteration of a chunk.
+struct ChunkTimer {
+    cudaEvent_t e[4] = {nullptr, nullptr, nullptr, nullptr};
+    bool armed = false;
+    int K = 1;
+};
+
+template <typename T>
+void launch_fast_chunk(nir_pdhg* h, const SolveCfg& cfg, int phase, ChunkTimer* tm) {
+    cudaStream_t s = h->stream;
+    const PartLayout L = part_layout(h);
+    const int K = cfg.K;
+    const size_t smem = size_t(h->A.cap) * sizeof(T);
+    const size_t smem64 = size_t(h->A.cap) * sizeof(double);
+    for (int i = 0; i < K; ++i) {
+        const bool check = (i == K - 1);
+        nir::IterArgs ap{h->At.blk, h->At.rp, h->At.ci, L.P, h->st, i, cfg.halpern, phase, cfg.p.reflection};
+        nir::IterArgs ad{h->A.blk, h->A.rp, h->A.ci, L.D, h->st, i, cfg.halpern, phase, cfg.p.reflection};
+        const bool timed = tm && tm->armed && i == 0;
+        if (timed) NIR_CUDA(cudaEventRecord(tm->e[0], s));
+        if (check)
+            nir::k_primal<T, true><<<h->At.nblk, nir::kBlock, smem, s>>>(
+                ap, View<T>::valAt(h), View<T>::y(h), View<T>::x(h), View<T>::xb(h), View<T>::xp(h), View<T>::c(h),
+                View<T>::l(h), View<T>::u(h), View<T>::x0(h));
+        else
+            nir::k_primal<T, false><<<h->At.nblk, nir::kBlock, smem, s>>>(
+                ap, View<T>::valAt(h), View<T>::y(h), View<T>::x(h), View<T>::xb(h), View<T>::xp(h), View<T>::c(h),
+                View<T>::l(h), View<T>::u(h), View<T>::x0(h));
+        NIR_LAUNCHED();
+        if (timed) NIR_CUDA(cudaEventRecord(tm->e[1], s));
+        if (check)
+            nir::k_dual<T, true><<<h->A.nblk, nir::kBlock, smem, s>>>(ad, View<T>::valA(h), View<T>::xb(h), View<T>::y(h),
+                                                                       View<T>::yp(h), View<T>::rl(h), View<T>::ru(h),
+                                                                       View<T>::y0(h));
+        else
+            nir::k_dual<T, false><<<h->A.nblk, nir::kBlock, smem, s>>>(ad, View<T>::valA(h), View<T>::xb(h), View<T>::y(h),
+                                                                        View<T>::yp(h), View<T>::rl(h), View<T>::ru(h),
+                                                                        View<T>::y0(h));
+        NIR_LAUNCHED();
+        if (timed) NIR_CUDA(cudaEventRecord(tm->e[2], s));
+        h->launches += 2;
+    }
+    nir::KktArgs kr{h->A.blk, h->A.rp, h->A.ci, h->A.v64, L.KR, h->st, phase};
+    nir::k_kkt_rows<T><<<h->A.nblk, nir::kBlock, smem64, s>>>(kr, View<T>::xp(h), View<T>::yp(h), h->dr, h->rl, h->ru);
+    NIR_LAUNCHED();
+    nir::KktArgs kc{h->At.blk, h->At.rp, h->At.ci, h->At.v64, L.KC, h->st, phase};
+    nir::k_kkt_cols<T><<<h->At.nblk, nir::kBlock, smem64, s>>>(kc, View<T>::xp(h), View<T>::yp(h), h->dc, h->c, h->l, h->u);
+    NIR_LAUNCHED();
+    nir::CtlArgs ca;
+    ca.partP = L.P;
+    ca.partD = L.D;
+    ca.partKR = L.KR;
+    ca.partKC = L.KC;
+    ca.nP = h->At.nblk;
+    ca.nD = h->A.nblk;
+    ca.bnorm = cfg.bnorm;
+    ca.cnorm = cfg.cnorm;
+    ca.offset = h->offset;
+    ca.tol = cfg.p.tol;
+    ca.feas_tol = cfg.p.feas_tol;
+    ca.K = K;
+    ca.restarts_on = cfg.restarts;
+    ca.mixed = (cfg.mixed && phase == 0) ? 1 : 0;
+    ca.phase = phase;
+    ca.suff = cfg.p.restart_sufficient;
+    ca.nec = cfg.p.restart_necessary;
+    ca.art = cfg.p.restart_artificial;
+    ca.theta = cfg.p.primal_weight_smoothing;
+    ca.polish_stall = cfg.p.polish_stall_checks;
+    ca.polish_switch = cfg.p.polish_switch_kkt;
+    ca.hist = h->hist;
+    nir::k_control<<<1, nir::kBlock, 0, s>>>(ca, h->st);
+    NIR_LAUNCHED();
+    const int nm = std::max(h->n, h->m);
+    nir::k_apply_restart<T><<<grid_for(nm), nir::kBlock, 0, s>>>(h->n, h->m, h->st, phase, View<T>::x(h), View<T>::x0(h),
+                                                                  View<T>::xp(h), View<T>::y(h), View<T>::y0(h),
+                                                                  View<T>::yp(h));
+    NIR_LAUNCHED();
+    nir::k_snap<<<1, 32, 0, s>>>(h->st, h->snap.ring, h->snap.d_seq);
+    NIR_LAUNCHED();
+    if (tm && tm->armed) NIR_CUDA(cudaEventRecord(tm->e[3], s));
+    h->launches += 5;
+}
+
+void launch_ref_chunk(nir_pdhg* h, int K) {
+    cudaStream_t s = h->stream;
+    const PartLayout L = part_layout(h);
+    const unsigned gm = grid_for(h->m), gn = grid_for(h->n);
+    for (int i = 0; i < K; ++i) {
+        nir::k_ref_primal<<<std::max(gn, 1u), nir::kBlock, 0, s>>>(h->n, h->At.rp, h->At.ci, h->At.v_orig, h->y64, h->c,
+                                                                    h->l, h->u, h->x64, h->xb64, h->st, i);
+        NIR_LAUNCHED();
+        nir::k_ref_dual<<<std::max(gm, 1u), nir::kBlock, 0, s>>>(h->m, h->A.rp, h->A.ci, h->A.v_orig, h->xb64, h->rl,
+                                                                  h->ru, h->y64, L.misc, h->st, i);
+        NIR_LAUNCHED();
+        nir::k_ref_stop<<<1, nir::kBlock, 0, s>>>(L.misc, std::max<int>(gm, 1), h->st, i, K);
+        NIR_LAUNCHED();
+        h->launches += 3;
+    }
+    nir::k_snap<<<1, 32, 0, s>>>(h->st, h->snap.ring, h->snap.d_seq);
+    NIR_LAUNCHED();
+    h->launches += 1;
+}
+
+// Captures (once) and returns the graph for a chunk kind.
+template <class F>
+cudaGraphExec_t chunk_graph(nir_pdhg* h, int slot, int key, F&& launch) {
+    ChunkGraph& g = h->graphs[slot];
+    if (g.ge && g.key == key) return g.ge;
+    if (g.ge) {
+        cudaGraphExecDestroy(g.ge);
+        g.ge = nullptr;
+    }
+    if (g.g) {
+        cudaGraphDestroy(g.g);
+        g.g = nullptr;
+    }
+    NIR_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    int before = h->launches;
+    try {
+        launch();
+    } catch (...) {
+        cudaGraph_t tmp;
+        cudaStreamEndCapture(h->stream, &tmp);
+        if (tmp) cudaGraphDestroy(tmp);
+        throw;
+    }
+    h->launches = before;  // counted when replayed
+    NIR_CUDA(cudaStreamEndCapture(h->stream, &g.g));
+    NIR_CUDA(cudaGraphInstantiate(&g.ge, g.g, 0));
+    g.key = key;
+    return g.ge;
+}
+
+struct LoopResult {
+    nir::HostSnap last{};
+    bool stopped_by_host = false;
+    double t_switch = 0.0;
+};
+
+int launches_per_chunk(int K, bool ref) { return ref ? 3 * K + 1 : 2 * K + 5; }
+
+// Runs chunks until the device reports done, the phase changes, or the
+// caller's poll / time limit stops it.  Keeps `depth` chunks in flight.
+template <class F>
+LoopResult run_chunks(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), void* ctx, double t_start, int phase,
+                      int per_chunk, F&& launch_one, ChunkTimer* tm) {
+    const int depth = tm ? 1 : 3;  // timed chunks run one at a time
+    cudaEvent_t ev[3];
+    for (auto& e : ev) NIR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    LoopResult R;
+    long long launched = 0, completed = 0;
+    bool stop_launch = false;
+    long long seq0 = 0;
+    {
+        // sequence number of the snapshot before this loop
+        long long s = 0;
+        d2h(h, &s, h->snap.d_seq, sizeof(long long));
+        seq0 = s;
+    }
+    try {
+        for (;;) {
+            while (!stop_launch && launched - completed < depth) {
+                launch_one();
+                h->launches += per_chunk;
+                NIR_CUDA(cudaEventRecord(ev[launched % depth], h->stream));
+                ++launched;
+            }
+            if (completed == launched) break;
+            NIR_CUDA(cudaEventSynchronize(ev[completed % depth]));
+            ++completed;
+            if (tm && tm->armed) {
+                float a = 0, b = 0, c = 0;
+                if (cudaEventElapsedTime(&a, tm->e[0], tm->e[1]) == cudaSuccess &&
+                    cudaEventElapsedTime(&b, tm->e[1], tm->e[2]) == cudaSuccess &&
+                    cudaEventElapsedTime(&c, tm->e[0], tm->e[3]) == cudaSuccess) {
+                    h->ktime.primal_us += 1000.0 * a;
+                    h->ktime.dual_us += 1000.0 * b;
+                    h->ktime.iter_us += 1000.0 * c / std::max(1, tm->K);
+                    h->ktime.samples += 1;
+                }
+            }
+            const nir::HostSnap snap = h->snap.ring[(seq0 + completed) % nir::kSnapRing];
+            R.last = snap;
+            if (stop_launch) continue;
+            if (snap.done || snap.phase != phase) {
+                stop_launch = true;
+                continue;
+            }
+            bool expire = (poll && poll(ctx) != 0);
+            if (p.time_limit > 0.0 && now_sec() - t_start >= p.time_limit) expire = true;
+            if (expire) {
+                R.stopped_by_host = true;
+                stop_launch = true;
+            }
+        }
+        NIR_CUDA(cudaStreamSynchronize(h->stream));
+    } catch (...) {
+        for (auto& e : ev) cudaEventDestroy(e);
+        throw;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    return R;
+}
+
+double host_objective(const nir_pdhg* h, const std::vector<double>& x) {
+    DD s;
+    s.hi = h->offset;
+    for (int j = 0; j < h->n; ++j)
+        if (h->h_c[j] != 0.0 && x[j] != 0.0) s = dd_add_prod(s, h->h_c[j], x[j]);
+    return s.hi + s.lo;
+}
+
+void fill_info_common(nir_pdhg* h, const nir::DevState& st, nir_pdhg_info* info) {
+    info->restarts = st.restarts;
+    info->rel_kkt = st.kkt;
+    info->rel_primal = st.kp;
+    info->rel_dual = st.kd;
+    info->rel_gap = st.kg;
+    info->max_rel_row_viol = st.max_rel_row;
+    info->primal_weight = st.omega;
+    info->step_size = st.eta;
+    (void)h;
+}
+
+// ---------------------------------------------------------------- reference algorithm
+
+int solve_reference(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), void* ctx, double* x_out, double* y_out,
+                    nir_pdhg_info* info) {
+    cudaStream_t s = h->stream;
+    const double t0 = now_sec();
+    ensure_partials(h);
+    const int n = h->n, m = h->m;
+    nir::DevState st0{};
+    st0.max_iters = p.max_iters;
+    st0.best_kkt = INFINITY;
+    NIR_CUDA(cudaMemcpyAsync(h->st, &st0, sizeof(st0), cudaMemcpyHostToDevice, s));
+    // power iteration, src/gpu/pdhg_solver.hpp:33-45
+    nir::k_fill<<<grid_for(n), nir::kBlock, 0, s>>>(n, 1.0, h->tmp_n);
+    NIR_LAUNCHED();
+    for (int r = 0; r < 12; ++r) {
+        nir::k_ref_spmv<<<std::max(grid_for(m), 1u), nir::kBlock, 0, s>>>(m, h->A.rp, h->A.ci, h->A.v_orig, h->tmp_n, h->tmp_m);
+        nir::k_ref_spmv<<<std::max(grid_for(n), 1u), nir::kBlock, 0, s>>>(n, h->At.rp, h->At.ci, h->At.v_orig, h->tmp_m, h->tmp_n);
+        nir::k_ref_norm<<<1, 32, 0, s>>>(n, h->tmp_n, h->st);
+        nir::k_ref_div<<<std::max(grid_for(n), 1u), nir::kBlock, 0, s>>>(n, h->tmp_n, h->st);
+        NIR_LAUNCHED();
+        h->launches += 4;
+    }
+    nir::k_ref_steps<<<1, 32, 0, s>>>(h->st);
+    nir::k_ref_init<<<std::max(grid_for(std::max(n, m)), 1u), nir::kBlock, 0, s>>>(n, m, h->l, h->u, h->x64, h->y64);
+    NIR_LAUNCHED();
+    h->launches += 3;
+    const int K = 32;
+    const double t_setup = now_sec();
+    LoopResult R;
+    if (p.max_iters > 0) {
+        auto launch = [&]() { launch_ref_chunk(h, K); };
+        if (p.use_graphs) {
+            cudaGraphExec_t ge = chunk_graph(h, 0, 1000, launch);
+            R = run_chunks(h, p, poll, ctx, t0, 0, launches_per_chunk(K, true), [&]() { NIR_CUDA(cudaGraphLaunch(ge, s)); },
+                           nullptr);
+        } else {
+            R = run_chunks(h, p, poll, ctx, t0, 0, 0, [&]() { launch_ref_chunk(h, K); }, nullptr);
+        }
+    }
+    nir::DevState st;
+    d2h(h, &st, h->st, sizeof(st));
+    std::vector<double> x(n), y(m);
+    d2h(h, x.data(), h->x64, n * sizeof(double));
+    d2h(h, y.data(), h->y64, m * sizeof(double));
+    if (x_out) std::memcpy(x_out, x.data(), n * sizeof(double));
+    if (y_out) std::memcpy(y_out, y.data(), m * sizeof(double));
+    int status;
+    if (st.ref_stopped) status = NIR_STATUS_OPTIMAL;
+    else if (st.done) status = NIR_STATUS_ITERATION_LIMIT;
+    else status = NIR_STATUS_TIME_LIMIT;
+    if (p.max_iters <= 0) status = NIR_STATUS_ITERATION_LIMIT;
+    info->status = status;
+    info->iterations = st.done ? st.ref_iterations : st.iter;
+    info->iterations_fp64 = info->iterations;
+    info->objective = host_objective(h, x);
+    info->step_size = st.tau;
+    info->primal_weight = 1.0;
+    info->setup_seconds = t_setup - t0;
+    info->solve_seconds = now_sec() - t_setup;
+    info->rel_kkt = info->rel_primal = info->rel_dual = info->rel_gap = NAN;
+    info->max_rel_row_viol = NAN;
+    (void)R;
+    return status;
+}
+
+// ---------------------------------------------------------------- PDHG / PDLP
+
+void precondition(nir_pdhg* h, const nir_pdhg_params& p, bool enable) {
+    cudaStream_t s = h->stream;
+    const int n = h->n, m = h->m;
+    nir::k_fill<<<grid_for(m), nir::kBlock, 0, s>>>(m, 1.0, h->dr);
+    nir::k_fill<<<grid_for(n), nir::kBlock, 0, s>>>(n, 1.0, h->dc);
+    NIR_LAUNCHED();
+    if (enable) {
+        const unsigned gwm = grid_for((long long)m * 32), gwn = grid_for((long long)n * 32);
+        for (int it = 0; it < p.ruiz_iters + (p.pock_chambolle ? 1 : 0); ++it) {
+            const int mode = it < p.ruiz_iters ? 0 : 1;  // 0 = l-inf (Ruiz), 1 = l1 (Pock-Chambolle)
+            nir::k_row_stat<<<std::max(gwm, 1u), nir::kBlock, 0, s>>>(m, h->A.rp, h->A.ci, h->A.v_orig, h->dr, h->dc, mode,
+                                                                     h->tmp_m);
+            nir::k_row_stat<<<std::max(gwn, 1u), nir::kBlock, 0, s>>>(n, h->At.rp, h->At.ci, h->At.v_orig, h->dc, h->dr,
+                                                                     mode, h->tmp_n);
+            nir::k_apply_stat<<<grid_for(m), nir::kBlock, 0, s>>>(m, h->tmp_m, h->dr);
+            nir::k_apply_stat<<<grid_for(n), nir::kBlock, 0, s>>>(n, h->tmp_n, h->dc);
+            NIR_LAUNCHED();
+            h->launches += 4;
+        }
+        nir::k_round_pow2<<<grid_for(m), nir::kBlock, 0, s>>>(m, h->dr);
+        nir::k_round_pow2<<<grid_for(n), nir::kBlock, 0, s>>>(n, h->dc);
+        NIR_LAUNCHED();
+    }
+    const unsigned gwm = grid_for((long long)m * 32), gwn = grid_for((long long)n * 32);
+    nir::k_scale_values<<<std::max(gwm, 1u), nir::kBlock, 0, s>>>(m, h->A.rp, h->A.ci, h->A.v_orig, h->dr, h->dc, 1,
+                                                                 h->A.v64, h->A.v32);
+    nir::k_scale_values<<<std::max(gwn, 1u), nir::kBlock, 0, s>>>(n, h->At.rp, h->At.ci, h->At.v_orig, h->dc, h->dr, 0,
+                                                                 h->At.v64, h->At.v32);
+    nir::k_scale_vectors<<<std::max(grid_for(std::max(n, m)), 1u), nir::kBlock, 0, s>>>(
+        n, m, h->c, h->l, h->u, h->rl, h->ru, h->dc, h->dr, h->c64, h->l64, h->u64, h->rl64, h->ru64, h->c32, h->l32,
+        h->u32, h->rl32, h->ru32);
+    NIR_LAUNCHED();
+    h->launches += 7;
+}
+
+// ||A_scaled||_2 by power iteration on A'A (FP64, deterministic).
+double power_norm(nir_pdhg* h, int rounds) {
+    cudaStream_t s = h->stream;
+    const int n = h->n, m = h->m;
+    const PartLayout L = part_layout(h);
+    const unsigned gwm = grid_for((long long)m * 32), gwn = grid_for((long long)n * 32);
+    nir::k_power_start<<<std::max(grid_for(n), 1u), nir::kBlock, 0, s>>>(n, h->tmp_n);
+    nir::k_sumsq_partials<<<std::max(grid_for(n), 1u), nir::kBlock, 0, s>>>(n, h->tmp_n, L.misc);
+    nir::k_norm_finalize<<<1, nir::kBlock, 0, s>>>(L.misc, std::max<int>(grid_for(n), 1), h->st);
+    nir::k_scale_by_inv_norm<<<std::max(grid_for(n), 1u), nir::kBlock, 0, s>>>(n, h->tmp_n, h->st);
+    NIR_LAUNCHED();
+    for (int r = 0; r < rounds; ++r) {
+        nir::k_spmv_warp64<<<std::max(gwm, 1u), nir::kBlock, 0, s>>>(m, h->A.rp, h->A.ci, h->A.v64, h->tmp_n, h->tmp_m);
+        nir::k_spmv_warp64<<<std::max(gwn, 1u), nir::kBlock, 0, s>>>(n, h->At.rp, h->At.ci, h->At.v64, h->tmp_m, h->tmp_n);
+        nir::k_sumsq_partials<<<std::max(grid_for(n), 1u), nir::kBlock, 0, s>>>(n, h->tmp_n, L.misc);
+        nir::k_norm_finalize<<<1, nir::kBlock, 0, s>>>(L.misc, std::max<int>(grid_for(n), 1), h->st);
+        nir::k_scale_by_inv_norm<<<std::max(grid_for(n), 1u), nir::kBlock, 0, s>>>(n, h->tmp_n, h->st);
+        NIR_LAUNCHED();
+        h->launches += 5;
+    }
+    nir::DevState st;
+    NIR_CUDA(cudaMemcpyAsync(&st, h->st, sizeof(st), cudaMemcpyDeviceToHost, s));
+    NIR_CUDA(cudaStreamSynchronize(s));
+    return std::sqrt(st.ref_norm_est);  // ||A'A u|| ~ sigma_max^2 for unit u
+}
+
+double norm2(const std::vector<double>& v) {
+    DD s;
+    for (double a : v) s = dd_add_prod(s, a, a);
+    return std::sqrt(s.hi + s.lo);
+}
+
+double rhs_norm(const nir_pdhg* h) {
+    DD s;
+    for (int i = 0; i < h->m; ++i) {
+        double b = 0.0;
+        if (std::isfinite(h->h_rl[i])) b = std::fabs(h->h_rl[i]);
+        if (std::isfinite(h->h_ru[i])) b = std::max(b, std::fabs(h->h_ru[i]));
+        s = dd_add_prod(s, b, b);
+    }
+    return std::sqrt(s.hi + s.lo);
+}
+
+int solve_fast(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), void* ctx, double* x_out, double* y_out,
+               nir_pdhg_info* info) {
+    cudaStream_t s = h->stream;
+    const double t0 = now_sec();
+    const int n = h->n, m = h->m;
+    const bool pdlp = p.algorithm == NIR_ALGO_PDLP;
+    const int cap = p.spmv_block_nnz > 0 ? p.spmv_block_nnz : auto_cap(h->nnz, std::max(m, n));
+    if (cap < 32 || cap > 4096) throw std::invalid_argument("spmv_block_nnz must be in [32, 4096]");
+    set_blocks(h, h->A, cap);
+    set_blocks(h, h->At, cap);
+    ensure_partials(h);
+    SolveCfg cfg;
+    cfg.p = p;
+    cfg.K = std::max(1, p.check_every);
+    cfg.halpern = pdlp ? 1 : 0;
+    cfg.restarts = pdlp ? 1 : 0;
+    cfg.mixed = (p.precision == NIR_PREC_MIXED) ? 1 : 0;
+    cfg.bnorm = rhs_norm(h);
+    cfg.cnorm = norm2(h->h_c);
+    h->ktime = nir_pdhg_kernel_time{};
+
+    precondition(h, p, pdlp && (p.ruiz_iters > 0 || p.pock_chambolle));
+    nir::DevState st0{};
+    st0.max_iters = p.max_iters;
+    st0.best_kkt = INFINITY;
+    double eta, omega;
+    if (pdlp) {
+        const double sig = power_norm(h, std::max(1, p.power_iters));
+        eta = p.step_factor / std::max(sig, 1e-30);
+        // primal weight: ||c^|| / ||b^|| in the scaled space
+        std::vector<double> dc(n), dr(m);
+        d2h(h, dc.data(), h->dc, n * sizeof(double));
+        d2h(h, dr.data(), h->dr, m * sizeof(double));
+        DD cs, bs;
+        for (int j = 0; j < n; ++j) cs = dd_add_prod(cs, h->h_c[j] * dc[j], h->h_c[j] * dc[j]);
+        for (int i = 0; i < m; ++i) {
+            double b = 0.0;
+            if (std::isfinite(h->h_rl[i])) b = std::fabs(h->h_rl[i]);
+            if (std::isfinite(h->h_ru[i])) b = std::max(b, std::fabs(h->h_ru[i]));
+            b *= dr[i];
+            bs = dd_add_prod(bs, b, b);
+        }
+        const double cn = std::sqrt(cs.hi + cs.lo), bn = std::sqrt(bs.hi + bs.lo);
+        omega = (cn > 1e-10 && bn > 1e-10) ? cn / bn : 1.0;
+        if (p.omega_init > 0.0) omega = p.omega_init;
+        st0.eta = eta;
+        st0.omega = omega;
+        st0.tau = eta / omega;
+        st0.sigma = eta * omega;
+    } else {
+        // plain PDHG: the reference's fixed steps from its own power iteration
+        NIR_CUDA(cudaMemcpyAsync(h->st, &st0, sizeof(st0), cudaMemcpyHostToDevice, s));
+        nir::k_fill<<<std::max(grid_for(n), 1u), nir::kBlock, 0, s>>>(n, 1.0, h->tmp_n);
+        for (int r = 0; r < 12; ++r) {
+            nir::k_ref_spmv<<<std::max(grid_for(m), 1u), nir::kBlock, 0, s>>>(m, h->A.rp, h->A.ci, h->A.v_orig, h->tmp_n, h->tmp_m);
+            nir::k_ref_spmv<<<std::max(grid_for(n), 1u), nir::kBlock, 0, s>>>(n, h->At.rp, h->At.ci, h->At.v_orig, h->tmp_m, h->tmp_n);
+            nir::k_ref_norm<<<1, 32, 0, s>>>(n, h->tmp_n, h->st);
+            nir::k_ref_div<<<std::max(grid_for(n), 1u), nir::kBlock, 0, s>>>(n, h->tmp_n, h->st);
+        }
+        nir::k_ref_steps<<<1, 32, 0, s>>>(h->st);
+        NIR_LAUNCHED();
+        nir::DevState tmp;
+        NIR_CUDA(cudaMemcpyAsync(&tmp, h->st, sizeof(tmp), cudaMemcpyDeviceToHost, s));
+        NIR_CUDA(cudaStreamSynchronize(s));
+        eta = tmp.tau;
+        omega = 1.0;
+        st0.eta = eta;
+        st0.omega = 1.0;
+        st0.tau = eta;
+        st0.sigma = eta;
+    }
+    NIR_CUDA(cudaMemcpyAsync(h->st, &st0, sizeof(st0), cudaMemcpyHostToDevice, s));
+    // starting point
+    double* d_xin = nullptr;
+    double* d_yin = nullptr;
+    if (p.x_init) {
+        NIR_CUDA(cudaMemcpyAsync(h->out_x, p.x_init, n * sizeof(double), cudaMemcpyHostToDevice, s));
+        d_xin = h->out_x;
+    }
+    if (p.y_init) {
+        NIR_CUDA(cudaMemcpyAsync(h->out_y, p.y_init, m * sizeof(double), cudaMemcpyHostToDevice, s));
+        d_yin = h->out_y;
+    }
+    if (!pdlp && !p.x_init) {
+        // the reference's box-midpoint start (dr = dc = 1 here)
+        nir::k_ref_init<<<std::max(grid_for(std::max(n, m)), 1u), nir::kBlock, 0, s>>>(n, m, h->l, h->u, h->out_x, h->out_y);
+        d_xin = h->out_x;
+        d_yin = h->out_y;
+    }
+    nir::k_init_iterates<<<std::max(grid_for(std::max(n, m)), 1u), nir::kBlock, 0, s>>>(
+        n, m, d_xin, d_yin, h->dc, h->dr, h->l64, h->u64, h->x64, h->x064, h->y64, h->y064, h->x32, h->x032, h->y32,
+        h->y032, h->l32, h->u32);
+    NIR_LAUNCHED();
+    // plain PDHG never reads the anchors in the update, but CHECK reads x0
+    NIR_CUDA(cudaStreamSynchronize(s));
+    const double t_setup = now_sec();
+
+    ChunkTimer tm;
+    if (h->profiling) {
+        for (auto& e : tm.e) NIR_CUDA(cudaEventCreate(&e));
+        tm.armed = true;
+        tm.K = cfg.K;
+    }
+    const bool fp64_first = (p.precision == NIR_PREC_FP64);
+    LoopResult R;
+    int final_phase = 0;
+    double t_switch = 0.0;
+    try {
+        auto run_phase = [&](int phase, bool f64) {
+            auto launch = [&, phase, f64]() {
+                if (f64) launch_fast_chunk<double>(h, cfg, phase, h->profiling ? &tm : nullptr);
+                else launch_fast_chunk<float>(h, cfg, phase, h->profiling ? &tm : nullptr);
+            };
+            const int per = launches_per_chunk(cfg.K, false);
+            if (p.use_graphs && !h->profiling) {
+                const int key = (f64 ? 1 : 0) + 2 * phase + 4 * cfg.K + 100000 * (cap + 1) + 1000000000 * (pdlp ? 1 : 0);
+                cudaGraphExec_t ge = chunk_graph(h, 1 + phase, key, launch);
+                return run_chunks(h, p, poll, ctx, t0, phase, per, [&]() { NIR_CUDA(cudaGraphLaunch(ge, s)); }, nullptr);
+            }
+            return run_chunks(h, p, poll, ctx, t0, phase, 0, launch, h->profiling ? &tm : nullptr);
+        };
+        if (p.max_iters > 0) {
+            R = run_phase(0, fp64_first);
+            if (!R.stopped_by_host && cfg.mixed && !R.last.done && R.last.phase == 1) {
+                // FP32 stalled: polish in FP64 from the last evaluated point
+                t_switch = now_sec() - t_setup;
+                nir::k_promote<<<std::max(grid_for(std::max(n, m)), 1u), nir::kBlock, 0, s>>>(
+                    n, m, h->xp32, h->yp32, h->l64, h->u64, h->x64, h->x064, h->xp64, h->y64, h->y064, h->yp64);
+                NIR_LAUNCHED();
+                nir::DevState cur;
+                d2h(h, &cur, h->st, sizeof(cur));
+                cur.k_base = 0;
+                cur.have_anchor = 0;
+                cur.apply_restart = 0;
+                cur.switch_request = 0;
+                cur.stall = 0;
+                h2d(h, h->st, &cur, sizeof(cur));
+                final_phase = 1;
+                long long it_switch = cur.iter;
+                R = run_phase(1, true);
+                info->iterations_fp64 = 0;
+                nir::DevState fin;
+                d2h(h, &fin, h->st, sizeof(fin));
+                info->iterations_fp64 = fin.iter - it_switch;
+            }
+        }
+    } catch (...) {
+        if (tm.armed)
+            for (auto& e : tm.e) cudaEventDestroy(e);
+        throw;
+    }
+    if (tm.armed)
+        for (auto& e : tm.e) cudaEventDestroy(e);
+    nir::DevState st;
+    d2h(h, &st, h->st, sizeof(st));
+    const bool out64 = fp64_first || final_phase == 1;
+    const unsigned g = std::max(grid_for(std::max(n, m)), 1u);
+    if (out64) nir::k_unscale_out<double><<<g, nir::kBlock, 0, s>>>(n, m, h->xp64, h->yp64, h->dc, h->dr, h->out_x, h->out_y);
+    else nir::k_unscale_out<float><<<g, nir::kBlock, 0, s>>>(n, m, h->xp32, h->yp32, h->dc, h->dr, h->out_x, h->out_y);
+    NIR_LAUNCHED();
+    std::vector<double> x(n), y(m);
+    NIR_CUDA(cudaMemcpyAsync(x.data(), h->out_x, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    NIR_CUDA(cudaMemcpyAsync(y.data(), h->out_y, m * sizeof(double), cudaMemcpyDeviceToHost, s));
+    NIR_CUDA(cudaStreamSynchronize(s));
+    if (x_out) std::memcpy(x_out, x.data(), n * sizeof(double));
+    if (y_out) std::memcpy(y_out, y.data(), m * sizeof(double));
+    int status;
+    if (st.done) status = st.status;
+    else if (R.stopped_by_host) status = NIR_STATUS_TIME_LIMIT;
+    else status = NIR_STATUS_ITERATION_LIMIT;
+    if (p.max_iters <= 0) status = NIR_STATUS_ITERATION_LIMIT;
+    fill_info_common(h, st, info);
+    info->status = status;
+    info->iterations = st.iter;
+    if (fp64_first) info->iterations_fp64 = st.iter;
+    info->objective = host_objective(h, x);
+    info->setup_seconds = t_setup - t0;
+    info->solve_seconds = now_sec() - t_setup;
+    info->time_to_fp64_seconds = t_switch;
+    return status;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- C ABI
+
+extern "C" {
+
+int nir_pdhg_default_params(nir_pdhg_params* p) {
+    if (!p) return NIR_STATUS_INPUT_ERROR;
+    std::memset(p, 0, sizeof(*p));
+    p->algorithm = NIR_ALGO_PDLP;
+    p->precision = NIR_PREC_MIXED;
+    p->tol = 1e-6;
+    p->feas_tol = 0.0;
+    p->max_iters = 1000000;
+    p->time_limit = 0.0;
+    p->check_every = 64;
+    p->ruiz_iters = 10;
+    p->pock_chambolle = 1;
+    p->reflection = 1.0;
+    p->restart_sufficient = 0.2;
+    p->restart_necessary = 0.8;
+    p->restart_artificial = 0.36;
+    p->primal_weight_smoothing = 0.5;
+    p->step_factor = 0.998;
+    p->power_iters = 64;
+    p->polish_stall_checks = 6;
+    p->polish_switch_kkt = 0.0;
+    p->spmv_block_nnz = 0;
+    p->use_graphs = 1;
+    p->verbose = 0;
+    p->x_init = nullptr;
+    p->y_init = nullptr;
+    p->omega_init = 0.0;
+    return 0;
+}
+
+const char* nir_pdhg_last_error(void) { return g_err.c_str(); }
+
+int nir_pdhg_create(const nir_lp_view* lp, int device, nir_pdhg** out) {
+    if (!out) {
+        g_err = "null output handle";
+        return NIR_STATUS_INPUT_ERROR;
+    }
+    *out = nullptr;
+    try {
+        validate_lp(lp);
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return NIR_STATUS_INPUT_ERROR;
+    }
+    auto h = std::make_unique<nir_pdhg>();
+    h->device = -1;
+    try {
+        create_impl(h.get(), lp, device);
+    } catch (const std::invalid_argument& e) {
+        g_err = e.what();
+        return NIR_STATUS_INPUT_ERROR;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return NIR_STATUS_INTERNAL_ERROR;
+    }
+    *out = h.release();
+    return 0;
+}
+
+int nir_pdhg_update_vectors(nir_pdhg* h, const double* cost, const double* collo, const double* colup,
+                            const double* rowlo, const double* rowup) {
+    if (!h) {
+        g_err = "null handle";
+        return NIR_STATUS_INPUT_ERROR;
+    }
+    try {
+        NIR_CUDA(cudaSetDevice(h->device));
+        if (cost)
+            for (int j = 0; j < h->n; ++j)
+                if (!std::isfinite(cost[j])) throw std::invalid_argument("non-finite cost");
+        upload_vectors(h, cost, collo, colup, rowlo, rowup);
+        return 0;
+    } catch (const std::invalid_argument& e) {
+        g_err = e.what();
+        return NIR_STATUS_INPUT_ERROR;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return NIR_STATUS_INTERNAL_ERROR;
+    }
+}
+
+int nir_pdhg_solve(nir_pdhg* h, const nir_pdhg_params* p_in, int (*poll)(void*), void* poll_ctx, double* x_out,
+                   double* y_out, nir_pdhg_info* info) {
+    nir_pdhg_info dummy;
+    if (!info) info = &dummy;
+    std::memset(info, 0, sizeof(*info));
+    if (!h) {
+        g_err = "null handle";
+        return info->status = NIR_STATUS_INPUT_ERROR;
+    }
+    nir_pdhg_params p;
+    if (p_in) p = *p_in;
+    else nir_pdhg_default_params(&p);
+    if (p.algorithm < 0 || p.algorithm > 2 || p.precision < 0 || p.precision > 2 || !(p.tol >= 0.0) ||
+        p.check_every < 1 || p.reflection < 0.0 || p.reflection > 1.0) {
+        g_err = "invalid parameters";
+        return info->status = NIR_STATUS_INPUT_ERROR;
+    }
+    try {
+        NIR_CUDA(cudaSetDevice(h->device));
+        const int before = h->launches;
+        int st;
+        if (p.algorithm == NIR_ALGO_REFERENCE) st = solve_reference(h, p, poll, poll_ctx, x_out, y_out, info);
+        else st = solve_fast(h, p, poll, poll_ctx, x_out, y_out, info);
+        info->kernel_launches = h->launches - before;
+        return st;
+    } catch (const std::invalid_argument& e) {
+        g_err = e.what();
+        return info->status = NIR_STATUS_INPUT_ERROR;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return info->status = NIR_STATUS_INTERNAL_ERROR;
+    }
+}
+
+int nir_pdhg_solve_lp(const nir_lp_view* lp, int device, const nir_pdhg_params* p, int (*poll)(void*), void* ctx,
+                      double* x_out, double* y_out, nir_pdhg_info* info) {
+    nir_pdhg* h = nullptr;
+    int rc = nir_pdhg_create(lp, device, &h);
+    if (rc != 0) {
+        if (info) {
+            std::memset(info, 0, sizeof(*info));
+            info->status = rc;
+        }
+        return rc;
+    }
+    const double t0 = now_sec();
+    rc = nir_pdhg_solve(h, p, poll, ctx, x_out, y_out, info);
+    (void)t0;
+    nir_pdhg_free(h);
+    return rc;
+}
+
+void nir_pdhg_free(nir_pdhg* h) { delete h; }
+
+int nir_pdhg_spmv(nir_pdhg* h, int transpose, int kernel, const double* x, double* y) {
+    if (!h || !x || !y || kernel < 0 || kernel > 2) {
+        g_err = "invalid arguments";
+        return NIR_STATUS_INPUT_ERROR;
+    }
+    try {
+        NIR_CUDA(cudaSetDevice(h->device));
+        cudaStream_t s = h->stream;
+        Orient& o = transpose ? h->At : h->A;
+        const int nin = o.cols, nout = o.rows;
+        double* din = transpose ? h->tmp_m : h->tmp_n;
+        double* dout = transpose ? h->tmp_n : h->tmp_m;
+        NIR_CUDA(cudaMemcpyAsync(din, x, nin * sizeof(double), cudaMemcpyHostToDevice, s));
+        if (kernel == 0) {
+            nir::k_ref_spmv<<<std::max(grid_for(nout), 1u), nir::kBlock, 0, s>>>(nout, o.rp, o.ci, o.v_orig, din, dout);
+            NIR_LAUNCHED();
+        } else {
+            if (!o.blk) set_blocks(h, o, auto_cap(h->nnz, nout));
+            if (kernel == 1) {
+                nir::k_spmv_adaptive<double, double, double><<<o.nblk, nir::kBlock, o.cap * sizeof(double), s>>>(
+                    o.blk, o.rp, o.ci, o.v_orig, din, dout);
+                NIR_LAUNCHED();
+            } else {
+                if (!o.v32_orig) {
+                    o.v32_orig = h->alloc<float>(o.nnz);
+                    nir::k_to_float<<<grid_for(o.nnz), nir::kBlock, 0, s>>>(o.nnz, o.v_orig, o.v32_orig);
+                }
+                float* fin = transpose ? h->tmp_m32 : h->tmp_n32;
+                float* fout = transpose ? h->tmp_n32 : h->tmp_m32;
+                nir::k_to_float<<<std::max(grid_for(nin), 1u), nir::kBlock, 0, s>>>(nin, din, fin);
+                nir::k_spmv_adaptive<float, float, float><<<o.nblk, nir::kBlock, o.cap * sizeof(float), s>>>(
+                    o.blk, o.rp, o.ci, o.v32_orig, fin, fout);
+                nir::k_to_double<<<std::max(grid_for(nout), 1u), nir::kBlock, 0, s>>>(nout, fout, dout);
+                NIR_LAUNCHED();
+            }
+        }
+        NIR_CUDA(cudaMemcpyAsync(y, dout, nout * sizeof(double), cudaMemcpyDeviceToHost, s));
+        NIR_CUDA(cudaStreamSynchronize(s));
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return NIR_STATUS_INTERNAL_ERROR;
+    }
+}
+
+int nir_pdhg_time_spmv(nir_pdhg* h, int transpose, int kernel, int reps, int flush_l2, double* usec) {
+    if (!h || !usec || reps < 1 || kernel < 0 || kernel > 2) {
+        g_err = "invalid arguments";
+        return NIR_STATUS_INPUT_ERROR;
+    }
+    try {
+        NIR_CUDA(cudaSetDevice(h->device));
+        cudaStream_t s = h->stream;
+        Orient& o = transpose ? h->At : h->A;
+        const int nin = o.cols, nout = o.rows;
+        if (!o.blk) set_blocks(h, o, auto_cap(h->nnz, nout));
+        if (kernel == 2 && !o.v32_orig) {
+            o.v32_orig = h->alloc<float>(o.nnz);
+            nir::k_to_float<<<grid_for(o.nnz), nir::kBlock, 0, s>>>(o.nnz, o.v_orig, o.v32_orig);
+        }
+        double* din = transpose ? h->tmp_m : h->tmp_n;
+        double* dout = transpose ? h->tmp_n : h->tmp_m;
+        float* fin = transpose ? h->tmp_m32 : h->tmp_n32;
+        float* fout = transpose ? h->tmp_n32 : h->tmp_m32;
+        nir::k_fill<<<std::max(grid_for(nin), 1u), nir::kBlock, 0, s>>>(nin, 1.0, din);
+        nir::k_to_float<<<std::max(grid_for(nin), 1u), nir::kBlock, 0, s>>>(nin, din, fin);
+        if (flush_l2 && !h->flush) {
+            h->flush_bytes = size_t(512) << 20;
+            h->flush = h->alloc<unsigned char>(h->flush_bytes);
+        }
+        cudaEvent_t a, b;
+        NIR_CUDA(cudaEventCreate(&a));
+        NIR_CUDA(cudaEventCreate(&b));
+        double total_ms = 0.0;
+        for (int r = 0; r < reps + 1; ++r) {
+            if (flush_l2) NIR_CUDA(cudaMemsetAsync(h->flush, r & 0xff, h->flush_bytes, s));
+            NIR_CUDA(cudaEventRecord(a, s));
+            if (kernel == 0)
+                nir::k_ref_spmv<<<std::max(grid_for(nout), 1u), nir::kBlock, 0, s>>>(nout, o.rp, o.ci, o.v_orig, din, dout);
+            else if (kernel == 1)
+                nir::k_spmv_adaptive<double, double, double><<<o.nblk, nir::kBlock, o.cap * sizeof(double), s>>>(
+                    o.blk, o.rp, o.ci, o.v_orig, din, dout);
+            else
+                nir::k_spmv_adaptive<float, float, float><<<o.nblk, nir::kBlock, o.cap * sizeof(float), s>>>(
+                    o.blk, o.rp, o.ci, o.v32_orig, fin, fout);
+            NIR_LAUNCHED();
+            NIR_CUDA(cudaEventRecord(b, s));
+            NIR_CUDA(cudaEventSynchronize(b));
+            float ms = 0.0f;
+            NIR_CUDA(cudaEventElapsedTime(&ms, a, b));
+            if (r > 0) total_ms += ms;  // the first launch is a warm-up
+        }
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        *usec = 1000.0 * total_ms / reps;
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return NIR_STATUS_INTERNAL_ERROR;
+    }
+}
+
+int nir_pdhg_set_profiling(nir_pdhg* h, int on) {
+    if (!h) return NIR_STATUS_INPUT_ERROR;
+    h->profiling = on != 0;
+    return 0;
+}
+
+int nir_pdhg_kernel_times(nir_pdhg* h, nir_pdhg_kernel_time* out) {
+    if (!h || !out) return NIR_STATUS_INPUT_ERROR;
+    *out = h->ktime;
+    if (out->samples > 0) {
+        out->primal_us /= double(out->samples);
+        out->dual_us /= double(out->samples);
+        out->iter_us /= double(out->samples);
+    }
+    return 0;
+}
+
+int nir_pdhg_get_layout(nir_pdhg* h, nir_pdhg_layout* out) {
+    if (!h || !out) return NIR_STATUS_INPUT_ERROR;
+    out->nrow = h->m;
+    out->ncol = h->n;
+    out->nnz = h->nnz;
+    out->blocks_a = h->A.nblk;
+    out->blocks_at = h->At.nblk;
+    out->block_nnz = h->A.cap;
+    out->device_bytes = h->device_bytes;
+    return 0;
+}
+
+}  // extern "C"

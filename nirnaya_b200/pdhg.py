@@ -1,0 +1,284 @@
+"""Python mirror of the reference's PDHG interface over the C ABI.
+
+The reference's path is `sov::PdhgSolver::solve(const Model&, const
+Options&, const Deadline&) -> PdhgResult` (src/gpu/pdhg_solver.hpp:14-25).
+This module keeps those names and meanings:
+
+  * `Options.threads`, `Options.simplex_iter_limit` and `Options.time_limit`
+    mean what they mean in src/core/options.hpp:10-32; the iteration cap is
+    max(5000, simplex_iter_limit // 10) as at src/gpu/pdhg_solver.hpp:60;
+  * `Deadline` mirrors src/core/timer.hpp:34-46 (wall limit plus a stop flag
+    that another thread may set, like Solver::interrupt);
+  * `PdhgResult` has the reference's fields (status, objective, x, y,
+    iterations) plus the engine's diagnostics.
+
+Everything runs in libnir_pdhg.so on the GPU.  There is no CPU fallback:
+if the library or a CUDA device is missing, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .lp import LP, NirLpView
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libnir_pdhg.so")
+
+# sov::Status (src/core/status.hpp:7-24)
+OPTIMAL, TIME_LIMIT, ITERATION_LIMIT, INTERRUPTED, NUMERICAL_TROUBLE, INPUT_ERROR, INTERNAL_ERROR = 0, 4, 6, 10, 11, 12, 14
+STATUS_NAMES = {0: "optimal", 4: "time_limit", 6: "iteration_limit", 10: "interrupted", 11: "numerical_trouble",
+                12: "input_error", 14: "internal_error"}
+
+ALGO_REFERENCE, ALGO_PDHG, ALGO_PDLP = 0, 1, 2
+PREC_FP64, PREC_MIXED, PREC_FP32 = 0, 1, 2
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("algorithm", C.c_int32), ("precision", C.c_int32), ("tol", C.c_double), ("feas_tol", C.c_double),
+        ("max_iters", C.c_int64), ("time_limit", C.c_double), ("check_every", C.c_int32),
+        ("ruiz_iters", C.c_int32), ("pock_chambolle", C.c_int32), ("reflection", C.c_double),
+        ("restart_sufficient", C.c_double), ("restart_necessary", C.c_double),
+        ("restart_artificial", C.c_double), ("primal_weight_smoothing", C.c_double),
+        ("step_factor", C.c_double), ("power_iters", C.c_int32), ("polish_stall_checks", C.c_int32),
+        ("polish_switch_kkt", C.c_double), ("spmv_block_nnz", C.c_int32), ("use_graphs", C.c_int32),
+        ("verbose", C.c_int32), ("x_init", C.POINTER(C.c_double)), ("y_init", C.POINTER(C.c_double)),
+        ("omega_init", C.c_double),
+    ]
+
+
+class Info(C.Structure):
+    _fields_ = [
+        ("status", C.c_int32), ("restarts", C.c_int32), ("iterations", C.c_int64),
+        ("iterations_fp64", C.c_int64), ("objective", C.c_double), ("rel_kkt", C.c_double),
+        ("rel_primal", C.c_double), ("rel_dual", C.c_double), ("rel_gap", C.c_double),
+        ("max_rel_row_viol", C.c_double), ("primal_weight", C.c_double), ("step_size", C.c_double),
+        ("setup_seconds", C.c_double), ("solve_seconds", C.c_double), ("time_to_fp64_seconds", C.c_double),
+        ("kernel_launches", C.c_int32),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class KernelTime(C.Structure):
+    _fields_ = [("primal_us", C.c_double), ("dual_us", C.c_double), ("iter_us", C.c_double),
+                ("samples", C.c_int64)]
+
+
+class Layout(C.Structure):
+    _fields_ = [("nrow", C.c_int32), ("ncol", C.c_int32), ("nnz", C.c_int64), ("blocks_a", C.c_int32),
+                ("blocks_at", C.c_int32), ("block_nnz", C.c_int32), ("device_bytes", C.c_int64)]
+
+
+POLL_FN = C.CFUNCTYPE(C.c_int, C.c_void_p)
+
+EXPORTED = [
+    "nir_pdhg_default_params", "nir_pdhg_create", "nir_pdhg_update_vectors", "nir_pdhg_solve",
+    "nir_pdhg_solve_lp", "nir_pdhg_free", "nir_pdhg_last_error", "nir_pdhg_spmv", "nir_pdhg_time_spmv",
+    "nir_pdhg_set_profiling", "nir_pdhg_kernel_times", "nir_pdhg_get_layout",
+]
+
+_lib = None
+
+
+def lib():
+    """Loads libnir_pdhg.so (raises if it is missing: no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing; build it with `python -m nirnaya_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        VP = C.POINTER(NirLpView)
+        D = C.POINTER(C.c_double)
+        L.nir_pdhg_default_params.argtypes = [C.POINTER(Params)]
+        L.nir_pdhg_create.argtypes = [VP, C.c_int, C.POINTER(C.c_void_p)]
+        L.nir_pdhg_update_vectors.argtypes = [C.c_void_p, D, D, D, D, D]
+        L.nir_pdhg_solve.argtypes = [C.c_void_p, C.POINTER(Params), POLL_FN, C.c_void_p, D, D, C.POINTER(Info)]
+        L.nir_pdhg_solve_lp.argtypes = [VP, C.c_int, C.POINTER(Params), POLL_FN, C.c_void_p, D, D, C.POINTER(Info)]
+        L.nir_pdhg_free.argtypes = [C.c_void_p]
+        L.nir_pdhg_last_error.restype = C.c_char_p
+        L.nir_pdhg_spmv.argtypes = [C.c_void_p, C.c_int, C.c_int, D, D]
+        L.nir_pdhg_time_spmv.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, D]
+        L.nir_pdhg_set_profiling.argtypes = [C.c_void_p, C.c_int]
+        L.nir_pdhg_kernel_times.argtypes = [C.c_void_p, C.POINTER(KernelTime)]
+        L.nir_pdhg_get_layout.argtypes = [C.c_void_p, C.POINTER(Layout)]
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    return lib().nir_pdhg_last_error().decode()
+
+
+def default_params(**overrides) -> Params:
+    p = Params()
+    lib().nir_pdhg_default_params(C.byref(p))
+    for k, v in overrides.items():
+        setattr(p, k, v)
+    return p
+
+
+def _dptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Engine:
+    """One LP resident on one GPU (nir_pdhg_create ... nir_pdhg_free)."""
+
+    def __init__(self, lp: LP, device: int = 0):
+        self.lp = lp
+        self._h = C.c_void_p()
+        rc = lib().nir_pdhg_create(C.byref(lp.view()), device, C.byref(self._h))
+        if rc != 0:
+            raise RuntimeError(f"nir_pdhg_create failed ({STATUS_NAMES.get(rc, rc)}): {last_error()}")
+
+    def close(self):
+        if self._h:
+            lib().nir_pdhg_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def update_vectors(self, cost=None, collo=None, colup=None, rowlo=None, rowup=None):
+        arrs = [None if a is None else np.ascontiguousarray(a, np.float64) for a in (cost, collo, colup, rowlo, rowup)]
+        ptrs = [None if a is None else _dptr(a) for a in arrs]
+        rc = lib().nir_pdhg_update_vectors(self._h, *ptrs)
+        if rc != 0:
+            raise RuntimeError(last_error())
+        for name, a in zip(("cost", "collo", "colup", "rowlo", "rowup"), arrs):
+            if a is not None:
+                setattr(self.lp, name, a)
+        self.lp._view = None
+
+    def solve(self, params: Params | None = None, poll=None, x_init=None, y_init=None, omega_init=None):
+        p = params if params is not None else default_params()
+        keep = []
+        if x_init is not None:
+            xa = np.ascontiguousarray(x_init, np.float64)
+            keep.append(xa)
+            p.x_init = _dptr(xa)
+        if y_init is not None:
+            ya = np.ascontiguousarray(y_init, np.float64)
+            keep.append(ya)
+            p.y_init = _dptr(ya)
+        if omega_init is not None:
+            p.omega_init = float(omega_init)
+        x = np.zeros(self.lp.ncol)
+        y = np.zeros(self.lp.nrow)
+        info = Info()
+        cb = POLL_FN(0) if poll is None else POLL_FN(lambda _ctx: 1 if poll() else 0)
+        lib().nir_pdhg_solve(self._h, C.byref(p), cb, None, _dptr(x), _dptr(y), C.byref(info))
+        if info.status in (INPUT_ERROR, INTERNAL_ERROR):
+            raise RuntimeError(f"nir_pdhg_solve failed ({STATUS_NAMES[info.status]}): {last_error()}")
+        return x, y, info
+
+    def spmv(self, x, transpose: bool = False, kernel: int = 1):
+        nout = self.lp.ncol if transpose else self.lp.nrow
+        y = np.zeros(nout)
+        rc = lib().nir_pdhg_spmv(self._h, int(transpose), kernel, _dptr(np.ascontiguousarray(x, np.float64)), _dptr(y))
+        if rc != 0:
+            raise RuntimeError(last_error())
+        return y
+
+    def time_spmv(self, transpose: bool, kernel: int, reps: int = 20, flush_l2: bool = True) -> float:
+        us = C.c_double()
+        rc = lib().nir_pdhg_time_spmv(self._h, int(transpose), kernel, reps, int(flush_l2), C.byref(us))
+        if rc != 0:
+            raise RuntimeError(last_error())
+        return us.value
+
+    def set_profiling(self, on: bool):
+        lib().nir_pdhg_set_profiling(self._h, int(on))
+
+    def kernel_times(self) -> KernelTime:
+        kt = KernelTime()
+        lib().nir_pdhg_kernel_times(self._h, C.byref(kt))
+        return kt
+
+    def layout(self) -> Layout:
+        lo = Layout()
+        lib().nir_pdhg_get_layout(self._h, C.byref(lo))
+        return lo
+
+
+# ------------------------------------------------------- reference-shaped API
+
+@dataclass
+class Options:
+    """The fields of sov::Options (src/core/options.hpp:9-32) the path reads,
+    plus the engine's knobs (defaults: include/nir_pdhg.h)."""
+    time_limit: float = 600.0
+    threads: int = 1
+    simplex_iter_limit: int = 500000
+    method: str = "pdhg"
+    pdhg_algorithm: int = ALGO_PDLP
+    pdhg_precision: int = PREC_MIXED
+    pdhg_tol: float = 1e-6
+    pdhg_feas_tol: float = 0.0
+    pdhg_max_iters: int = 0            # 0 = the reference's max(5000, simplex_iter_limit // 10)
+    device: int = 0
+    extra: dict = field(default_factory=dict)
+
+
+class Deadline:
+    """sov::Deadline (src/core/timer.hpp:34-46): wall limit + stop flag."""
+
+    def __init__(self, wall_limit_sec: float = float("inf")):
+        self.start = time.monotonic()
+        self.wall_limit_sec = wall_limit_sec
+        self._stop = threading.Event()
+
+    def interrupt(self):
+        self._stop.set()
+
+    def expired(self) -> bool:
+        return self._stop.is_set() or (time.monotonic() - self.start) >= self.wall_limit_sec
+
+
+@dataclass
+class PdhgResult:
+    status: int
+    objective: float
+    x: np.ndarray
+    y: np.ndarray
+    iterations: int
+    info: dict = field(default_factory=dict)
+
+
+class PdhgSolver:
+    """sov::PdhgSolver (src/gpu/pdhg_solver.hpp:23-108) on the GPU."""
+
+    @staticmethod
+    def params_from(options: Options) -> Params:
+        cap = options.pdhg_max_iters or max(5000, options.simplex_iter_limit // 10)
+        p = default_params(algorithm=options.pdhg_algorithm, precision=options.pdhg_precision,
+                           tol=options.pdhg_tol, feas_tol=options.pdhg_feas_tol, max_iters=cap)
+        for k, v in options.extra.items():
+            setattr(p, k, v)
+        return p
+
+    @staticmethod
+    def solve(model: LP, options: Options | None = None, deadline: Deadline | None = None) -> PdhgResult:
+        options = options or Options()
+        deadline = deadline or Deadline(options.time_limit)
+        p = PdhgSolver.params_from(options)
+        with Engine(model, options.device) as eng:
+            x, y, info = eng.solve(p, poll=deadline.expired)
+        return PdhgResult(info.status, info.objective, x, y, int(info.iterations), info.as_dict())

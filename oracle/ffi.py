@@ -1,0 +1,239 @@
+"""ctypes bindings of the oracle (liboracle.so, our C restatement) and of the
+reference compiled from source (_ref/libref_nirnaya.so).
+
+Test infrastructure only: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline leg.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from nirnaya_b200.lp import LP, NirLpView
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libref_nirnaya.so")
+
+_VP = C.POINTER(NirLpView)
+_D = C.POINTER(C.c_double)
+
+
+class PdhgOut(C.Structure):
+    _fields_ = [("iterations", C.c_int64), ("stopped", C.c_int32), ("objective", C.c_double),
+                ("tau", C.c_double), ("sigma", C.c_double), ("first_hit", C.c_int64),
+                ("last_kkt", C.c_double)]
+
+
+class VerifyReport(C.Structure):
+    _fields_ = [("passed", C.c_int32), ("max_bound_viol", C.c_double), ("max_row_viol", C.c_double),
+                ("computed_obj", C.c_double), ("obj_rel_err", C.c_double)]
+
+
+class Kkt(C.Structure):
+    _fields_ = [("rel_primal", C.c_double), ("rel_dual", C.c_double), ("rel_gap", C.c_double),
+                ("rel_kkt", C.c_double), ("pobj", C.c_double), ("dobj", C.c_double),
+                ("max_rel_row_viol", C.c_double)]
+
+
+def _dptr(a):
+    return a.ctypes.data_as(_D)
+
+
+_oracle = None
+_ref = None
+
+
+def oracle_lib():
+    global _oracle
+    if _oracle is None:
+        if not os.path.exists(ORACLE_SO):
+            subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
+        lib = C.CDLL(ORACLE_SO)
+        lib.or_dd_cancellation_probe.restype = C.c_double
+        lib.or_dd_cancellation_probe.argtypes = [C.c_double] * 3
+        lib.or_neumaier_probe.restype = C.c_double
+        lib.or_neumaier_probe.argtypes = [C.c_double] * 3
+        lib.or_spmv.argtypes = [_VP, _D, _D]
+        lib.or_spmv_t.argtypes = [_VP, _D, _D]
+        lib.or_csc_from_triplets.restype = C.c_int64
+        lib.or_csc_from_triplets.argtypes = [C.c_int32, C.c_int32, C.c_int64, C.POINTER(C.c_int32),
+                                             C.POINTER(C.c_int32), _D, C.POINTER(C.c_int64),
+                                             C.POINTER(C.c_int32), _D]
+        lib.or_ref_pdhg.argtypes = [_VP, C.c_int64, C.c_int64, C.c_double, C.c_int, _D, _D, C.POINTER(PdhgOut)]
+        lib.or_eval_objective.restype = C.c_double
+        lib.or_eval_objective.argtypes = [_VP, _D]
+        lib.or_verify.argtypes = [_VP, _D, C.c_double, C.c_double, C.POINTER(VerifyReport)]
+        lib.or_rel_kkt.argtypes = [_VP, _D, _D, C.POINTER(Kkt)]
+        _oracle = lib
+    return _oracle
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        if not ref_available():
+            raise RuntimeError(f"{REF_SO} is missing (built from the reference sources by oracle/Makefile)")
+        lib = C.CDLL(REF_SO)
+        lib.ref_last_error.restype = C.c_char_p
+        lib.ref_pdhg_solve.argtypes = [_VP, C.c_int, C.c_int, C.c_double, _D, _D, C.POINTER(C.c_int),
+                                       _D, C.POINTER(C.c_int)]
+        lib.ref_solver_solve.argtypes = [_VP, C.c_int, C.c_char_p, C.c_int, C.c_int, _D, C.POINTER(C.c_int),
+                                         _D, C.POINTER(C.c_int)]
+        lib.ref_verify.argtypes = [_VP, _D, C.c_double, C.c_double, C.POINTER(C.c_int), _D, _D, _D, _D]
+        lib.ref_eval_objective.restype = C.c_double
+        lib.ref_eval_objective.argtypes = [_VP, _D]
+        lib.ref_spmv.argtypes = [_VP, _D, _D]
+        lib.ref_spmv_t.argtypes = [_VP, _D, _D]
+        lib.ref_from_triplets.restype = C.c_int64
+        lib.ref_from_triplets.argtypes = [C.c_int32, C.c_int32, C.c_int64, C.POINTER(C.c_int32),
+                                          C.POINTER(C.c_int32), _D, C.POINTER(C.c_int64),
+                                          C.POINTER(C.c_int32), _D]
+        lib.ref_dd_probe.argtypes = [C.c_double] * 3 + [_D, _D]
+        lib.ref_read_mps.restype = C.c_void_p
+        lib.ref_read_mps.argtypes = [C.c_char_p]
+        lib.ref_model_view.argtypes = [C.c_void_p, _VP, C.POINTER(C.c_int)]
+        lib.ref_model_free.argtypes = [C.c_void_p]
+        _ref = lib
+    return _ref
+
+
+# ------------------------------------------------------------------ oracle
+
+def spmv(lp: LP, x):
+    y = np.zeros(lp.nrow)
+    oracle_lib().or_spmv(C.byref(lp.view()), _dptr(np.ascontiguousarray(x, float)), _dptr(y))
+    return y
+
+
+def spmv_t(lp: LP, y):
+    x = np.zeros(lp.ncol)
+    oracle_lib().or_spmv_t(C.byref(lp.view()), _dptr(np.ascontiguousarray(y, float)), _dptr(x))
+    return x
+
+
+def ref_pdhg_restated(lp: LP, max_iters: int, probe_every: int = 0, probe_tol: float = 1e-6,
+                      stop_at_probe: bool = False):
+    """The reference PDHG loop restated in C (bit-identical arithmetic)."""
+    x = np.zeros(lp.ncol)
+    y = np.zeros(lp.nrow)
+    out = PdhgOut()
+    oracle_lib().or_ref_pdhg(C.byref(lp.view()), max_iters, probe_every, probe_tol, int(stop_at_probe),
+                             _dptr(x), _dptr(y), C.byref(out))
+    return x, y, out
+
+
+def eval_objective(lp: LP, x) -> float:
+    return oracle_lib().or_eval_objective(C.byref(lp.view()), _dptr(np.ascontiguousarray(x, float)))
+
+
+def verify(lp: LP, x, claimed: float, tol: float = 1e-6) -> VerifyReport:
+    r = VerifyReport()
+    oracle_lib().or_verify(C.byref(lp.view()), _dptr(np.ascontiguousarray(x, float)), claimed, tol, C.byref(r))
+    return r
+
+
+def rel_kkt(lp: LP, x, y) -> Kkt:
+    k = Kkt()
+    oracle_lib().or_rel_kkt(C.byref(lp.view()), _dptr(np.ascontiguousarray(x, float)),
+                            _dptr(np.ascontiguousarray(y, float)), C.byref(k))
+    return k
+
+
+def csc_from_triplets(nrow, ncol, rows, cols, vals, use_ref=False):
+    rows = np.ascontiguousarray(rows, np.int32)
+    cols = np.ascontiguousarray(cols, np.int32)
+    vals = np.ascontiguousarray(vals, np.float64)
+    start = np.zeros(ncol + 1, np.int64)
+    idx = np.zeros(max(1, len(rows)), np.int32)
+    val = np.zeros(max(1, len(rows)), np.float64)
+    lib = ref_lib() if use_ref else oracle_lib()
+    fn = lib.ref_from_triplets if use_ref else lib.or_csc_from_triplets
+    nnz = fn(nrow, ncol, len(rows), rows.ctypes.data_as(C.POINTER(C.c_int32)),
+             cols.ctypes.data_as(C.POINTER(C.c_int32)), _dptr(vals), start.ctypes.data_as(C.POINTER(C.c_int64)),
+             idx.ctypes.data_as(C.POINTER(C.c_int32)), _dptr(val))
+    return start, idx[:nnz].copy(), val[:nnz].copy()
+
+
+# --------------------------------------------------------------- reference
+
+def ref_pdhg(lp: LP, threads: int = 1, simplex_iter_limit: int = 500000, time_limit: float = 1e30):
+    """sov::PdhgSolver::solve, the reference's own compiled code."""
+    lib = ref_lib()
+    x = np.zeros(lp.ncol)
+    y = np.zeros(lp.nrow)
+    st, it = C.c_int(), C.c_int()
+    obj = C.c_double()
+    if lib.ref_pdhg_solve(C.byref(lp.view()), threads, simplex_iter_limit, time_limit, _dptr(x), _dptr(y),
+                          C.byref(st), C.byref(obj), C.byref(it)) != 0:
+        raise RuntimeError(lib.ref_last_error().decode())
+    return x, y, st.value, obj.value, it.value
+
+
+def ref_solver(lp: LP, sense: int = 1, method: str = "auto", presolve: int = 2, scale: bool = True):
+    """sov::Solver::solve (validate, presolve, scale, engine, postsolve, dd check)."""
+    lib = ref_lib()
+    x = np.zeros(lp.ncol)
+    st, ver = C.c_int(), C.c_int()
+    obj = C.c_double()
+    if lib.ref_solver_solve(C.byref(lp.view()), sense, method.encode(), presolve, int(scale), _dptr(x),
+                            C.byref(st), C.byref(obj), C.byref(ver)) != 0:
+        raise RuntimeError(lib.ref_last_error().decode())
+    return x, st.value, obj.value, bool(ver.value)
+
+
+def ref_spmv(lp: LP, x):
+    y = np.zeros(lp.nrow)
+    ref_lib().ref_spmv(C.byref(lp.view()), _dptr(np.ascontiguousarray(x, float)), _dptr(y))
+    return y
+
+
+def ref_spmv_t(lp: LP, y):
+    x = np.zeros(lp.ncol)
+    ref_lib().ref_spmv_t(C.byref(lp.view()), _dptr(np.ascontiguousarray(y, float)), _dptr(x))
+    return x
+
+
+def ref_verify(lp: LP, x, claimed, tol=1e-6):
+    p = C.c_int()
+    vals = [C.c_double() for _ in range(4)]
+    ref_lib().ref_verify(C.byref(lp.view()), _dptr(np.ascontiguousarray(x, float)), claimed, tol, C.byref(p),
+                         *[C.byref(v) for v in vals])
+    return dict(passed=bool(p.value), max_bound_viol=vals[0].value, max_row_viol=vals[1].value,
+                computed_obj=vals[2].value, obj_rel_err=vals[3].value)
+
+
+def ref_dd_probe(a, b, c):
+    d, nsum = C.c_double(), C.c_double()
+    ref_lib().ref_dd_probe(a, b, c, C.byref(d), C.byref(nsum))
+    return d.value, nsum.value
+
+
+def ref_read_mps(path: str):
+    """MpsReader::read + to_internal_min; returns (LP, sense)."""
+    lib = ref_lib()
+    h = lib.ref_read_mps(path.encode())
+    if not h:
+        raise RuntimeError(lib.ref_last_error().decode())
+    try:
+        v = NirLpView()
+        sense = C.c_int()
+        lib.ref_model_view(h, C.byref(v), C.byref(sense))
+
+        def cp(p, n, dt):
+            return np.ctypeslib.as_array(p, shape=(n,)).astype(dt, copy=True) if n else np.zeros(0, dt)
+
+        lp = LP(v.nrow, v.ncol, cp(v.col_start, v.ncol + 1, np.int64), cp(v.row_index, v.nnz, np.int32),
+                cp(v.value, v.nnz, np.float64), cp(v.cost, v.ncol, np.float64), cp(v.collo, v.ncol, np.float64),
+                cp(v.colup, v.ncol, np.float64), cp(v.rowlo, v.nrow, np.float64), cp(v.rowup, v.nrow, np.float64),
+                v.obj_offset)
+        return lp, sense.value
+    finally:
+        lib.ref_model_free(h)

@@ -1,0 +1,205 @@
+// ref_shim.cpp -- C ABI over the reference's own code, compiled from the
+// reference's sources in place (oracle/Makefile, output oracle/_ref/).
+//
+// TEST INFRASTRUCTURE ONLY: the tests use it to pin the oracle and the CUDA
+// engine against the reference itself, and the benchmark's CPU-baseline leg
+// times sov::PdhgSolver::solve through it.  It holds no algorithm of its
+// own; every entry point forwards to a reference function:
+//   ref_pdhg_solve      sov::PdhgSolver::solve        src/gpu/pdhg_solver.hpp:25-107
+//   ref_solver_solve    sov::Solver::solve            include/sov/solver.hpp:128-326
+//   ref_verify          sov::verify_solution          src/io/sol_io.hpp:25-106
+//   ref_eval_objective  sov::Model::eval_objective    src/model/model.hpp:73-98
+//   ref_spmv(_t)        sov::CscMatrix::spmv(_transpose) src/core/csc_matrix.hpp:99-120
+//   ref_from_triplets   sov::CscMatrix::from_triplets src/core/csc_matrix.hpp:30-96
+//   ref_read_mps        sov::MpsReader::read          src/io/mps_reader.hpp:15-304
+//   ref_dd_probe        sov::dd_real / NeumaierSum    src/core/dd_real.hpp:27-104
+
+#include "include/sov/solver.hpp"
+
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "../include/nir_lp.h"
+
+namespace {
+
+thread_local std::string g_err;
+
+sov::Model to_model(const nir_lp_view* v) {
+    sov::Model m;
+    m.name = "shim";
+    m.sense = sov::Sense::Minimize;
+    m.obj_offset = v->obj_offset;
+    m.ncol = v->ncol;
+    m.nrow = v->nrow;
+    m.cost.assign(v->cost, v->cost + v->ncol);
+    m.collo.assign(v->collo, v->collo + v->ncol);
+    m.colup.assign(v->colup, v->colup + v->ncol);
+    m.vartype.assign(v->ncol, sov::VarType::Continuous);
+    m.rowlo.assign(v->rowlo, v->rowlo + v->nrow);
+    m.rowup.assign(v->rowup, v->rowup + v->nrow);
+    m.A = sov::CscMatrix(v->nrow, v->ncol);
+    m.A.start.assign(v->col_start, v->col_start + v->ncol + 1);
+    m.A.index.assign(v->row_index, v->row_index + v->nnz);
+    m.A.value.assign(v->value, v->value + v->nnz);
+    m.Q = sov::CscMatrix(v->ncol, v->ncol);
+    for (sov::Idx j = 0; j < v->ncol; ++j) m.col_names.push_back("C" + std::to_string(j));
+    for (sov::Idx i = 0; i < v->nrow; ++i) m.row_names.push_back("R" + std::to_string(i));
+    return m;
+}
+
+}  // namespace
+
+struct ref_model {
+    sov::Model m;
+    int sense = 1;
+};
+
+extern "C" {
+
+const char* ref_last_error(void) { return g_err.c_str(); }
+
+// PdhgSolver::solve on an already-internal (minimisation) LP.
+int ref_pdhg_solve(const nir_lp_view* v, int threads, int simplex_iter_limit, double time_limit,
+                   double* x_out, double* y_out, int* status, double* objective, int* iterations) {
+    try {
+        sov::Model m = to_model(v);
+        sov::Options opt;
+        opt.threads = threads;
+        opt.simplex_iter_limit = simplex_iter_limit;
+        opt.log_level = 0;
+        sov::Deadline dl;
+        dl.wall_limit_sec = time_limit;
+        sov::PdhgResult r = sov::PdhgSolver::solve(m, opt, dl);
+        if (x_out) std::memcpy(x_out, r.x.data(), sizeof(double) * r.x.size());
+        if (y_out) std::memcpy(y_out, r.y.data(), sizeof(double) * r.y.size());
+        *status = static_cast<int>(r.status);
+        *objective = r.objective;
+        *iterations = r.iterations;
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return 1;
+    }
+}
+
+// Solver::solve with a method ("auto" = dual simplex, "ipm", "pdhg") on a
+// model with the given sense; x_out gets the user-space solution.
+int ref_solver_solve(const nir_lp_view* v, int sense, const char* method, int presolve, int scale,
+                     double* x_out, int* status, double* objective, int* verified) {
+    try {
+        sov::Model m = to_model(v);
+        m.sense = sense < 0 ? sov::Sense::Maximize : sov::Sense::Minimize;
+        sov::Options opt;
+        opt.log_level = 0;
+        opt.method = method ? method : "auto";
+        opt.presolve = presolve;
+        opt.scale = scale != 0;
+        sov::Solver s(opt);
+        sov::SolveResult r = s.solve(m);
+        *status = static_cast<int>(r.status);
+        *objective = r.objective;
+        *verified = r.verification.passed ? 1 : 0;
+        if (x_out && r.x.size() == static_cast<size_t>(v->ncol))
+            std::memcpy(x_out, r.x.data(), sizeof(double) * r.x.size());
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return 1;
+    }
+}
+
+int ref_verify(const nir_lp_view* v, const double* x, double claimed, double tol, int* passed,
+               double* max_bound_viol, double* max_row_viol, double* computed_obj, double* obj_rel_err) {
+    sov::Model m = to_model(v);
+    std::vector<double> xv(x, x + v->ncol);
+    sov::VerificationReport r = sov::verify_solution(m, xv, claimed, tol);
+    *passed = r.passed ? 1 : 0;
+    *max_bound_viol = r.max_bound_viol;
+    *max_row_viol = r.max_row_viol;
+    *computed_obj = r.computed_obj;
+    *obj_rel_err = r.obj_rel_err;
+    return 0;
+}
+
+double ref_eval_objective(const nir_lp_view* v, const double* x) {
+    sov::Model m = to_model(v);
+    return m.eval_objective(std::vector<double>(x, x + v->ncol));
+}
+
+void ref_spmv(const nir_lp_view* v, const double* x, double* y) {
+    sov::Model m = to_model(v);
+    std::vector<double> yy;
+    m.A.spmv(std::vector<double>(x, x + v->ncol), yy);
+    std::memcpy(y, yy.data(), sizeof(double) * yy.size());
+}
+
+void ref_spmv_t(const nir_lp_view* v, const double* x, double* y) {
+    sov::Model m = to_model(v);
+    std::vector<double> yy;
+    m.A.spmv_transpose(std::vector<double>(x, x + v->nrow), yy);
+    std::memcpy(y, yy.data(), sizeof(double) * yy.size());
+}
+
+int64_t ref_from_triplets(int32_t nrow, int32_t ncol, int64_t ntrip, const int32_t* r, const int32_t* c,
+                          const double* val, int64_t* start, int32_t* index, double* value) {
+    std::vector<sov::Triplet> t(ntrip);
+    for (int64_t k = 0; k < ntrip; ++k) t[k] = {r[k], c[k], val[k]};
+    sov::CscMatrix A = sov::CscMatrix::from_triplets(nrow, ncol, t);
+    std::memcpy(start, A.start.data(), sizeof(int64_t) * A.start.size());
+    std::memcpy(index, A.index.data(), sizeof(int32_t) * A.index.size());
+    std::memcpy(value, A.value.data(), sizeof(double) * A.value.size());
+    return A.nnz();
+}
+
+void ref_dd_probe(double a, double b, double c, double* dd_out, double* neumaier_out) {
+    sov::dd_real acc(0.0);
+    acc += a;
+    acc += b;
+    acc += c;
+    *dd_out = acc.to_double();
+    sov::NeumaierSum s;
+    s.add(a);
+    s.add(b);
+    s.add(c);
+    *neumaier_out = s.result();
+}
+
+// MPS reader: returns a handle whose internal-minimisation LP is exposed
+// through ref_model_view (sense is +1 min / -1 max of the file).
+ref_model* ref_read_mps(const char* path) {
+    auto h = std::make_unique<ref_model>();
+    std::string err;
+    sov::Status st = sov::MpsReader::read(path, h->m, err);
+    if (st != sov::Status::Optimal) {
+        g_err = err;
+        return nullptr;
+    }
+    h->sense = (h->m.sense == sov::Sense::Maximize) ? -1 : 1;
+    h->m = h->m.to_internal_min();
+    return h.release();
+}
+
+int ref_model_view(const ref_model* h, nir_lp_view* v, int* sense) {
+    if (!h) return 1;
+    const sov::Model& m = h->m;
+    v->nrow = m.nrow;
+    v->ncol = m.ncol;
+    v->nnz = m.A.nnz();
+    v->col_start = m.A.start.data();
+    v->row_index = m.A.index.data();
+    v->value = m.A.value.data();
+    v->cost = m.cost.data();
+    v->collo = m.collo.data();
+    v->colup = m.colup.data();
+    v->rowlo = m.rowlo.data();
+    v->rowup = m.rowup.data();
+    v->obj_offset = m.obj_offset;
+    *sense = h->sense;
+    return 0;
+}
+
+void ref_model_free(ref_model* h) { delete h; }
+
+}  // extern "C"

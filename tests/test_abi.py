@@ -1,0 +1,73 @@
+"""The C-ABI libraries load and export every symbol their headers declare.
+
+CPU only: no compute call is made here, except nir_pdhg_create on a
+machine without a GPU, which must fail loudly (no CPU fallback).
+"""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from conftest import ROOT, has_gpu
+
+INCLUDE = os.path.join(ROOT, "include")
+
+
+def declared(header):
+    text = open(os.path.join(INCLUDE, header)).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(nir_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_engine_exports_every_declared_symbol():
+    path = os.path.join(ROOT, "nirnaya_b200", "libnir_pdhg.so")
+    if not os.path.exists(path):
+        pytest.skip("libnir_pdhg.so not built (run __graft_entry__.build())")
+    lib = C.CDLL(path)
+    names = declared("nir_pdhg.h")
+    assert len(names) >= 12
+    for name in names:
+        assert hasattr(lib, name), name
+    from nirnaya_b200 import pdhg
+
+    assert sorted(pdhg.EXPORTED) == sorted(n for n in names)
+
+
+def test_lpgen_exports_every_declared_symbol():
+    lib = C.CDLL(os.path.join(ROOT, "nirnaya_b200", "libnir_lpgen.so"))
+    for name in declared("nir_lpgen.h"):
+        assert hasattr(lib, name), name
+
+
+def test_structs_match_header_sizes():
+    from nirnaya_b200 import pdhg
+    from nirnaya_b200.lp import NirLpView
+
+    assert C.sizeof(NirLpView) == 4 + 4 + 8 + 8 * 8 + 8
+    # nir_pdhg_params: 2 int32, 2 double, int64, double, 3 int32, 5 double,
+    # double, 2 int32, double, 3 int32 (+pad), 2 pointers, double
+    assert C.sizeof(pdhg.Params) == 160
+    assert C.sizeof(pdhg.Info) == 4 + 4 + 8 + 8 + 8 * 11 + 4 + 4
+
+
+@pytest.mark.skipif(has_gpu(), reason="checks the no-GPU failure mode")
+def test_create_without_gpu_fails_loudly():
+    from nirnaya_b200 import lp as L
+    from nirnaya_b200 import pdhg
+
+    if not os.path.exists(pdhg.LIB_PATH):
+        pytest.skip("libnir_pdhg.so not built")
+    lp = L.generate(L.RANDOM_EQ, 1, m=20, n=50)
+    with pytest.raises(RuntimeError, match="CUDA|device"):
+        pdhg.Engine(lp)
+
+
+def test_params_defaults_roundtrip():
+    from nirnaya_b200 import pdhg
+
+    if not os.path.exists(pdhg.LIB_PATH):
+        pytest.skip("libnir_pdhg.so not built")
+    p = pdhg.default_params()
+    assert p.algorithm == pdhg.ALGO_PDLP and p.precision == pdhg.PREC_MIXED and p.tol == 1e-6
+    assert p.check_every == 64 and p.reflection == 1.0 and p.use_graphs == 1
