@@ -295,9 +295,19 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--max-iters", type=int, default=1000000)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--ncu-case", action="store_true",
+                    help="one short solve (2 checks) of the workload for an ncu capture, then exit")
     args = ap.parse_args()
-    rank, world, local = dist_setup(args.gpus)
     wl = WORKLOADS[args.workload]
+    if args.ncu_case:
+        from nirnaya_b200 import lp as L
+        from nirnaya_b200 import pdhg
+
+        lp = L.generate(wl["kind"], wl["seed"], **wl["kw"])
+        with pdhg.Engine(lp, 0) as eng:
+            eng.solve(pdhg.default_params(precision=wl["precision"], max_iters=128, tol=0.0))
+        return
+    rank, world, local = dist_setup(args.gpus)
 
     if args.impl == "reference":
         if rank != 0:

@@ -85,9 +85,9 @@ typedef struct nir_pdhg_params {
     double step_factor;           /* eta = step_factor / ||A||_2 estimate        (0.998) */
     int32_t power_iters;          /* power-iteration rounds for ||A||_2          (64)    */
     int32_t polish_stall_checks;  /* MIXED: FP64 polish after this many checks
-                                     without a 0.8x improvement of the best KKT   (6)    */
+                                     without a 0.8x improvement of the best KKT   (40)   */
     double polish_switch_kkt;     /* MIXED: ... or as soon as KKT <= this        (0)     */
-    int32_t spmv_block_nnz;       /* nonzeros per CSR-adaptive row block; 0=auto (0)     */
+    int32_t spmv_block_nnz;       /* nonzeros per warp row block, 1..256; 0 = auto (0)   */
     int32_t use_graphs;           /* capture launch chunks in CUDA graphs        (1)     */
     int32_t verbose;              /* 1 = one line per check on stderr            (0)     */
     const double* x_init;         /* warm start in original space, ncol, or NULL          */
@@ -167,6 +167,12 @@ typedef struct nir_pdhg_kernel_time {
  * nir_pdhg_set_profiling before the solve). */
 int nir_pdhg_set_profiling(nir_pdhg* h, int on);
 int nir_pdhg_kernel_times(nir_pdhg* h, nir_pdhg_kernel_time* out);
+
+/* KKT history of the last PDHG/PDLP solve, one entry per check, oldest
+ * first: 8 doubles per entry (iteration, rel KKT, rel primal, rel dual,
+ * rel gap, fixed-point residual, primal weight, phase).  Returns the number
+ * of entries written (at most max_entries and the last 4096 checks). */
+int nir_pdhg_history(nir_pdhg* h, double* out, int max_entries);
 
 /* Matrix and layout facts: nnz, rows, row blocks of each orientation. */
 typedef struct nir_pdhg_layout {

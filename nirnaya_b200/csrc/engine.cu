@@ -110,7 +110,7 @@ struct Orient {
     std::vector<int> h_rp;
     int cap = 0;
     int nblk = 0;
-    int* blk = nullptr;
+    int2* blk = nullptr;  // (first row, first nonzero) of each row block, plus an end entry
 };
 
 struct Snapshot {
@@ -121,7 +121,8 @@ struct Snapshot {
 struct ChunkGraph {
     cudaGraph_t g = nullptr;
     cudaGraphExec_t ge = nullptr;
-    int key = -1;
+    unsigned long long key = 0;
+    bool valid = false;
 };
 
 struct nir_pdhg {
@@ -155,9 +156,26 @@ struct nir_pdhg {
     std::vector<DevBuf> bufs;
     long long device_bytes = 0;
     ChunkGraph graphs[3];
+    long long last_iters = 0;
+    int sms = 148;
+    struct Occ {
+        const void* fn;
+        size_t smem;
+        int per_sm;
+    };
+    std::vector<Occ> occ;
     bool profiling = false;
     nir_pdhg_kernel_time ktime{};
     int launches = 0;
+
+    // zero-filled allocation with `pad` spare elements past the end (the
+    // row-block copies read 16-byte windows that may reach past the end)
+    template <typename T>
+    T* allocz(size_t count, size_t pad = 8) {
+        T* p = alloc<T>(count + pad);
+        NIR_CUDA(cudaMemsetAsync(p, 0, (count + pad) * sizeof(T), stream));
+        return p;
+    }
 
     template <typename T>
     T* alloc(size_t count) {
@@ -194,19 +212,24 @@ void d2h(nir_pdhg* h, void* dst, const void* src, size_t bytes) {
     NIR_CUDA(cudaStreamSynchronize(h->stream));
 }
 
-// CSR-adaptive row blocks: consecutive rows packed while their nonzeros
-// fit in `cap`; a longer row gets a block of its own.
-std::vector<int> build_row_blocks(const std::vector<int>& rp, int cap) {
-    std::vector<int> blk{0};
+// Warp row blocks: consecutive rows packed while their nonzeros fit in
+// `cap` (<= 256) and there are at most 32 of them; a longer row gets a
+// block of its own.  Returns the (first row, first nonzero) descriptors,
+// one per block plus the end (rows, nnz).
+std::vector<int2> build_row_blocks(const std::vector<int>& rp, int cap) {
     const int rows = int(rp.size()) - 1;
-    if (rows <= 0) return {0, 0};
+    std::vector<int2> blk{make_int2(0, 0)};
+    if (rows <= 0) {
+        blk.push_back(make_int2(0, 0));
+        return blk;
+    }
     int s = 0;
     while (s < rows) {
         int r = s + 1;
         if (rp[s + 1] - rp[s] <= cap) {
-            while (r < rows && rp[r + 1] - rp[s] <= cap && r - s < cap) ++r;
+            while (r < rows && rp[r + 1] - rp[s] <= cap && r - s < nir::kRowsPerWarpBlock) ++r;
         }
-        blk.push_back(r);
+        blk.push_back(make_int2(r, rp[r]));
         s = r;
     }
     return blk;
@@ -214,17 +237,25 @@ std::vector<int> build_row_blocks(const std::vector<int>& rp, int cap) {
 
 void set_blocks(nir_pdhg* h, Orient& o, int cap) {
     if (o.cap == cap && o.blk) return;
-    std::vector<int> b = build_row_blocks(o.h_rp, cap);
+    std::vector<int2> b = build_row_blocks(o.h_rp, cap);
     o.nblk = int(b.size()) - 1;
-    o.blk = h->alloc<int>(b.size());
-    h2d(h, o.blk, b.data(), b.size() * sizeof(int));
+    o.blk = h->alloc<int2>(b.size());
+    h2d(h, o.blk, b.data(), b.size() * sizeof(int2));
     o.cap = cap;
 }
 
+// Warp row-block capacity: 256 nonzeros (8 per lane) when the matrix gives
+// every SM many warps, smaller for small matrices so that the grid still
+// covers the GPU.
 int auto_cap(long long nnz, int rows) {
     (void)rows;
-    (void)nnz;
-    return 2048;
+    int sms = 148;
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    long long per = nnz / (long long)(32 * std::max(sms, 1));
+    int cap = 32;
+    while (cap < nir::kWarpCapMax && cap * 2 <= per) cap *= 2;
+    return cap;
 }
 
 void validate_lp(const nir_lp_view* lp) {
@@ -289,6 +320,7 @@ void create_impl(nir_pdhg* h, const nir_lp_view* lp, int device) {
     h->device = device;
     NIR_CUDA(cudaSetDevice(device));
     NIR_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    NIR_CUDA(cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, device));
     const int m = lp->nrow, n = lp->ncol;
     const long long nnz = lp->nnz;
     h->m = m;
@@ -302,11 +334,11 @@ void create_impl(nir_pdhg* h, const nir_lp_view* lp, int device) {
     T.rows = n;
     T.cols = m;
     T.nnz = nnz;
-    T.rp = h->alloc<int>(n + 1);
-    T.ci = h->alloc<int>(nnz);
-    T.v_orig = h->alloc<double>(nnz);
-    T.v64 = h->alloc<double>(nnz);
-    T.v32 = h->alloc<float>(nnz);
+    T.rp = h->allocz<int>(n + 1);
+    T.ci = h->allocz<int>(nnz);
+    T.v_orig = h->allocz<double>(nnz);
+    T.v64 = h->allocz<double>(nnz);
+    T.v32 = h->allocz<float>(nnz);
     long long* d_start = h->alloc<long long>(n + 1);
     NIR_CUDA(cudaMemcpyAsync(d_start, lp->col_start, (n + 1) * sizeof(long long), cudaMemcpyHostToDevice, s));
     NIR_CUDA(cudaMemcpyAsync(T.ci, lp->row_index, nnz * sizeof(int), cudaMemcpyHostToDevice, s));
@@ -322,11 +354,11 @@ void create_impl(nir_pdhg* h, const nir_lp_view* lp, int device) {
     R.rows = m;
     R.cols = n;
     R.nnz = nnz;
-    R.rp = h->alloc<int>(m + 1);
-    R.ci = h->alloc<int>(nnz);
-    R.v_orig = h->alloc<double>(nnz);
-    R.v64 = h->alloc<double>(nnz);
-    R.v32 = h->alloc<float>(nnz);
+    R.rp = h->allocz<int>(m + 1);
+    R.ci = h->allocz<int>(nnz);
+    R.v_orig = h->allocz<double>(nnz);
+    R.v64 = h->allocz<double>(nnz);
+    R.v32 = h->allocz<float>(nnz);
     {
         int* col_of = h->alloc<int>(nnz);
         int* ids = h->alloc<int>(nnz);
@@ -409,11 +441,35 @@ void create_impl(nir_pdhg* h, const nir_lp_view* lp, int device) {
     NIR_CUDA(cudaStreamSynchronize(s));
 }
 
+// Launch shape of a row-block kernel: one warp per warp row block.
+struct LaunchCfg {
+    int grid;
+    size_t smem;
+};
+
+// Persistent grid: as many CTAs as are resident at once (occupancy), at most
+// one warp per warp row block.  The occupancy query runs once per kernel
+// (outside any stream capture: warm_cfgs is called before capturing).
+template <typename TA, typename K>
+LaunchCfg warp_cfg(nir_pdhg* h, K* kernel, int nblk) {
+    const size_t smem = size_t(nir::warp_smem_bytes<TA>());
+    int per = 0;
+    for (auto& e : h->occ)
+        if (e.fn == (const void*)kernel && e.smem == smem) per = e.per_sm;
+    if (per == 0) {
+        NIR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, nir::kBlock, smem));
+        per = std::max(per, 1);
+        h->occ.push_back({(const void*)kernel, smem, per});
+    }
+    const int need = std::max(1, (nblk + nir::kWarps - 1) / nir::kWarps);
+    return {std::min(need, per * h->sms), smem};
+}
+
+int max_grid(const nir_pdhg* h) { return 8 * h->sms; }  // 2048 threads per SM / kBlock
+
 // Partial-sum area large enough for any kernel of this handle.
 void ensure_partials(nir_pdhg* h) {
-    size_t need = 4 * size_t(std::max(h->A.nblk, 1)) + 4 * size_t(std::max(h->At.nblk, 1)) +
-                  2 * size_t(std::max(h->A.nblk, 1)) + 2 * size_t(std::max(h->At.nblk, 1)) +
-                  size_t(grid_for(std::max(h->m, h->n))) + 16;
+    size_t need = 12 * size_t(max_grid(h)) + size_t(grid_for(std::max(h->m, h->n))) + 16;
     if (h->part && h->part_len >= need) return;
     h->part = h->alloc<double>(need);
     h->part_len = need;
@@ -424,12 +480,13 @@ struct PartLayout {
 };
 
 PartLayout part_layout(nir_pdhg* h) {
+    const int G = max_grid(h);
     PartLayout L;
     L.P = h->part;
-    L.D = L.P + 2 * std::max(h->At.nblk, 1);
-    L.KR = L.D + 2 * std::max(h->A.nblk, 1);
-    L.KC = L.KR + 4 * std::max(h->A.nblk, 1);
-    L.misc = L.KC + 4 * std::max(h->At.nblk, 1);
+    L.D = L.P + 2 * G;
+    L.KR = L.D + 2 * G;
+    L.KC = L.KR + 4 * G;
+    L.misc = L.KC + 4 * G;
     return L;
 }
 
@@ -495,49 +552,59 @@ void launch_fast_chunk(nir_pdhg* h, const SolveCfg& cfg, int phase, ChunkTimer* 
     cudaStream_t s = h->stream;
     const PartLayout L = part_layout(h);
     const int K = cfg.K;
-    const size_t smem = size_t(h->A.cap) * sizeof(T);
-    const size_t smem64 = size_t(h->A.cap) * sizeof(double);
+    const int cap = h->A.cap;
+    const LaunchCfg cp1 = warp_cfg<T>(h, nir::k_primal<T, true>, h->At.nblk);
+    const LaunchCfg cp0 = warp_cfg<T>(h, nir::k_primal<T, false>, h->At.nblk);
+    const LaunchCfg cd1 = warp_cfg<T>(h, nir::k_dual<T, true>, h->A.nblk);
+    const LaunchCfg cd0 = warp_cfg<T>(h, nir::k_dual<T, false>, h->A.nblk);
+    const LaunchCfg ckr = warp_cfg<double>(h, nir::k_kkt_rows<T>, h->A.nblk);
+    const LaunchCfg ckc = warp_cfg<double>(h, nir::k_kkt_cols<T>, h->At.nblk);
+    const size_t smem = cp1.smem, smem64 = ckr.smem;
     for (int i = 0; i < K; ++i) {
         const bool check = (i == K - 1);
-        nir::IterArgs ap{h->At.blk, h->At.rp, h->At.ci, L.P, h->st, i, cfg.halpern, phase, cfg.p.reflection};
-        nir::IterArgs ad{h->A.blk, h->A.rp, h->A.ci, L.D, h->st, i, cfg.halpern, phase, cfg.p.reflection};
+        nir::IterArgs ap{h->At.blk, h->At.nblk, cap, h->At.rp, h->At.ci, L.P, h->st, i, cfg.halpern, phase,
+                         cfg.p.reflection};
+        nir::IterArgs ad{h->A.blk, h->A.nblk, cap, h->A.rp, h->A.ci, L.D, h->st, i, cfg.halpern, phase,
+                         cfg.p.reflection};
         const bool timed = tm && tm->armed && i == 0;
         if (timed) NIR_CUDA(cudaEventRecord(tm->e[0], s));
         if (check)
-            nir::k_primal<T, true><<<h->At.nblk, nir::kBlock, smem, s>>>(
+            nir::k_primal<T, true><<<cp1.grid, nir::kBlock, smem, s>>>(
                 ap, View<T>::valAt(h), View<T>::y(h), View<T>::x(h), View<T>::xb(h), View<T>::xp(h), View<T>::c(h),
                 View<T>::l(h), View<T>::u(h), View<T>::x0(h));
         else
-            nir::k_primal<T, false><<<h->At.nblk, nir::kBlock, smem, s>>>(
+            nir::k_primal<T, false><<<cp0.grid, nir::kBlock, smem, s>>>(
                 ap, View<T>::valAt(h), View<T>::y(h), View<T>::x(h), View<T>::xb(h), View<T>::xp(h), View<T>::c(h),
                 View<T>::l(h), View<T>::u(h), View<T>::x0(h));
         NIR_LAUNCHED();
         if (timed) NIR_CUDA(cudaEventRecord(tm->e[1], s));
         if (check)
-            nir::k_dual<T, true><<<h->A.nblk, nir::kBlock, smem, s>>>(ad, View<T>::valA(h), View<T>::xb(h), View<T>::y(h),
+            nir::k_dual<T, true><<<cd1.grid, nir::kBlock, smem, s>>>(ad, View<T>::valA(h), View<T>::xb(h), View<T>::y(h),
+                                                                      View<T>::yp(h), View<T>::rl(h), View<T>::ru(h),
+                                                                      View<T>::y0(h));
+        else
+            nir::k_dual<T, false><<<cd0.grid, nir::kBlock, smem, s>>>(ad, View<T>::valA(h), View<T>::xb(h), View<T>::y(h),
                                                                        View<T>::yp(h), View<T>::rl(h), View<T>::ru(h),
                                                                        View<T>::y0(h));
-        else
-            nir::k_dual<T, false><<<h->A.nblk, nir::kBlock, smem, s>>>(ad, View<T>::valA(h), View<T>::xb(h), View<T>::y(h),
-                                                                        View<T>::yp(h), View<T>::rl(h), View<T>::ru(h),
-                                                                        View<T>::y0(h));
         NIR_LAUNCHED();
         if (timed) NIR_CUDA(cudaEventRecord(tm->e[2], s));
         h->launches += 2;
     }
-    nir::KktArgs kr{h->A.blk, h->A.rp, h->A.ci, h->A.v64, L.KR, h->st, phase};
-    nir::k_kkt_rows<T><<<h->A.nblk, nir::kBlock, smem64, s>>>(kr, View<T>::xp(h), View<T>::yp(h), h->dr, h->rl, h->ru);
+    nir::KktArgs kr{h->A.blk, h->A.nblk, cap, h->A.rp, h->A.ci, h->A.v64, L.KR, h->st, phase};
+    nir::k_kkt_rows<T><<<ckr.grid, nir::kBlock, smem64, s>>>(kr, View<T>::xp(h), View<T>::yp(h), h->dr, h->rl, h->ru);
     NIR_LAUNCHED();
-    nir::KktArgs kc{h->At.blk, h->At.rp, h->At.ci, h->At.v64, L.KC, h->st, phase};
-    nir::k_kkt_cols<T><<<h->At.nblk, nir::kBlock, smem64, s>>>(kc, View<T>::xp(h), View<T>::yp(h), h->dc, h->c, h->l, h->u);
+    nir::KktArgs kc{h->At.blk, h->At.nblk, cap, h->At.rp, h->At.ci, h->At.v64, L.KC, h->st, phase};
+    nir::k_kkt_cols<T><<<ckc.grid, nir::kBlock, smem64, s>>>(kc, View<T>::xp(h), View<T>::yp(h), h->dc, h->c, h->l, h->u);
     NIR_LAUNCHED();
     nir::CtlArgs ca;
     ca.partP = L.P;
     ca.partD = L.D;
     ca.partKR = L.KR;
     ca.partKC = L.KC;
-    ca.nP = h->At.nblk;
-    ca.nD = h->A.nblk;
+    ca.nP = cp1.grid;
+    ca.nD = cd1.grid;
+    ca.nKR = ckr.grid;
+    ca.nKC = ckc.grid;
     ca.bnorm = cfg.bnorm;
     ca.cnorm = cfg.cnorm;
     ca.offset = h->offset;
@@ -567,6 +634,41 @@ void launch_fast_chunk(nir_pdhg* h, const SolveCfg& cfg, int phase, ChunkTimer* 
     h->launches += 5;
 }
 
+// Runs the occupancy queries of a chunk's kernels before any capture.
+template <typename T>
+void warm_cfgs(nir_pdhg* h) {
+    warp_cfg<T>(h, nir::k_primal<T, true>, h->At.nblk);
+    warp_cfg<T>(h, nir::k_primal<T, false>, h->At.nblk);
+    warp_cfg<T>(h, nir::k_dual<T, true>, h->A.nblk);
+    warp_cfg<T>(h, nir::k_dual<T, false>, h->A.nblk);
+    warp_cfg<double>(h, nir::k_kkt_rows<T>, h->A.nblk);
+    warp_cfg<double>(h, nir::k_kkt_cols<T>, h->At.nblk);
+}
+
+// Identity of everything a captured chunk bakes into its kernel arguments
+// (FNV-1a over the values), so a graph is only replayed for the same ones.
+struct KeyHash {
+    unsigned long long h = 1469598103934665603ULL;
+    template <typename V>
+    KeyHash& add(const V& v) {
+        const unsigned char* p = reinterpret_cast<const unsigned char*>(&v);
+        for (size_t i = 0; i < sizeof(V); ++i) {
+            h ^= p[i];
+            h *= 1099511628211ULL;
+        }
+        return *this;
+    }
+};
+
+unsigned long long chunk_key(const nir_pdhg* h, const SolveCfg& c, int phase, bool f64) {
+    KeyHash k;
+    k.add(phase).add(f64).add(c.K).add(c.halpern).add(c.restarts).add(c.mixed).add(c.bnorm).add(c.cnorm);
+    k.add(c.p.reflection).add(c.p.restart_sufficient).add(c.p.restart_necessary).add(c.p.restart_artificial);
+    k.add(c.p.primal_weight_smoothing).add(c.p.polish_stall_checks).add(c.p.polish_switch_kkt).add(c.p.tol);
+    k.add(c.p.feas_tol).add(h->offset).add(h->A.cap).add(h->A.blk).add(h->At.blk).add(h->part).add(h->hist);
+    return k.h;
+}
+
 void launch_ref_chunk(nir_pdhg* h, int K) {
     cudaStream_t s = h->stream;
     const PartLayout L = part_layout(h);
@@ -589,9 +691,9 @@ void launch_ref_chunk(nir_pdhg* h, int K) {
 
 // Captures (once) and returns the graph for a chunk kind.
 template <class F>
-cudaGraphExec_t chunk_graph(nir_pdhg* h, int slot, int key, F&& launch) {
+cudaGraphExec_t chunk_graph(nir_pdhg* h, int slot, unsigned long long key, F&& launch) {
     ChunkGraph& g = h->graphs[slot];
-    if (g.ge && g.key == key) return g.ge;
+    if (g.ge && g.valid && g.key == key) return g.ge;
     if (g.ge) {
         cudaGraphExecDestroy(g.ge);
         g.ge = nullptr;
@@ -614,6 +716,7 @@ cudaGraphExec_t chunk_graph(nir_pdhg* h, int slot, int key, F&& launch) {
     NIR_CUDA(cudaStreamEndCapture(h->stream, &g.g));
     NIR_CUDA(cudaGraphInstantiate(&g.ge, g.g, 0));
     g.key = key;
+    g.valid = true;
     return g.ge;
 }
 
@@ -861,10 +964,12 @@ int solve_fast(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), void* 
     const int n = h->n, m = h->m;
     const bool pdlp = p.algorithm == NIR_ALGO_PDLP;
     const int cap = p.spmv_block_nnz > 0 ? p.spmv_block_nnz : auto_cap(h->nnz, std::max(m, n));
-    if (cap < 32 || cap > 4096) throw std::invalid_argument("spmv_block_nnz must be in [32, 4096]");
+    if (cap < 1 || cap > nir::kWarpCapMax) throw std::invalid_argument("spmv_block_nnz must be in [1, 256]");
     set_blocks(h, h->A, cap);
     set_blocks(h, h->At, cap);
     ensure_partials(h);
+    warm_cfgs<float>(h);
+    warm_cfgs<double>(h);
     SolveCfg cfg;
     cfg.p = p;
     cfg.K = std::max(1, p.check_every);
@@ -875,6 +980,7 @@ int solve_fast(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), void* 
     cfg.cnorm = norm2(h->h_c);
     h->ktime = nir_pdhg_kernel_time{};
 
+    NIR_CUDA(cudaMemsetAsync(h->hist, 0, sizeof(double) * 8 * nir::kHist, s));
     precondition(h, p, pdlp && (p.ruiz_iters > 0 || p.pock_chambolle));
     nir::DevState st0{};
     st0.max_iters = p.max_iters;
@@ -969,8 +1075,7 @@ int solve_fast(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), void* 
             };
             const int per = launches_per_chunk(cfg.K, false);
             if (p.use_graphs && !h->profiling) {
-                const int key = (f64 ? 1 : 0) + 2 * phase + 4 * cfg.K + 100000 * (cap + 1) + 1000000000 * (pdlp ? 1 : 0);
-                cudaGraphExec_t ge = chunk_graph(h, 1 + phase, key, launch);
+                cudaGraphExec_t ge = chunk_graph(h, 1 + phase, chunk_key(h, cfg, phase, f64), launch);
                 return run_chunks(h, p, poll, ctx, t0, phase, per, [&]() { NIR_CUDA(cudaGraphLaunch(ge, s)); }, nullptr);
             }
             return run_chunks(h, p, poll, ctx, t0, phase, 0, launch, h->profiling ? &tm : nullptr);
@@ -1028,6 +1133,7 @@ int solve_fast(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), void* 
     fill_info_common(h, st, info);
     info->status = status;
     info->iterations = st.iter;
+    h->last_iters = st.iter;
     if (fp64_first) info->iterations_fp64 = st.iter;
     info->objective = host_objective(h, x);
     info->setup_seconds = t_setup - t0;
@@ -1061,7 +1167,7 @@ int nir_pdhg_default_params(nir_pdhg_params* p) {
     p->primal_weight_smoothing = 0.5;
     p->step_factor = 0.998;
     p->power_iters = 64;
-    p->polish_stall_checks = 6;
+    p->polish_stall_checks = 40;
     p->polish_switch_kkt = 0.0;
     p->spmv_block_nnz = 0;
     p->use_graphs = 1;
@@ -1196,19 +1302,21 @@ int nir_pdhg_spmv(nir_pdhg* h, int transpose, int kernel, const double* x, doubl
         } else {
             if (!o.blk) set_blocks(h, o, auto_cap(h->nnz, nout));
             if (kernel == 1) {
-                nir::k_spmv_adaptive<double, double, double><<<o.nblk, nir::kBlock, o.cap * sizeof(double), s>>>(
-                    o.blk, o.rp, o.ci, o.v_orig, din, dout);
+                const LaunchCfg lc = warp_cfg<double>(h, nir::k_spmv_adaptive<double, double, double>, o.nblk);
+                nir::k_spmv_adaptive<double, double, double><<<lc.grid, nir::kBlock, lc.smem, s>>>(
+                    o.blk, o.nblk, o.cap, o.rp, o.ci, o.v_orig, din, dout);
                 NIR_LAUNCHED();
             } else {
                 if (!o.v32_orig) {
-                    o.v32_orig = h->alloc<float>(o.nnz);
+                    o.v32_orig = h->allocz<float>(o.nnz);
                     nir::k_to_float<<<grid_for(o.nnz), nir::kBlock, 0, s>>>(o.nnz, o.v_orig, o.v32_orig);
                 }
                 float* fin = transpose ? h->tmp_m32 : h->tmp_n32;
                 float* fout = transpose ? h->tmp_n32 : h->tmp_m32;
                 nir::k_to_float<<<std::max(grid_for(nin), 1u), nir::kBlock, 0, s>>>(nin, din, fin);
-                nir::k_spmv_adaptive<float, float, float><<<o.nblk, nir::kBlock, o.cap * sizeof(float), s>>>(
-                    o.blk, o.rp, o.ci, o.v32_orig, fin, fout);
+                const LaunchCfg lc = warp_cfg<float>(h, nir::k_spmv_adaptive<float, float, float>, o.nblk);
+                nir::k_spmv_adaptive<float, float, float><<<lc.grid, nir::kBlock, lc.smem, s>>>(
+                    o.blk, o.nblk, o.cap, o.rp, o.ci, o.v32_orig, fin, fout);
                 nir::k_to_double<<<std::max(grid_for(nout), 1u), nir::kBlock, 0, s>>>(nout, fout, dout);
                 NIR_LAUNCHED();
             }
@@ -1234,7 +1342,7 @@ int nir_pdhg_time_spmv(nir_pdhg* h, int transpose, int kernel, int reps, int flu
         const int nin = o.cols, nout = o.rows;
         if (!o.blk) set_blocks(h, o, auto_cap(h->nnz, nout));
         if (kernel == 2 && !o.v32_orig) {
-            o.v32_orig = h->alloc<float>(o.nnz);
+            o.v32_orig = h->allocz<float>(o.nnz);
             nir::k_to_float<<<grid_for(o.nnz), nir::kBlock, 0, s>>>(o.nnz, o.v_orig, o.v32_orig);
         }
         double* din = transpose ? h->tmp_m : h->tmp_n;
@@ -1247,6 +1355,8 @@ int nir_pdhg_time_spmv(nir_pdhg* h, int transpose, int kernel, int reps, int flu
             h->flush_bytes = size_t(512) << 20;
             h->flush = h->alloc<unsigned char>(h->flush_bytes);
         }
+        const LaunchCfg l64 = warp_cfg<double>(h, nir::k_spmv_adaptive<double, double, double>, o.nblk);
+        const LaunchCfg l32 = warp_cfg<float>(h, nir::k_spmv_adaptive<float, float, float>, o.nblk);
         cudaEvent_t a, b;
         NIR_CUDA(cudaEventCreate(&a));
         NIR_CUDA(cudaEventCreate(&b));
@@ -1257,11 +1367,11 @@ int nir_pdhg_time_spmv(nir_pdhg* h, int transpose, int kernel, int reps, int flu
             if (kernel == 0)
                 nir::k_ref_spmv<<<std::max(grid_for(nout), 1u), nir::kBlock, 0, s>>>(nout, o.rp, o.ci, o.v_orig, din, dout);
             else if (kernel == 1)
-                nir::k_spmv_adaptive<double, double, double><<<o.nblk, nir::kBlock, o.cap * sizeof(double), s>>>(
-                    o.blk, o.rp, o.ci, o.v_orig, din, dout);
+                nir::k_spmv_adaptive<double, double, double><<<l64.grid, nir::kBlock, l64.smem, s>>>(
+                    o.blk, o.nblk, o.cap, o.rp, o.ci, o.v_orig, din, dout);
             else
-                nir::k_spmv_adaptive<float, float, float><<<o.nblk, nir::kBlock, o.cap * sizeof(float), s>>>(
-                    o.blk, o.rp, o.ci, o.v32_orig, fin, fout);
+                nir::k_spmv_adaptive<float, float, float><<<l32.grid, nir::kBlock, l32.smem, s>>>(
+                    o.blk, o.nblk, o.cap, o.rp, o.ci, o.v32_orig, fin, fout);
             NIR_LAUNCHED();
             NIR_CUDA(cudaEventRecord(b, s));
             NIR_CUDA(cudaEventSynchronize(b));
@@ -1294,6 +1404,30 @@ int nir_pdhg_kernel_times(nir_pdhg* h, nir_pdhg_kernel_time* out) {
         out->iter_us /= double(out->samples);
     }
     return 0;
+}
+
+int nir_pdhg_history(nir_pdhg* h, double* out, int max_entries) {
+    if (!h || !out || max_entries < 0) return -1;
+    try {
+        NIR_CUDA(cudaSetDevice(h->device));
+        std::vector<double> ring(8 * nir::kHist);
+        d2h(h, ring.data(), h->hist, ring.size() * sizeof(double));
+        // entries carry their iteration count; keep those of the last solve
+        std::vector<int> idx;
+        for (int i = 0; i < nir::kHist; ++i)
+            if (ring[8 * i] > 0.0 && ring[8 * i] <= double(h->last_iters)) idx.push_back(i);
+        std::sort(idx.begin(), idx.end(), [&](int a, int b) { return ring[8 * a] < ring[8 * b]; });
+        int cnt = 0;
+        for (int i : idx) {
+            if (cnt >= max_entries) break;
+            std::memcpy(out + 8 * cnt, &ring[8 * i], 8 * sizeof(double));
+            ++cnt;
+        }
+        return cnt;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    }
 }
 
 int nir_pdhg_get_layout(nir_pdhg* h, nir_pdhg_layout* out) {

@@ -2,13 +2,16 @@
 // fused into its epilogue.
 //
 // A matrix orientation (A, or the stored transpose A') is cut into row
-// blocks holding at most `cap` nonzeros (one row per block if the row is
-// longer).  One CUDA block of kBlock threads takes one row block:
-//  * several rows: the block streams the row block's index/value pairs
-//    with consecutive threads on consecutive nonzeros (coalesced), forms the
-//    products val*x[col] into shared memory, then teams of T threads (T a
-//    power of two <= 32 chosen from the row count) reduce one row each by a
-//    fixed shuffle tree and the team leader runs the epilogue for that row;
+// blocks holding at most `cap` nonzeros and at most kBlock rows (a row
+// longer than `cap` gets a block of its own).  Block b is described by
+// blk[b] = (first row, first nonzero), so one 8-byte load gives a CUDA block
+// its whole range.  One CUDA block of kBlock threads takes one row block:
+//  * several rows: consecutive threads stream consecutive nonzeros
+//    (coalesced, 8 loads in flight per thread), form val*x[col] into shared
+//    memory while the row pointers of the block are staged next to them and
+//    every row's epilogue operands are already being fetched; after one
+//    barrier, a team of T threads (T a power of two <= 32) reduces each row
+//    by a fixed shuffle tree and its leader runs the epilogue;
 //  * one long row: all threads stride over it and a block tree reduces.
 // The reduction order depends only on the layout, so results are
 // deterministic run to run, and no atomics are used.  Each epilogue reads
@@ -27,64 +30,147 @@ namespace nir {
 
 // ---------------------------------------------------------------- core
 
+constexpr int kWarpU = 8;                    // nonzeros per lane per round
+constexpr int kWarpCapMax = 32 * kWarpU;     // largest warp row block (256)
+constexpr int kRowsPerWarpBlock = 32;        // rows in one warp row block
+
+// Dynamic shared memory of an iteration kernel: one product slice per warp.
+template <typename TA>
+__host__ __device__ constexpr int warp_smem_bytes() {
+    return kWarps * kWarpCapMax * int(sizeof(TA));
+}
+
+// Loads the index/value stream of a packed warp row block into registers
+// (lane l gets nonzeros l, l+32, ...).  Long rows are not preloaded.
+template <typename TV>
+__device__ __forceinline__ void stream_load(int2 d0, int2 d1, int cap, const int* __restrict__ ci,
+                                            const TV* __restrict__ val, int (&c)[kWarpU], TV (&v)[kWarpU]) {
+    const int lane = threadIdx.x & 31;
+    const int p0 = d0.y, nnzb = d1.y - d0.y;
+    const bool packed = nnzb <= cap;
+#pragma unroll
+    for (int q = 0; q < kWarpU; ++q) {
+        const int k = lane + 32 * q;
+        const bool ok = packed && k < nnzb;
+        c[q] = ok ? __ldg(ci + p0 + k) : 0;
+        v[q] = ok ? __ldg(val + p0 + k) : TV(0);
+    }
+}
+
+// One warp processes one warp row block whose stream (c, v) is already in
+// registers.  A block holds either at most kRowsPerWarpBlock rows with at
+// most `cap` (<= 256) nonzeros in total, or one row of any length.
+//  * Packed rows: gathers of x for the staged indices, epilogue operands
+//    and row pointers are issued together; products go to the warp's
+//    shared slice; after __syncwarp a team of T lanes (T a power of two,
+//    T * rows <= 32) sums each row by a fixed shuffle tree and the team
+//    leader applies the epilogue.
+//  * One long row: the warp strides over it from global memory, 256
+//    nonzeros per round.
 template <typename TA, typename TV, typename TX, class Epi>
-__device__ __forceinline__ void rowblock_spmv(const int* __restrict__ blk, const int* __restrict__ rp,
-                                              const int* __restrict__ ci, const TV* __restrict__ val,
-                                              const TX* __restrict__ x, Epi& epi, TA* s_prod, TA* s_red) {
-    const int b = blockIdx.x;
-    const int tid = threadIdx.x;
-    const int r0 = blk[b], r1 = blk[b + 1];
-    const int nrows = r1 - r0;
-    const int p0 = rp[r0], p1 = rp[r1];
-    const int nnzb = p1 - p0;
-    if (nrows == 1) {
+__device__ __forceinline__ void warp_process(int2 d0, int2 d1, int cap, const int* __restrict__ rp,
+                                             const int* __restrict__ ci, const TV* __restrict__ val,
+                                             const TX* __restrict__ x, Epi& epi, TA* s_prod, const int (&c)[kWarpU],
+                                             const TV (&v)[kWarpU]) {
+    const int lane = threadIdx.x & 31;
+    const int r0 = d0.x, p0 = d0.y, r1 = d1.x, p1 = d1.y;
+    const int nrows = r1 - r0, nnzb = p1 - p0;
+    constexpr int U = kWarpU;
+    typename Epi::Pre pre{};
+    if (nnzb > cap) {
+        if (lane == 0) pre = epi.prefetch(r0);
         TA s = TA(0);
-        int k = p0 + tid;
-        for (; k + 3 * kBlock < p1; k += 4 * kBlock) {
-            int c0 = __ldg(ci + k), c1 = __ldg(ci + k + kBlock), c2 = __ldg(ci + k + 2 * kBlock),
-                c3 = __ldg(ci + k + 3 * kBlock);
-            TV v0 = __ldg(val + k), v1 = __ldg(val + k + kBlock), v2 = __ldg(val + k + 2 * kBlock),
-               v3 = __ldg(val + k + 3 * kBlock);
-            TA a0 = TA(v0) * TA(__ldg(x + c0)), a1 = TA(v1) * TA(__ldg(x + c1));
-            TA a2 = TA(v2) * TA(__ldg(x + c2)), a3 = TA(v3) * TA(__ldg(x + c3));
-            s += (a0 + a1) + (a2 + a3);
+        for (int base = p0 + lane; base < p1; base += 32 * U) {
+            int cc[U];
+            TV vv[U];
+            TX xv[U];
+#pragma unroll
+            for (int q = 0; q < U; ++q) {
+                const int k = base + 32 * q;
+                cc[q] = (k < p1) ? __ldg(ci + k) : 0;
+                vv[q] = (k < p1) ? __ldg(val + k) : TV(0);
+            }
+#pragma unroll
+            for (int q = 0; q < U; ++q) xv[q] = (base + 32 * q < p1) ? __ldg(x + cc[q]) : TX(0);
+#pragma unroll
+            for (int q = 0; q < U; ++q) s += TA(vv[q]) * TA(xv[q]);
         }
-        for (; k < p1; k += kBlock) s += TA(__ldg(val + k)) * TA(__ldg(x + __ldg(ci + k)));
-        s = block_sum(s, s_red);
-        if (tid == 0) epi.row(r0, s);
+        s = warp_sum(s);
+        if (lane == 0) epi.row(r0, s, pre);
         return;
     }
-    // stage the products of the whole row block
-    {
-        int k = tid;
-        for (; k + 3 * kBlock < nnzb; k += 4 * kBlock) {
-            int c0 = __ldg(ci + p0 + k), c1 = __ldg(ci + p0 + k + kBlock), c2 = __ldg(ci + p0 + k + 2 * kBlock),
-                c3 = __ldg(ci + p0 + k + 3 * kBlock);
-            TV v0 = __ldg(val + p0 + k), v1 = __ldg(val + p0 + k + kBlock), v2 = __ldg(val + p0 + k + 2 * kBlock),
-               v3 = __ldg(val + p0 + k + 3 * kBlock);
-            TX x0 = __ldg(x + c0), x1 = __ldg(x + c1), x2 = __ldg(x + c2), x3 = __ldg(x + c3);
-            s_prod[k] = TA(v0) * TA(x0);
-            s_prod[k + kBlock] = TA(v1) * TA(x1);
-            s_prod[k + 2 * kBlock] = TA(v2) * TA(x2);
-            s_prod[k + 3 * kBlock] = TA(v3) * TA(x3);
-        }
-        for (; k < nnzb; k += kBlock) s_prod[k] = TA(__ldg(val + p0 + k)) * TA(__ldg(x + __ldg(ci + p0 + k)));
-    }
-    __syncthreads();
-    // team size: largest power of two <= kBlock / nrows, at most 32
     int T = 32;
-    while (T > 1 && T * nrows > kBlock) T >>= 1;
-    const int team = tid / T, lane = tid & (T - 1), nteams = kBlock / T;
-    const int rounds = (nrows + nteams - 1) / nteams;  // uniform across the block
-    for (int q = 0; q < rounds; ++q) {
-        const int r = r0 + q * nteams + team;
-        TA s = TA(0);
-        if (r < r1) {
-            const int a = rp[r] - p0, e = rp[r + 1] - p0;
-            for (int k = a + lane; k < e; k += T) s += s_prod[k];
+    while (T > 1 && T * nrows > 32) T >>= 1;
+    const int team = lane / T, tl = lane & (T - 1);
+    const int r = r0 + team;
+    const bool mine = r < r1;
+    TX xv[U];
+#pragma unroll
+    for (int q = 0; q < U; ++q) xv[q] = (lane + 32 * q < nnzb) ? __ldg(x + c[q]) : TX(0);
+    if (mine && tl == 0) pre = epi.prefetch(r);
+    int ra = 0, re = 0;
+    if (mine) {
+        ra = __ldg(rp + r) - p0;
+        re = __ldg(rp + r + 1) - p0;
+    }
+#pragma unroll
+    for (int q = 0; q < U; ++q)
+        if (lane + 32 * q < nnzb) s_prod[lane + 32 * q] = TA(v[q]) * TA(xv[q]);
+    __syncwarp();
+    TA s = TA(0);
+    for (int k = ra + tl; k < re; k += T) s += s_prod[k];
+    for (int o = T >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (mine && tl == 0) epi.row(r, s, pre);
+    __syncwarp();  // the slice is rewritten by the next block
+}
+
+// Persistent warps: warp g of G takes warp row blocks g, g+G, g+2G, ...
+// While it gathers and reduces one block, the next block's index/value
+// stream and the descriptor after that are already in flight (register
+// double buffering).  The per-row reduction order depends only on the
+// layout, so results do not depend on the grid.
+template <typename TA, typename TV, typename TX, class Epi>
+__device__ __forceinline__ void rowblock_spmv(const int2* __restrict__ blk, int nblk, int cap,
+                                              const int* __restrict__ rp, const int* __restrict__ ci,
+                                              const TV* __restrict__ val, const TX* __restrict__ x, Epi& epi,
+                                              TA* /*s_red*/) {
+    extern __shared__ __align__(16) unsigned char nir_smem[];
+    const int w = threadIdx.x >> 5;
+    TA* s_prod = reinterpret_cast<TA*>(nir_smem) + w * kWarpCapMax;
+    const int G = gridDim.x * kWarps;
+    int b = blockIdx.x * kWarps + w;
+    if (b >= nblk) return;
+    int2 d0 = __ldg(blk + b), d1 = __ldg(blk + b + 1);
+    int c[kWarpU];
+    TV v[kWarpU];
+    stream_load<TV>(d0, d1, cap, ci, val, c, v);
+    int2 n0 = make_int2(0, 0), n1 = make_int2(0, 0);
+    if (b + G < nblk) {
+        n0 = __ldg(blk + b + G);
+        n1 = __ldg(blk + b + G + 1);
+    }
+    for (;;) {
+        const bool has_next = b + G < nblk;
+        int cn[kWarpU];
+        TV vn[kWarpU];
+        stream_load<TV>(n0, n1, has_next ? cap : -1, ci, val, cn, vn);
+        int2 m0 = make_int2(0, 0), m1 = make_int2(0, 0);
+        if (b + 2 * G < nblk) {
+            m0 = __ldg(blk + b + 2 * G);
+            m1 = __ldg(blk + b + 2 * G + 1);
         }
-        for (int o = T >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0 && r < r1) epi.row(r, s);
+        warp_process<TA, TV, TX>(d0, d1, cap, rp, ci, val, x, epi, s_prod, c, v);
+        if (!has_next) break;
+#pragma unroll
+        for (int q = 0; q < kWarpU; ++q) {
+            c[q] = cn[q];
+            v[q] = vn[q];
+        }
+        d0 = n0;
+        d1 = n1;
+        n0 = m0;
+        n1 = m1;
+        b += G;
     }
 }
 
@@ -100,31 +186,28 @@ __device__ __forceinline__ void write_partials(const Epi& epi, double* __restric
     }
 }
 
-template <typename TA>
-__device__ __forceinline__ TA* smem_products() {
-    extern __shared__ __align__(16) unsigned char nir_smem[];
-    return reinterpret_cast<TA*>(nir_smem);
-}
-
 // ---------------------------------------------------------------- plain SpMV
 
 template <typename TA>
 struct PlainEpi {
     static constexpr int NQ = 0;
     static constexpr bool kLastIsMax = false;
+    struct Pre {};
     double q[1];
     TA* y;
-    __device__ void row(int r, TA s) { y[r] = s; }
+    __device__ Pre prefetch(int) const { return Pre{}; }
+    __device__ void row(int r, TA s, const Pre&) { y[r] = s; }
 };
 
 template <typename TA, typename TV, typename TX>
-__global__ void __launch_bounds__(kBlock) k_spmv_adaptive(const int* __restrict__ blk, const int* __restrict__ rp,
-                                                          const int* __restrict__ ci, const TV* __restrict__ val,
-                                                          const TX* __restrict__ x, TA* __restrict__ y) {
+__global__ void __launch_bounds__(kBlock) k_spmv_adaptive(const int2* __restrict__ blk, int nblk, int cap,
+                                                          const int* __restrict__ rp, const int* __restrict__ ci,
+                                                          const TV* __restrict__ val, const TX* __restrict__ x,
+                                                          TA* __restrict__ y) {
     __shared__ TA s_red[kWarps];
     PlainEpi<TA> epi;
     epi.y = y;
-    rowblock_spmv<TA, TV, TX>(blk, rp, ci, val, x, epi, smem_products<TA>(), s_red);
+    rowblock_spmv<TA, TV, TX>(blk, nblk, cap, rp, ci, val, x, epi, s_red);
 }
 
 // ---------------------------------------------------------------- PDHG step
@@ -157,6 +240,9 @@ template <typename T, bool CHECK>
 struct PrimalEpi {
     static constexpr int NQ = CHECK ? 2 : 0;
     static constexpr bool kLastIsMax = false;
+    struct Pre {
+        T x, c, lo, up, x0;
+    };
     double q[2] = {0.0, 0.0};
     T* __restrict__ x;
     T* __restrict__ xbar;
@@ -167,21 +253,26 @@ struct PrimalEpi {
     const T* __restrict__ x0;
     StepScalars<T> s;
     int halpern;
-    __device__ void row(int j, T aty) {
-        const T xj = x[j];
-        const T xp = clamp_box(xj - s.tau * (c[j] - aty), lo[j], up[j]);
+    __device__ Pre prefetch(int j) const {
+        Pre p;
+        p.x = x[j];
+        p.c = __ldg(c + j);
+        p.lo = __ldg(lo + j);
+        p.up = __ldg(up + j);
+        p.x0 = (halpern || CHECK) ? x0[j] : T(0);
+        return p;
+    }
+    __device__ void row(int j, T aty, const Pre& p) {
+        const T xj = p.x;
+        const T xp = clamp_box(xj - s.tau * (p.c - aty), p.lo, p.up);
         xbar[j] = T(2) * xp - xj;
         T xn = xp;
-        T a0 = T(0);
-        if (halpern) {
-            a0 = x0[j];
-            xn = s.w * ((T(1) + s.rho) * xp - s.rho * xj) + s.onemw * a0;
-        }
+        if (halpern) xn = s.w * ((T(1) + s.rho) * xp - s.rho * xj) + s.onemw * p.x0;
         x[j] = xn;
         if (CHECK) {
             xplus[j] = xp;
             const double d = double(xj) - double(xp);
-            const double e = double(xp) - double(halpern ? a0 : x0[j]);
+            const double e = double(xp) - double(p.x0);
             q[0] += d * d;
             q[1] += e * e;
         }
@@ -192,6 +283,9 @@ template <typename T, bool CHECK>
 struct DualEpi {
     static constexpr int NQ = CHECK ? 2 : 0;
     static constexpr bool kLastIsMax = false;
+    struct Pre {
+        T y, rl, ru, y0;
+    };
     double q[2] = {0.0, 0.0};
     T* __restrict__ y;
     T* __restrict__ yplus;
@@ -200,21 +294,25 @@ struct DualEpi {
     const T* __restrict__ y0;
     StepScalars<T> s;
     int halpern;
-    __device__ void row(int i, T ax) {
-        const T yi = y[i];
-        const T p = clamp_box(ax - yi / s.sigma, rl[i], ru[i]);
-        const T yp = yi + s.sigma * (p - ax);
+    __device__ Pre prefetch(int i) const {
+        Pre p;
+        p.y = y[i];
+        p.rl = __ldg(rl + i);
+        p.ru = __ldg(ru + i);
+        p.y0 = (halpern || CHECK) ? y0[i] : T(0);
+        return p;
+    }
+    __device__ void row(int i, T ax, const Pre& p) {
+        const T yi = p.y;
+        const T pr = clamp_box(ax - yi / s.sigma, p.rl, p.ru);
+        const T yp = yi + s.sigma * (pr - ax);
         T yn = yp;
-        T a0 = T(0);
-        if (halpern) {
-            a0 = y0[i];
-            yn = s.w * ((T(1) + s.rho) * yp - s.rho * yi) + s.onemw * a0;
-        }
+        if (halpern) yn = s.w * ((T(1) + s.rho) * yp - s.rho * yi) + s.onemw * p.y0;
         y[i] = yn;
         if (CHECK) {
             yplus[i] = yp;
             const double d = double(yi) - double(yp);
-            const double e = double(yp) - double(halpern ? a0 : y0[i]);
+            const double e = double(yp) - double(p.y0);
             q[0] += d * d;
             q[1] += e * e;
         }
@@ -222,7 +320,9 @@ struct DualEpi {
 };
 
 struct IterArgs {
-    const int* blk;
+    const int2* blk;
+    int nblk;
+    int cap;
     const int* rp;
     const int* ci;
     double* part;
@@ -250,7 +350,7 @@ __global__ void __launch_bounds__(kBlock) k_primal(IterArgs a, const T* __restri
     epi.x0 = x0;
     epi.s = step_scalars<T>(a.st, a.i_in_chunk, a.halpern, a.rho);
     epi.halpern = a.halpern;
-    rowblock_spmv<T, T, T>(a.blk, a.rp, a.ci, val, y, epi, smem_products<T>(), reinterpret_cast<T*>(s_red));
+    rowblock_spmv<T, T, T>(a.blk, a.nblk, a.cap, a.rp, a.ci, val, y, epi, reinterpret_cast<T*>(s_red));
     if (CHECK) write_partials(epi, a.part, s_red);
 }
 
@@ -268,7 +368,7 @@ __global__ void __launch_bounds__(kBlock) k_dual(IterArgs a, const T* __restrict
     epi.y0 = y0;
     epi.s = step_scalars<T>(a.st, a.i_in_chunk, a.halpern, a.rho);
     epi.halpern = a.halpern;
-    rowblock_spmv<T, T, T>(a.blk, a.rp, a.ci, val, xbar, epi, smem_products<T>(), reinterpret_cast<T*>(s_red));
+    rowblock_spmv<T, T, T>(a.blk, a.nblk, a.cap, a.rp, a.ci, val, xbar, epi, reinterpret_cast<T*>(s_red));
     if (CHECK) write_partials(epi, a.part, s_red);
 }
 
@@ -281,15 +381,19 @@ template <typename TX>
 struct KktRowEpi {
     static constexpr int NQ = 4;
     static constexpr bool kLastIsMax = true;
+    struct Pre {
+        double d, lo, hi;
+        TX y;
+    };
     double q[4] = {0.0, 0.0, 0.0, 0.0};
     const double* __restrict__ dr;
     const double* __restrict__ rl;  // original row bounds, +-inf = none
     const double* __restrict__ ru;
     const TX* __restrict__ yplus;
-    __device__ void row(int i, double ax_s) {
-        const double d = dr[i];
-        const double ax = ax_s / d;
-        const double lo = rl[i], hi = ru[i];
+    __device__ Pre prefetch(int i) const { return Pre{__ldg(dr + i), __ldg(rl + i), __ldg(ru + i), yplus[i]}; }
+    __device__ void row(int i, double ax_s, const Pre& p) {
+        const double ax = ax_s / p.d;
+        const double lo = p.lo, hi = p.hi;
         double v = 0.0, b = 0.0;
         if (ax < lo) {
             v = ax - lo;
@@ -300,7 +404,7 @@ struct KktRowEpi {
         }
         q[0] += v * v;
         if (v != 0.0) q[3] = fmax(q[3], fabs(v) / (1.0 + fabs(b)));
-        const double yi = double(yplus[i]) * d;
+        const double yi = double(p.y) * p.d;
         if (yi > 0.0) {
             if (isfinite(lo)) q[1] += lo * yi;
             else q[2] += yi * yi;
@@ -318,16 +422,22 @@ template <typename TX>
 struct KktColEpi {
     static constexpr int NQ = 4;
     static constexpr bool kLastIsMax = false;
+    struct Pre {
+        double d, c, lo, hi;
+        TX x;
+    };
     double q[4] = {0.0, 0.0, 0.0, 0.0};
     const double* __restrict__ dc;
     const double* __restrict__ c;   // original cost
     const double* __restrict__ l;   // original column bounds, +-inf = none
     const double* __restrict__ u;
     const TX* __restrict__ xplus;
-    __device__ void row(int j, double aty_s) {
-        const double d = dc[j];
-        const double rc = c[j] - aty_s / d;
-        const double lo = l[j], hi = u[j];
+    __device__ Pre prefetch(int j) const {
+        return Pre{__ldg(dc + j), __ldg(c + j), __ldg(l + j), __ldg(u + j), xplus[j]};
+    }
+    __device__ void row(int j, double aty_s, const Pre& p) {
+        const double rc = p.c - aty_s / p.d;
+        const double lo = p.lo, hi = p.hi;
         double lam = 0.0;
         if (rc > 0.0 && isfinite(lo)) lam = rc;
         if (rc < 0.0 && isfinite(hi)) lam = rc;
@@ -335,8 +445,8 @@ struct KktColEpi {
         q[0] += r * r;
         if (lam > 0.0) q[1] += lo * lam;
         else if (lam < 0.0) q[1] += hi * lam;
-        const double xj = double(xplus[j]) * d;
-        q[2] += c[j] * xj;
+        const double xj = double(p.x) * p.d;
+        q[2] += p.c * xj;
         double xv = 0.0;
         if (xj < lo) xv = xj - lo;
         else if (xj > hi) xv = xj - hi;
@@ -345,7 +455,9 @@ struct KktColEpi {
 };
 
 struct KktArgs {
-    const int* blk;
+    const int2* blk;
+    int nblk;
+    int cap;
     const int* rp;
     const int* ci;
     const double* val;  // scaled FP64 values
@@ -365,7 +477,7 @@ __global__ void __launch_bounds__(kBlock) k_kkt_rows(KktArgs a, const TX* __rest
     epi.rl = rl;
     epi.ru = ru;
     epi.yplus = yplus;
-    rowblock_spmv<double, double, TX>(a.blk, a.rp, a.ci, a.val, xplus, epi, smem_products<double>(), s_red);
+    rowblock_spmv<double, double, TX>(a.blk, a.nblk, a.cap, a.rp, a.ci, a.val, xplus, epi, s_red);
     write_partials(epi, a.part, s_red);
 }
 
@@ -381,7 +493,7 @@ __global__ void __launch_bounds__(kBlock) k_kkt_cols(KktArgs a, const TX* __rest
     epi.l = l;
     epi.u = u;
     epi.xplus = xplus;
-    rowblock_spmv<double, double, TX>(a.blk, a.rp, a.ci, a.val, yplus, epi, smem_products<double>(), s_red);
+    rowblock_spmv<double, double, TX>(a.blk, a.nblk, a.cap, a.rp, a.ci, a.val, yplus, epi, s_red);
     write_partials(epi, a.part, s_red);
 }
 
@@ -390,9 +502,9 @@ __global__ void __launch_bounds__(kBlock) k_kkt_cols(KktArgs a, const TX* __rest
 struct CtlArgs {
     const double* partP;   // primal kernel partials, 2 x nP
     const double* partD;   // dual kernel partials, 2 x nD
-    const double* partKR;  // KKT row partials, 4 x nD
-    const double* partKC;  // KKT column partials, 4 x nP
-    int nP, nD;
+    const double* partKR;  // KKT row partials, 4 x nKR
+    const double* partKC;  // KKT column partials, 4 x nKC
+    int nP, nD, nKR, nKC;  // grids of the kernels that wrote them
     double bnorm, cnorm, offset;
     double tol, feas_tol;
     int K;
@@ -414,14 +526,14 @@ __global__ void __launch_bounds__(kBlock) k_control(CtlArgs a, DevState* st) {
     const double dxa2 = block_sum_array(a.partP + a.nP, a.nP, sh);
     const double dy2 = block_sum_array(a.partD, a.nD, sh);
     const double dya2 = block_sum_array(a.partD + a.nD, a.nD, sh);
-    const double pres2 = block_sum_array(a.partKR, a.nD, sh);
-    const double dobj_r = block_sum_array(a.partKR + a.nD, a.nD, sh);
-    const double ywrong2 = block_sum_array(a.partKR + 2 * a.nD, a.nD, sh);
-    const double maxrel = block_max_array(a.partKR + 3 * a.nD, a.nD, sh);
-    const double dres2 = block_sum_array(a.partKC, a.nP, sh);
-    const double dobj_c = block_sum_array(a.partKC + a.nP, a.nP, sh);
-    const double pobj_c = block_sum_array(a.partKC + 2 * a.nP, a.nP, sh);
-    const double xviol2 = block_sum_array(a.partKC + 3 * a.nP, a.nP, sh);
+    const double pres2 = block_sum_array(a.partKR, a.nKR, sh);
+    const double dobj_r = block_sum_array(a.partKR + a.nKR, a.nKR, sh);
+    const double ywrong2 = block_sum_array(a.partKR + 2 * a.nKR, a.nKR, sh);
+    const double maxrel = block_max_array(a.partKR + 3 * a.nKR, a.nKR, sh);
+    const double dres2 = block_sum_array(a.partKC, a.nKC, sh);
+    const double dobj_c = block_sum_array(a.partKC + a.nKC, a.nKC, sh);
+    const double pobj_c = block_sum_array(a.partKC + 2 * a.nKC, a.nKC, sh);
+    const double xviol2 = block_sum_array(a.partKC + 3 * a.nKC, a.nKC, sh);
     if (threadIdx.x != 0) return;
 
     const long long it = st->iter + a.K;

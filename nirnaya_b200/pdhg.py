@@ -82,7 +82,7 @@ POLL_FN = C.CFUNCTYPE(C.c_int, C.c_void_p)
 EXPORTED = [
     "nir_pdhg_default_params", "nir_pdhg_create", "nir_pdhg_update_vectors", "nir_pdhg_solve",
     "nir_pdhg_solve_lp", "nir_pdhg_free", "nir_pdhg_last_error", "nir_pdhg_spmv", "nir_pdhg_time_spmv",
-    "nir_pdhg_set_profiling", "nir_pdhg_kernel_times", "nir_pdhg_get_layout",
+    "nir_pdhg_set_profiling", "nir_pdhg_kernel_times", "nir_pdhg_get_layout", "nir_pdhg_history",
 ]
 
 _lib = None
@@ -109,6 +109,7 @@ def lib():
         L.nir_pdhg_set_profiling.argtypes = [C.c_void_p, C.c_int]
         L.nir_pdhg_kernel_times.argtypes = [C.c_void_p, C.POINTER(KernelTime)]
         L.nir_pdhg_get_layout.argtypes = [C.c_void_p, C.POINTER(Layout)]
+        L.nir_pdhg_history.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.c_int]
         _lib = L
     return _lib
 
@@ -211,6 +212,14 @@ class Engine:
         kt = KernelTime()
         lib().nir_pdhg_kernel_times(self._h, C.byref(kt))
         return kt
+
+    def history(self, max_entries: int = 4096) -> np.ndarray:
+        """(iteration, kkt, primal, dual, gap, residual, omega, phase) per check."""
+        buf = np.zeros((max_entries, 8))
+        cnt = lib().nir_pdhg_history(self._h, _dptr(buf), max_entries)
+        if cnt < 0:
+            raise RuntimeError(last_error())
+        return buf[:cnt].copy()
 
     def layout(self) -> Layout:
         lo = Layout()

@@ -221,7 +221,7 @@ def test_plain_pdhg_on_fast_kernels_tracks_reference_loop():
 def test_iteration_limit_and_host_stop():
     lp = L.generate(L.RANDOM_EQ, 5, m=500, n=1250)
     with pdhg.Engine(lp) as eng:
-        _, _, info = eng.solve(pdhg.default_params(max_iters=128, tol=1e-12))
+        _, _, info = eng.solve(pdhg.default_params(max_iters=128, tol=0.0))
         assert info.status == pdhg.ITERATION_LIMIT and info.iterations == 128
         _, _, info = eng.solve(pdhg.default_params(algorithm=pdhg.ALGO_REFERENCE, max_iters=100))
         assert info.iterations == 100
@@ -231,10 +231,10 @@ def test_iteration_limit_and_host_stop():
             calls.append(1)
             return len(calls) > 3
 
-        _, _, info = eng.solve(pdhg.default_params(tol=1e-14, max_iters=10 ** 7), poll=poll)
+        _, _, info = eng.solve(pdhg.default_params(tol=0.0, max_iters=10 ** 7), poll=poll)
         assert info.status == pdhg.TIME_LIMIT and len(calls) >= 4
         t = time.time()
-        _, _, info = eng.solve(pdhg.default_params(tol=1e-14, max_iters=10 ** 8, time_limit=0.5))
+        _, _, info = eng.solve(pdhg.default_params(tol=0.0, max_iters=10 ** 8, time_limit=0.5))
         assert info.status == pdhg.TIME_LIMIT and time.time() - t < 10
 
 
@@ -280,5 +280,5 @@ def test_reference_shaped_api():
     assert r.x.shape == (2,) and r.y.shape == (2,) and r.iterations > 0
     d = pdhg.Deadline(60.0)
     d.interrupt()
-    r = pdhg.PdhgSolver.solve(L.generate(L.RANDOM_EQ, 1), pdhg.Options(pdhg_tol=1e-12), d)
+    r = pdhg.PdhgSolver.solve(L.generate(L.RANDOM_EQ, 1), pdhg.Options(pdhg_tol=0.0), d)
     assert r.status == pdhg.TIME_LIMIT
