@@ -184,6 +184,41 @@ typedef struct nir_pdhg_layout {
 } nir_pdhg_layout;
 int nir_pdhg_get_layout(nir_pdhg* h, nir_pdhg_layout* out);
 
+/* --- no-allocation entry point --- */
+
+/* A CSR matrix that already lives in device memory (all DEVICE pointers). */
+typedef struct nir_csr_dev {
+    int32_t rows, cols;
+    const int32_t* row_ptr;   /* rows+1, row_ptr[0] = 0                        */
+    const int32_t* col_idx;   /* row_ptr[rows] entries                          */
+    const double* value;      /* row_ptr[rows] entries                          */
+} nir_csr_dev;
+
+/* The reference PDHG loop (the NIR_ALGO_REFERENCE kernels, bit for bit) on
+ * an LP the caller already holds in device memory, without allocating any
+ * device memory.  No counterpart in the reference: it exists for callers
+ * that cannot call cudaMalloc -- processes whose device memory is owned by
+ * their own pool allocator, and latency-critical callers that may not take
+ * cudaMalloc's implicit device synchronisation.
+ *   A, At          CSR of A (nrow x ncol) and of A' (ncol x nrow), each row's
+ *                  entries in ascending column order (A' = the CSC of A)
+ *   cost..rowup    device vectors (bounds as in nir_lp.h)
+ *   stream         cudaStream_t to run on (NULL = the default stream)
+ *   x_out, y_out   device outputs (ncol, nrow), also the loop's iterates
+ *   iterations, status  host outputs (as nir_pdhg_solve with REFERENCE)
+ * Scratch lives in one file-scope device array of 2^20 doubles (8 MiB) per
+ * GPU, held until the process exits; the LP must satisfy
+ * 32 + 2*ncol + nrow + ceil(nrow/256) <= 2^20, else NIR_STATUS_INPUT_ERROR.
+ * The first call on a device resolves the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture.  All calls share the array and each call
+ * clears the state it needs: calls that overlap on the GPU (other streams,
+ * other threads) race.  Returns *status. */
+int nir_pdhg_reference_solve_noalloc(const nir_csr_dev* A, const nir_csr_dev* At, const double* cost,
+                                     const double* collo, const double* colup, const double* rowlo,
+                                     const double* rowup, int64_t max_iters, void* stream, double* x_out,
+                                     double* y_out, int64_t* iterations, int32_t* status);
+
 #ifdef __cplusplus
 }
 #endif

@@ -19,6 +19,7 @@
 #include <cstring>
 #include <limits>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -1443,3 +1444,120 @@ int nir_pdhg_get_layout(nir_pdhg* h, nir_pdhg_layout* out) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- no-allocation entry point
+//
+// nir_pdhg_reference_solve_noalloc runs the reference PDHG loop (the same
+// kernels as NIR_ALGO_REFERENCE) on an LP that the caller already holds in
+// device memory, for callers that cannot allocate device memory themselves:
+// a process whose whole device budget belongs to its own pool allocator, or
+// a latency-critical caller that may not take cudaMalloc's implicit device
+// synchronisation.  Its working memory (the extrapolated primal, the two
+// power-iteration vectors, per-block maxima and the solver state) lives in
+// the file-scope array below; every GPU that loads this library holds the
+// array until the process exits.
+
+namespace {
+
+constexpr long long kNoAllocScratchDoubles = 1LL << 20;  // 8 MiB per device
+
+__device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
+
+// Device address of g_noalloc_scratch, resolved once per device with that
+// device current.  In host code the symbol itself is only a host-side
+// stand-in and must never be passed to a kernel.
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double* g_noalloc_addr[kMaxDevices] = {};
+
+double* noalloc_scratch(int device) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            throw CudaError(std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
+        g_noalloc_addr[device] = static_cast<double*>(p);
+    }
+    return g_noalloc_addr[device];
+}
+
+}  // namespace
+
+extern "C" int nir_pdhg_reference_solve_noalloc(const nir_csr_dev* A, const nir_csr_dev* At, const double* cost,
+                                                const double* collo, const double* colup, const double* rowlo,
+                                                const double* rowup, int64_t max_iters, void* stream, double* x_out,
+                                                double* y_out, int64_t* iterations, int32_t* status) {
+    if (!A || !At || !cost || !collo || !colup || !rowlo || !rowup || !x_out || !y_out || !iterations || !status) {
+        g_err = "null argument";
+        return NIR_STATUS_INPUT_ERROR;
+    }
+    const long long m = A->rows, n = A->cols;
+    if (m < 0 || n < 0 || At->rows != n || At->cols != m || max_iters < 0) {
+        g_err = "inconsistent dimensions of A and A'";
+        return NIR_STATUS_INPUT_ERROR;
+    }
+    // scratch: state (256 B) | xbar (n) | u (n) | v (m) | per-block maxima
+    const long long state_d = 32;
+    const long long nblk = (m + nir::kBlock - 1) / nir::kBlock;
+    const long long need = state_d + 2 * n + m + std::max(nblk, 1LL);
+    if (need > kNoAllocScratchDoubles) {
+        g_err = "LP too large for the no-allocation entry point: needs 32 + 2*ncol + nrow + ceil(nrow/256) = " +
+                std::to_string(need) + " doubles of scratch, the limit is " + std::to_string(kNoAllocScratchDoubles);
+        return NIR_STATUS_INPUT_ERROR;
+    }
+    try {
+        int dev = 0;
+        NIR_CUDA(cudaGetDevice(&dev));
+        if (dev < 0 || dev >= kMaxDevices) throw std::invalid_argument("device ordinal beyond the supported range");
+        double* base = noalloc_scratch(dev);
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        nir::DevState* st = reinterpret_cast<nir::DevState*>(base);
+        double* xbar = base + state_d;
+        double* u = xbar + n;
+        double* v = u + n;
+        double* part = v + m;
+        const int mi = int(m), ni = int(n);
+        // every call starts from a cleared state: the array keeps the last call's contents
+        nir::DevState st0{};
+        st0.max_iters = max_iters;
+        NIR_CUDA(cudaMemcpyAsync(st, &st0, sizeof(st0), cudaMemcpyHostToDevice, s));
+        const unsigned gm = grid_for(m), gn = grid_for(n);
+        nir::k_fill<<<gn, nir::kBlock, 0, s>>>(n, 1.0, u);
+        for (int r = 0; r < 12; ++r) {
+            nir::k_ref_spmv<<<gm, nir::kBlock, 0, s>>>(mi, A->row_ptr, A->col_idx, A->value, u, v);
+            nir::k_ref_spmv<<<gn, nir::kBlock, 0, s>>>(ni, At->row_ptr, At->col_idx, At->value, v, u);
+            nir::k_ref_norm<<<1, 32, 0, s>>>(ni, u, st);
+            nir::k_ref_div<<<gn, nir::kBlock, 0, s>>>(ni, u, st);
+        }
+        nir::k_ref_steps<<<1, 32, 0, s>>>(st);
+        nir::k_ref_init<<<grid_for(std::max(m, n)), nir::kBlock, 0, s>>>(ni, mi, collo, colup, x_out, y_out);
+        NIR_LAUNCHED();
+        const int K = 32;
+        nir::DevState host{};
+        for (long long done_it = 0; done_it < max_iters; done_it += K) {
+            for (int i = 0; i < K; ++i) {
+                nir::k_ref_primal<<<gn, nir::kBlock, 0, s>>>(ni, At->row_ptr, At->col_idx, At->value, y_out, cost, collo,
+                                                            colup, x_out, xbar, st, i);
+                nir::k_ref_dual<<<gm, nir::kBlock, 0, s>>>(mi, A->row_ptr, A->col_idx, A->value, xbar, rowlo, rowup,
+                                                          y_out, part, st, i);
+                nir::k_ref_stop<<<1, nir::kBlock, 0, s>>>(part, int(std::max(nblk, 1LL)), st, i, K);
+            }
+            NIR_LAUNCHED();
+            NIR_CUDA(cudaMemcpyAsync(&host, st, sizeof(host), cudaMemcpyDeviceToHost, s));
+            NIR_CUDA(cudaStreamSynchronize(s));
+            if (host.done) break;
+        }
+        NIR_CUDA(cudaMemcpyAsync(&host, st, sizeof(host), cudaMemcpyDeviceToHost, s));
+        NIR_CUDA(cudaStreamSynchronize(s));
+        *iterations = max_iters > 0 ? host.ref_iterations : 0;
+        *status = host.ref_stopped ? NIR_STATUS_OPTIMAL : NIR_STATUS_ITERATION_LIMIT;
+        return *status;
+    } catch (const std::invalid_argument& e) {
+        g_err = e.what();
+        return NIR_STATUS_INPUT_ERROR;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return NIR_STATUS_INTERNAL_ERROR;
+    }
+}
