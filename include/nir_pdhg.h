@@ -90,9 +90,17 @@ typedef struct nir_pdhg_params {
     int32_t spmv_block_nnz;       /* nonzeros per warp row block, 1..256; 0 = auto (0)   */
     int32_t use_graphs;           /* capture launch chunks in CUDA graphs        (1)     */
     int32_t verbose;              /* 1 = one line per check on stderr            (0)     */
+    int32_t restart_anchor;       /* residual the restart tests compare with: 0 = first
+                                     check after a restart, 1 = at the restart     (1)    */
+    int32_t polish_fresh;         /* MIXED hand-over to FP64: 2 = pure change of precision
+                                     (iterate, anchor and counters carry on), 1 = fresh
+                                     FP64 solve from the last FP32 point with the initial
+                                     weight, 0 = as 1 but keeping the weight     (2)    */
     const double* x_init;         /* warm start in original space, ncol, or NULL          */
     const double* y_init;         /* warm start duals, nrow, or NULL                      */
     double omega_init;            /* warm-start primal weight; <= 0 = default             */
+    double primal_weight_decades; /* the weight stays within this many decades of
+                                     its initial value                           (1.0)   */
 } nir_pdhg_params;
 
 typedef struct nir_pdhg_info {

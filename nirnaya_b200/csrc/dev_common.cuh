@@ -28,6 +28,8 @@ __device__ inline T clamp_box(T v, T lo, T hi) {  // lo/hi may be +-inf
 struct DevState {
     // step sizes and weight (FP64)
     double eta, omega, tau, sigma;
+    double log_omega0;     // log of the initial primal weight (bounds the updates)
+    long long it_phase;    // iteration at which the current phase began
     // restart bookkeeping
     long long iter;        // completed iterations
     long long k_base;      // Halpern inner count at the start of the current chunk

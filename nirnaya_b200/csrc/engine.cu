@@ -621,6 +621,8 @@ void launch_fast_chunk(nir_pdhg* h, const SolveCfg& cfg, int phase, ChunkTimer* 
     ca.theta = cfg.p.primal_weight_smoothing;
     ca.polish_stall = cfg.p.polish_stall_checks;
     ca.polish_switch = cfg.p.polish_switch_kkt;
+    ca.anchor_at_restart = cfg.p.restart_anchor ? 1 : 0;
+    ca.weight_decades = cfg.p.primal_weight_decades;
     ca.hist = h->hist;
     nir::k_control<<<1, nir::kBlock, 0, s>>>(ca, h->st);
     NIR_LAUNCHED();
@@ -666,7 +668,7 @@ unsigned long long chunk_key(const nir_pdhg* h, const SolveCfg& c, int phase, bo
     k.add(phase).add(f64).add(c.K).add(c.halpern).add(c.restarts).add(c.mixed).add(c.bnorm).add(c.cnorm);
     k.add(c.p.reflection).add(c.p.restart_sufficient).add(c.p.restart_necessary).add(c.p.restart_artificial);
     k.add(c.p.primal_weight_smoothing).add(c.p.polish_stall_checks).add(c.p.polish_switch_kkt).add(c.p.tol);
-    k.add(c.p.feas_tol).add(h->offset).add(h->A.cap).add(h->A.blk).add(h->At.blk).add(h->part).add(h->hist);
+    k.add(c.p.feas_tol).add(c.p.restart_anchor).add(c.p.primal_weight_decades).add(c.p.polish_fresh).add(h->offset).add(h->A.cap).add(h->A.blk).add(h->At.blk).add(h->part).add(h->hist);
     return k.h;
 }
 
@@ -1008,6 +1010,7 @@ int solve_fast(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), void* 
         if (p.omega_init > 0.0) omega = p.omega_init;
         st0.eta = eta;
         st0.omega = omega;
+        st0.log_omega0 = std::log(omega);
         st0.tau = eta / omega;
         st0.sigma = eta * omega;
     } else {
@@ -1086,16 +1089,37 @@ int solve_fast(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), void* 
             if (!R.stopped_by_host && cfg.mixed && !R.last.done && R.last.phase == 1) {
                 // FP32 stalled: polish in FP64 from the last evaluated point
                 t_switch = now_sec() - t_setup;
-                nir::k_promote<<<std::max(grid_for(std::max(n, m)), 1u), nir::kBlock, 0, s>>>(
-                    n, m, h->xp32, h->yp32, h->l64, h->u64, h->x64, h->x064, h->xp64, h->y64, h->y064, h->yp64);
-                NIR_LAUNCHED();
                 nir::DevState cur;
                 d2h(h, &cur, h->st, sizeof(cur));
-                cur.k_base = 0;
-                cur.have_anchor = 0;
+                if (p.polish_fresh == 2) {
+                    // a pure change of precision: the Halpern iterate, its anchor
+                    // and every counter carry on unchanged
+                    const long long nm = std::max(n, m);
+                    nir::k_to_double<<<grid_for(n), nir::kBlock, 0, s>>>(n, h->x32, h->x64);
+                    nir::k_to_double<<<grid_for(n), nir::kBlock, 0, s>>>(n, h->x032, h->x064);
+                    nir::k_to_double<<<grid_for(n), nir::kBlock, 0, s>>>(n, h->xp32, h->xp64);
+                    nir::k_to_double<<<grid_for(m), nir::kBlock, 0, s>>>(m, h->y32, h->y64);
+                    nir::k_to_double<<<grid_for(m), nir::kBlock, 0, s>>>(m, h->y032, h->y064);
+                    nir::k_to_double<<<grid_for(m), nir::kBlock, 0, s>>>(m, h->yp32, h->yp64);
+                    (void)nm;
+                } else {
+                    nir::k_promote<<<std::max(grid_for(std::max(n, m)), 1u), nir::kBlock, 0, s>>>(
+                        n, m, h->xp32, h->yp32, h->l64, h->u64, h->x64, h->x064, h->xp64, h->y64, h->y064, h->yp64);
+                    cur.k_base = 0;
+                    cur.have_anchor = 0;
+                }
+                NIR_LAUNCHED();
                 cur.apply_restart = 0;
                 cur.switch_request = 0;
                 cur.stall = 0;
+                if (p.polish_fresh == 1) {
+                    // the FP64 phase as a fresh solve warm-started at (x+, y+):
+                    // initial primal weight, restart schedule from the switch
+                    cur.omega = std::exp(cur.log_omega0);
+                    cur.tau = cur.eta / cur.omega;
+                    cur.sigma = cur.eta * cur.omega;
+                    cur.it_phase = cur.iter;
+                }
                 h2d(h, h->st, &cur, sizeof(cur));
                 final_phase = 1;
                 long long it_switch = cur.iter;
@@ -1173,9 +1197,12 @@ int nir_pdhg_default_params(nir_pdhg_params* p) {
     p->spmv_block_nnz = 0;
     p->use_graphs = 1;
     p->verbose = 0;
+    p->restart_anchor = 1;
+    p->polish_fresh = 2;
     p->x_init = nullptr;
     p->y_init = nullptr;
     p->omega_init = 0.0;
+    p->primal_weight_decades = 1.0;
     return 0;
 }
 

@@ -514,6 +514,8 @@ struct CtlArgs {
     double suff, nec, art, theta;
     int polish_stall;
     double polish_switch;
+    int anchor_at_restart; // 1: the residual at a restart becomes the new anchor
+    double weight_decades; // primal weight stays within this many decades of its start
     double* hist;          // ring of kHist entries x 8 doubles
 };
 
@@ -603,20 +605,30 @@ __global__ void __launch_bounds__(kBlock) k_control(CtlArgs a, DevState* st) {
     // fixed-point-residual restart test
     const long long k_after = st->k_base + a.K;
     bool restart = false;
+    const double it_phase = double(it - st->it_phase);
     if (!st->have_anchor) {
         st->r_anchor = res;
         st->have_anchor = 1;
         st->r_prev = res;
-        restart = (double(k_after) >= a.art * double(it));
+        restart = (double(k_after) >= a.art * it_phase);
     } else {
         restart = (res <= a.suff * st->r_anchor) || (res <= a.nec * st->r_anchor && res > st->r_prev) ||
-                  (double(k_after) >= a.art * double(it));
+                  (double(k_after) >= a.art * it_phase);
         st->r_prev = res;
     }
     if (restart) {
         const double dxa = sqrt(dxa2), dya = sqrt(dya2);
         if (dxa > 1e-10 && dya > 1e-10 && isfinite(dxa) && isfinite(dya)) {
-            const double lw = a.theta * log(dya / dxa) + (1.0 - a.theta) * log(omega);
+            // log-space smoothing toward ||dy||/||dx||, with two guards
+            // against a runaway (a primal pinned at its bounds makes dx tiny,
+            // a larger weight shrinks the primal step further): at most a
+            // factor 10 per restart, and within `weight_decades` decades of
+            // the initial weight
+            const double lo = log(omega) - 2.302585092994046, hi = log(omega) + 2.302585092994046;
+            double lw = a.theta * log(dya / dxa) + (1.0 - a.theta) * log(omega);
+            lw = fmin(fmax(lw, lo), hi);
+            const double span = 2.302585092994046 * a.weight_decades;
+            lw = fmin(fmax(lw, st->log_omega0 - span), st->log_omega0 + span);
             st->omega = exp(lw);
         }
         st->tau = st->eta / st->omega;
@@ -624,7 +636,10 @@ __global__ void __launch_bounds__(kBlock) k_control(CtlArgs a, DevState* st) {
         st->apply_restart = 1;
         st->restarts += 1;
         st->k_base = 0;
-        st->have_anchor = 0;
+        // the new anchor is z+ = T(z); ||z+ - T(z+)|| <= ||z - T(z)|| = res
+        st->have_anchor = a.anchor_at_restart;
+        st->r_anchor = res;
+        st->r_prev = res;
     } else {
         st->k_base = k_after;
     }

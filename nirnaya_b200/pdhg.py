@@ -48,8 +48,9 @@ class Params(C.Structure):
         ("restart_artificial", C.c_double), ("primal_weight_smoothing", C.c_double),
         ("step_factor", C.c_double), ("power_iters", C.c_int32), ("polish_stall_checks", C.c_int32),
         ("polish_switch_kkt", C.c_double), ("spmv_block_nnz", C.c_int32), ("use_graphs", C.c_int32),
-        ("verbose", C.c_int32), ("x_init", C.POINTER(C.c_double)), ("y_init", C.POINTER(C.c_double)),
-        ("omega_init", C.c_double),
+        ("verbose", C.c_int32), ("restart_anchor", C.c_int32), ("polish_fresh", C.c_int32),
+        ("x_init", C.POINTER(C.c_double)), ("y_init", C.POINTER(C.c_double)),
+        ("omega_init", C.c_double), ("primal_weight_decades", C.c_double),
     ]
 
 
