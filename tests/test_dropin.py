@@ -1,0 +1,148 @@
+"""The drop-in: the reference's own programs built with
+nirnaya_b200/sov/pdhg_solver.hpp in place of src/gpu/pdhg_solver.hpp
+(nirnaya_b200/sov/Makefile), so that Solver::solve, the CLI's
+`--method pdhg` / `--set method=pdhg`, the sov.h C API and the ctypes SDK
+reach the B200 engine.
+
+The binaries are built from the reference's sources where they are present
+and travel prebuilt; the tests skip when they were not built.
+"""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import golden_io as G
+from conftest import ROOT, has_gpu
+
+DROPIN = os.path.join(ROOT, "nirnaya_b200", "sov", "_dropin")
+GOLD = G.load()
+
+
+def _need(name):
+    path = os.path.join(DROPIN, name)
+    if not os.path.exists(path):
+        pytest.skip(f"{name} not built (needs the reference sources: make -C nirnaya_b200/sov)")
+    return path
+
+
+@pytest.mark.skipif(has_gpu(), reason="checks the no-GPU failure mode")
+def test_dropin_fails_loudly_without_gpu():
+    exe = _need("unit_tests")
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode != 0 and "no CUDA device" in (r.stdout + r.stderr)
+
+
+def test_dropin_links_the_engine():
+    exe = _need("unit_tests")
+    out = subprocess.run(["readelf", "-d", exe], capture_output=True, text=True).stdout
+    assert "libnir_pdhg.so" in out
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not has_gpu(), reason="needs a CUDA device")
+def test_reference_unit_tests_pass_on_the_gpu_engine():
+    # tests/unit_tests.cpp: 12 tests, GPU/PDHG-01 asserts status Optimal and
+    # objective 9 +- 1e-2 (:316-331); the other 11 must stay green
+    r = subprocess.run([_need("unit_tests")], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "12 / 12 tests passed" in r.stdout
+    assert "[PASS] GPU/PDHG-01" in r.stdout
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not has_gpu(), reason="needs a CUDA device")
+def test_reference_bench_runner_pdhg_row():
+    # tools/bench_runner.cpp:61-66,79-81: PDHG on Degenerate_Transport_LP
+    r = subprocess.run([_need("bench_runner")], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    row = [ln for ln in r.stdout.splitlines() if "PDHG (GPU)" in ln]
+    assert row, r.stdout
+    f = [t.strip() for t in row[0].split("|")]
+    assert abs(float(f[2]) - 13.0) <= 1e-5 and f[5] == "PASS"
+
+
+def _sov(lib_path):
+    lib = C.CDLL(lib_path)
+    lib.sov_env_create.restype = C.c_void_p
+    lib.sov_model_create.restype = C.c_void_p
+    lib.sov_model_create.argtypes = [C.c_void_p, C.c_char_p]
+    lib.sov_add_col.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int, C.c_char_p]
+    lib.sov_add_row.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int, C.POINTER(C.c_int),
+                                C.POINTER(C.c_double), C.c_char_p]
+    lib.sov_set_sense.argtypes = [C.c_void_p, C.c_int]
+    lib.sov_set_option_string.argtypes = [C.c_void_p, C.c_char_p, C.c_char_p]
+    lib.sov_optimize.argtypes = [C.c_void_p]
+    lib.sov_get_status.argtypes = [C.c_void_p]
+    lib.sov_get_obj.argtypes = [C.c_void_p]
+    lib.sov_get_obj.restype = C.c_double
+    lib.sov_get_x.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+    lib.sov_write_mps.argtypes = [C.c_void_p, C.c_char_p]
+    lib.sov_error_message.argtypes = [C.c_void_p]
+    lib.sov_error_message.restype = C.c_char_p
+    lib.sov_model_free.argtypes = [C.c_void_p]
+    lib.sov_env_free.argtypes = [C.c_void_p]
+    return lib
+
+
+def _build_model(lib, m, lp, sense):
+    """Adds an internal-minimisation LP to a sov model in the user's sense."""
+    sign = -1.0 if sense < 0 else 1.0
+    for j in range(lp.ncol):
+        lib.sov_add_col(m, sign * lp.cost[j], lp.collo[j], lp.colup[j], 0, f"x{j}".encode())
+    rows = [[] for _ in range(lp.nrow)]
+    for j in range(lp.ncol):
+        for k in range(lp.col_start[j], lp.col_start[j + 1]):
+            rows[lp.row_index[k]].append((j, lp.value[k]))
+    for i, r in enumerate(rows):
+        idx = (C.c_int * len(r))(*[a for a, _ in r])
+        val = (C.c_double * len(r))(*[b for _, b in r])
+        lib.sov_add_row(m, lp.rowlo[i], lp.rowup[i], len(r), idx, val, f"r{i}".encode())
+    lib.sov_set_sense(m, sense)
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not has_gpu(), reason="needs a CUDA device")
+def test_c_api_and_ctypes_sdk_reach_the_engine():
+    # the binding python/nirnaya.py makes (its :32-62), against the drop-in libsov.so
+    lib = _sov(_need("libsov.so"))
+    env = lib.sov_env_create()
+    m = lib.sov_model_create(env, b"pdhg_lp")
+    lib.sov_set_option_string(m, b"log_level", b"0")
+    g = GOLD["unit_test_pdhg_lp"]
+    _build_model(lib, m, G.lp_from(g["lp"]), 1)
+    assert lib.sov_set_option_string(m, b"method", b"pdhg") == 0
+    assert lib.sov_optimize(m) == 0, lib.sov_error_message(m)
+    assert lib.sov_get_status(m) == 0
+    assert abs(lib.sov_get_obj(m) - 9.0) <= 1e-4
+    x = (C.c_double * 2)()
+    lib.sov_get_x(m, x)
+    assert abs(x[0] - 3.0) <= 1e-3 and abs(x[1] - 1.0) <= 1e-3
+    lib.sov_model_free(m)
+    lib.sov_env_free(env)
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not has_gpu(), reason="needs a CUDA device")
+@pytest.mark.parametrize("args", [["--method", "pdhg"], ["--set", "method=pdhg"], ["--set", "method=gpu"]])
+def test_cli_method_pdhg_on_crude_blending(tmp_path, args):
+    # data/refinery/MRPL_Crude_Blending_LP: optimum 22171.59777424483 (.sol:2)
+    g = GOLD["crude_blending"]
+    lib = _sov(_need("libsov.so"))
+    env = lib.sov_env_create()
+    m = lib.sov_model_create(env, b"MRPL_Crude_Blending_LP")
+    _build_model(lib, m, G.lp_from(g["lp_internal_min"]), g["sense"])
+    path = str(tmp_path / "crude.mps")
+    assert lib.sov_write_mps(m, path.encode()) == 0
+    lib.sov_model_free(m)
+    lib.sov_env_free(env)
+    sol = str(tmp_path / "crude.sol")
+    r = subprocess.run([_need("sovsolve"), path, *args, "--sol", sol], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "PDHG" in r.stdout
+    obj = float(re.search(r"Objective:\s+([-0-9.eE+]+)", r.stdout).group(1))
+    assert abs(obj - g["sol_objective"]) / g["sol_objective"] <= 1e-6
+    assert "PASS=YES" in r.stdout
