@@ -9,6 +9,10 @@ instances of include/nir_lpgen.h; the reference publishes no dataset):
   c2  ZIPF 200,000 x 500,000, ~5M nonzeros, mixed precision (default)
   c1  RANDOM_EQ 2,000 x 5,000, 40,000 nonzeros
   c5  BADLY_SCALED 50,000 x 120,000, ~1M nonzeros
+  c3  256 MULTIPERIOD instances, m log-uniform in [500, 20,000], n = 2.5 m
+      (~1.3M rows, ~3.3M columns, ~33M nonzeros in total), solved as one
+      batch (nir_pdhg_batch_solve); with --gpus N the instances are sharded
+      over the ranks (strong scaling, no data-path collective)
 
 `value` is the time to tolerance with the LP already resident in HBM
 (handle created before the timed region); `e2e` is the same metric through
@@ -45,7 +49,20 @@ WORKLOADS = {
     "c2": dict(kind=2, seed=1, kw={}, label="zipf_200000x500000_nnz5M", precision=1),
     "c1": dict(kind=1, seed=1, kw={}, label="random_eq_2000x5000_nnz40000", precision=1),
     "c5": dict(kind=5, seed=1, kw={}, label="badly_scaled_50000x120000_nnz1M", precision=1),
+    "c3": dict(kind=3, seed=1000, kw={}, label="multiperiod_batch256_m500-20000", precision=1, batch=256),
 }
+
+
+def batch_instances(wl):
+    """The c3 batch: instance i is MULTIPERIOD seed (seed + i) with m drawn
+    log-uniformly from [500, 20000] by a seeded generator."""
+    import numpy as np
+
+    from nirnaya_b200 import lp as L
+
+    rng = np.random.default_rng(wl["seed"])
+    ms = np.exp(rng.uniform(np.log(500), np.log(20000), wl["batch"])).astype(int)
+    return [L.generate(wl["kind"], wl["seed"] + i, m=int(m)) for i, m in enumerate(ms)]
 
 
 def peaks():
@@ -286,6 +303,138 @@ def cpu_baseline(lp, label, seconds=15.0, threads=None):
                 iterations_per_s=it_s, lower_bound=bool(lower))
 
 
+def run_batch_ours(args, rank, world, local):
+    """c3: this rank's shard of the 256 instances as one batch."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from nirnaya_b200 import batch as B
+    from nirnaya_b200 import pdhg
+    from nirnaya_b200.lp import NirLpView
+
+    wl = WORKLOADS[args.workload]
+    lps = batch_instances(wl)
+    mine = B.shard_instances([lp.nnz for lp in lps], world)[rank]
+    sub = [lps[i] for i in mine]
+    params = pdhg.default_params(precision=wl["precision"], tol=1e-6, max_iters=args.max_iters)
+    flush = torch.empty(2 * L2_BYTES, dtype=torch.uint8, device=f"cuda:{local}")
+    eng = B.BatchEngine(sub, local)
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        eng.solve(params)
+    barrier(world)
+    launches = 0
+    with ClockSampler(local) as clk:
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record()
+        for _ in range(args.steps):
+            flush.fill_(1)
+            res, total = eng.solve(params)
+            launches += total.kernel_launches
+        b.record()
+        torch.cuda.synchronize()
+    ms = allmax(a.elapsed_time(b) / args.steps, world)
+    eng.close()
+    # end to end: create (host->device copy, transpose), solve, copy out, free
+    views = (NirLpView * len(sub))(*[lp.view() for lp in sub])
+    n = sum(lp.ncol for lp in sub)
+    m = sum(lp.nrow for lp in sub)
+    e2e_s = []
+    L = B._lib()
+    for _ in range(max(1, min(args.steps, 2))):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        h = C.c_void_p()
+        if L.nir_pdhg_batch_create(views, len(sub), local, C.byref(h)) != 0:
+            raise RuntimeError(pdhg.last_error())
+        x = np.zeros(n)
+        y = np.zeros(m)
+        infos = (pdhg.Info * len(sub))()
+        tot = pdhg.Info()
+        L.nir_pdhg_batch_solve(h, C.byref(params), pdhg.POLL_FN(0), None, pdhg._dptr(x), pdhg._dptr(y), infos,
+                               C.byref(tot))
+        L.nir_pdhg_batch_free(h)
+        e2e_s.append(time.perf_counter() - t0)
+    e2e = allmax(statistics.median(e2e_s), world)
+    per = [dict(status=r[2].status, iterations=r[2].iterations, rel_kkt=r[2].rel_kkt) for r in res]
+    # algorithmic bytes of the iterations actually run: per instance and
+    # iteration, one FP32 pass over A' and one over A (index + value per
+    # nonzero, row pointers, the gathered vector and the epilogue vectors)
+    alg = 0.0
+    for lp, r in zip(sub, per):
+        alg += r["iterations"] * (16.0 * lp.nnz + 4 * 9 * lp.ncol + 4 * 8 * lp.nrow)
+    return dict(ms=ms, per=per, launches=launches, e2e=e2e, clocks=clk.summary(), alg=alg,
+                h2d=sum(lp.host_bytes() for lp in sub), d2h=8 * (n + m), rows=m, cols=n,
+                nnz=sum(lp.nnz for lp in sub), count=len(sub))
+
+
+def batch_line(args, r, world):
+    peak, peak_kind = peaks()
+    alg_total = allmax(r["alg"], 1)
+    achieved = alg_total / (r["ms"] * 1e-3) / 1e9
+    per = r["per"]
+    return {
+        "metric": METRIC,
+        "value": r["ms"] / 1000.0,
+        "unit": "s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": r["ms"],
+        "higher_is_better": False,
+        "scaling": "strong",
+        "vs_baseline": None,
+        "dtype": "f32+f64",
+        "data": "synthetic (seeded generator, include/nir_lpgen.h)",
+        "config": {"workload": WORKLOADS["c3"]["label"], "instances": 256, "instances_rank0": r["count"],
+                   "rows_rank0": r["rows"], "cols_rank0": r["cols"], "nnz_rank0": r["nnz"], "tol": 1e-6,
+                   "algorithm": "pdlp batch (per-instance restarts, primal weight and stop)",
+                   "precision": "mixed (fp32 + fp64 polish)",
+                   "parallelism": f"instance shards x{world}" if world > 1 else "single gpu",
+                   "l2": "flushed (2x L2 write) before every solve; the batch (~0.5 GB of matrix) exceeds L2"},
+        "instances_per_s": 256 / (r["ms"] / 1000.0) if world == 1 else None,
+        "status_counts": {str(k): sum(1 for p in per if p["status"] == k) for k in sorted({p["status"] for p in per})},
+        "iterations_max": max(p["iterations"] for p in per),
+        "iterations_median": statistics.median(p["iterations"] for p in per),
+        "rel_kkt_max": max(p["rel_kkt"] for p in per),
+        "e2e": {"value": r["e2e"], "unit": "s", "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"]},
+        "gpu_launches": r["launches"],
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None,
+                     "kernel": "whole batch loop (k_bprimal + k_bdual + checks), algorithmic bytes of the "
+                               "iterations each instance ran / solve time (rank 0)",
+                     "peak_kind": peak_kind},
+        "cpu_baseline": None,
+        "clocks": r["clocks"],
+    }
+
+
+def reference_iterations(args):
+    """Counts the reference PDHG's iterations to its own stopping rule on the
+    workload with the bit-identical GPU restatement of its loop
+    (NIR_ALGO_REFERENCE), bounded by --ref-seconds; prints one line."""
+    from nirnaya_b200 import lp as L
+    from nirnaya_b200 import pdhg
+
+    wl = WORKLOADS[args.workload]
+    lp = L.generate(wl["kind"], wl["seed"], **wl["kw"])
+    p = pdhg.default_params(algorithm=pdhg.ALGO_REFERENCE, max_iters=args.ref_iterations,
+                            time_limit=args.ref_seconds)
+    with pdhg.Engine(lp, 0) as eng:
+        t0 = time.perf_counter()
+        _, _, info = eng.solve(p)
+        dt = time.perf_counter() - t0
+    stopped = info.status == pdhg.OPTIMAL and info.iterations < args.ref_iterations
+    print(json.dumps({"workload": wl["label"], "iterations": info.iterations, "stopped_by_reference_rule": stopped,
+                      "status": pdhg.STATUS_NAMES.get(info.status), "seconds": dt,
+                      "max_rel_row_viol": info.max_rel_row_viol, "objective": info.objective}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -295,14 +444,26 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--max-iters", type=int, default=1000000)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--ref-iterations", type=int, default=0,
+                    help="count the reference loop's iterations to its stopping rule (cap), then exit")
+    ap.add_argument("--ref-seconds", type=float, default=600.0)
     ap.add_argument("--ncu-case", action="store_true",
                     help="one short solve (2 checks) of the workload for an ncu capture, then exit")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
+    if args.ref_iterations > 0:
+        reference_iterations(args)
+        return
     if args.ncu_case:
         from nirnaya_b200 import lp as L
         from nirnaya_b200 import pdhg
 
+        if wl.get("batch"):
+            from nirnaya_b200 import batch as B
+
+            with B.BatchEngine(batch_instances(wl)[:32], 0) as eng:
+                eng.solve(pdhg.default_params(precision=wl["precision"], max_iters=128, tol=0.0))
+            return
         lp = L.generate(wl["kind"], wl["seed"], **wl["kw"])
         with pdhg.Engine(lp, 0) as eng:
             eng.solve(pdhg.default_params(precision=wl["precision"], max_iters=128, tol=0.0))
@@ -314,6 +475,26 @@ def main():
             return
         from nirnaya_b200 import lp as L
 
+        if wl.get("batch"):
+            # the reference solves one model per call; its rate on the
+            # median-size instance of the batch is reported, without a time
+            # to tolerance (its iteration counts on these are not recorded)
+            lps = batch_instances(wl)
+            lp = sorted(lps, key=lambda q: q.nnz)[len(lps) // 2]
+            res = cpu_baseline(lp, wl["label"] + ":median", seconds=args.cpu_seconds)
+            if res is None:
+                print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_nirnaya.so was not built "
+                                  "from the reference sources"}))
+                return
+            print(json.dumps({"impl": "reference", "metric": METRIC, "value": None, "unit": "s",
+                              "n_gpus": args.gpus, "steps": 1, "warmup": 0, "ms_per_step": None,
+                              "higher_is_better": False, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+                              "data": "synthetic (seeded generator, include/nir_lpgen.h)",
+                              "config": {"workload": wl["label"], "tol": 1e-6, "threads": res["cores"]},
+                              "cpu_baseline": res,
+                              "e2e": {"value": None, "unit": "s", "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}))
+            return
         lp = L.generate(wl["kind"], wl["seed"], **wl["kw"])
         vals = []
         for _ in range(args.warmup):
@@ -337,6 +518,11 @@ def main():
         print(json.dumps(line))
         return
 
+    if wl.get("batch"):
+        r = run_batch_ours(args, rank, world, local)
+        if rank == 0:
+            print(json.dumps(batch_line(args, r, world)))
+        return
     r = run_ours(args, rank, world, local)
     if rank != 0:
         return

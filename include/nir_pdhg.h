@@ -87,7 +87,7 @@ typedef struct nir_pdhg_params {
     int32_t polish_stall_checks;  /* MIXED: FP64 polish after this many checks
                                      without a 0.8x improvement of the best KKT   (40)   */
     double polish_switch_kkt;     /* MIXED: ... or as soon as KKT <= this        (0)     */
-    int32_t spmv_block_nnz;       /* nonzeros per warp row block, 1..256; 0 = auto (0)   */
+    int32_t spmv_block_nnz;       /* nonzeros per warp row block, 1..256; 0 = autotuned (0) */
     int32_t use_graphs;           /* capture launch chunks in CUDA graphs        (1)     */
     int32_t verbose;              /* 1 = one line per check on stderr            (0)     */
     int32_t restart_anchor;       /* residual the restart tests compare with: 0 = first
@@ -191,6 +191,31 @@ typedef struct nir_pdhg_layout {
     int64_t device_bytes;               /* device memory held by the handle    */
 } nir_pdhg_layout;
 int nir_pdhg_get_layout(nir_pdhg* h, nir_pdhg_layout* out);
+
+/* --- batched solves ---
+ *
+ * Many LPs of uneven sizes in one handle, solved by the PDLP iteration with
+ * one launch per half-iteration for the whole batch.  The reference solves
+ * one Model per PdhgSolver::solve call (src/gpu/pdhg_solver.hpp:25); a
+ * batch replaces `count` such calls.  Every instance keeps its own step
+ * sizes, primal weight, restart state, precision phase and convergence flag
+ * on the device and stops on its own relative KKT error; converged
+ * instances drop out of the work.  In MIXED precision the instances that
+ * stall in FP32 continue in FP64 after the FP32 pass. */
+typedef struct nir_pdhg_batch nir_pdhg_batch;
+
+/* lps[0..count): the instances (host arrays, copied). */
+int nir_pdhg_batch_create(const nir_lp_view* lps, int32_t count, int device, nir_pdhg_batch** out);
+
+/* x_out / y_out receive the instances' primal / dual vectors concatenated in
+ * instance order (sum of ncol, sum of nrow doubles; may be NULL); infos[i]
+ * (may be NULL) the result of instance i; total the batch (status = the
+ * first non-optimal instance status, or OPTIMAL).  params->algorithm must be
+ * NIR_ALGO_PDLP; warm starts are not taken. */
+int nir_pdhg_batch_solve(nir_pdhg_batch* b, const nir_pdhg_params* params, int (*poll)(void* ctx), void* poll_ctx,
+                         double* x_out, double* y_out, nir_pdhg_info* infos, nir_pdhg_info* total);
+
+void nir_pdhg_batch_free(nir_pdhg_batch* b);
 
 /* --- no-allocation entry point --- */
 

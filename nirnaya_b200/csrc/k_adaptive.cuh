@@ -1,18 +1,16 @@
-// The hot path: CSR-adaptive SpMV over row blocks with the PDHG update
+// The hot path: a warp-granular CSR-adaptive SpMV with the PDHG update
 // fused into its epilogue.
 //
-// A matrix orientation (A, or the stored transpose A') is cut into row
-// blocks holding at most `cap` nonzeros and at most kBlock rows (a row
-// longer than `cap` gets a block of its own).  Block b is described by
-// blk[b] = (first row, first nonzero), so one 8-byte load gives a CUDA block
-// its whole range.  One CUDA block of kBlock threads takes one row block:
-//  * several rows: consecutive threads stream consecutive nonzeros
-//    (coalesced, 8 loads in flight per thread), form val*x[col] into shared
-//    memory while the row pointers of the block are staged next to them and
-//    every row's epilogue operands are already being fetched; after one
-//    barrier, a team of T threads (T a power of two <= 32) reduces each row
-//    by a fixed shuffle tree and its leader runs the epilogue;
-//  * one long row: all threads stride over it and a block tree reduces.
+// A matrix orientation (A, or the stored transpose A') is cut into warp row
+// blocks of at most `cap` (<= 256) nonzeros and at most 32 rows; a longer row
+// gets a block of its own.  Block b is described by blk[b] = (first row,
+// first nonzero), so one 8-byte load gives a warp its whole range.
+// Persistent warps walk their blocks with register double buffering (the
+// next block's index/value stream is in flight while the current one is
+// gathered and reduced); within a block the lanes stream consecutive
+// nonzeros (coalesced), gather x, leave the products in the warp's shared
+// slice, and teams of lanes reduce each row by a fixed shuffle tree before
+// the team leader runs the epilogue.  No block-wide barrier is involved.
 // The reduction order depends only on the layout, so results are
 // deterministic run to run, and no atomics are used.  Each epilogue reads
 // and writes only its own row's vector entries, so the update of x (or y)
@@ -25,14 +23,13 @@
 #pragma once
 
 #include "dev_common.cuh"
+#include "row_blocks.hpp"
 
 namespace nir {
 
 // ---------------------------------------------------------------- core
 
-constexpr int kWarpU = 8;                    // nonzeros per lane per round
-constexpr int kWarpCapMax = 32 * kWarpU;     // largest warp row block (256)
-constexpr int kRowsPerWarpBlock = 32;        // rows in one warp row block
+// kWarpU, kWarpCapMax and kRowsPerWarpBlock: row_blocks.hpp
 
 // Dynamic shared memory of an iteration kernel: one product slice per warp.
 template <typename TA>
@@ -521,29 +518,26 @@ struct CtlArgs {
 
 constexpr int kHist = 4096;
 
-__global__ void __launch_bounds__(kBlock) k_control(CtlArgs a, DevState* st) {
-    __shared__ double sh[kWarps];
-    if (st->done || st->phase != a.phase) return;
-    const double dx2 = block_sum_array(a.partP, a.nP, sh);
-    const double dxa2 = block_sum_array(a.partP + a.nP, a.nP, sh);
-    const double dy2 = block_sum_array(a.partD, a.nD, sh);
-    const double dya2 = block_sum_array(a.partD + a.nD, a.nD, sh);
-    const double pres2 = block_sum_array(a.partKR, a.nKR, sh);
-    const double dobj_r = block_sum_array(a.partKR + a.nKR, a.nKR, sh);
-    const double ywrong2 = block_sum_array(a.partKR + 2 * a.nKR, a.nKR, sh);
-    const double maxrel = block_max_array(a.partKR + 3 * a.nKR, a.nKR, sh);
-    const double dres2 = block_sum_array(a.partKC, a.nKC, sh);
-    const double dobj_c = block_sum_array(a.partKC + a.nKC, a.nKC, sh);
-    const double pobj_c = block_sum_array(a.partKC + 2 * a.nKC, a.nKC, sh);
-    const double xviol2 = block_sum_array(a.partKC + 3 * a.nKC, a.nKC, sh);
-    if (threadIdx.x != 0) return;
+// The scalar part of a check (thread 0 only): relative KKT in the original
+// space, termination, FP32->FP64 hand-over, fixed-point-residual restart
+// test and primal-weight update.  Shared by the single-LP controller and
+// the per-instance batch controller.
+struct CtlSums {
+    double dx2, dxa2, dy2, dya2, pres2, dobj_r, ywrong2, maxrel, dres2, dobj_c, pobj_c, xviol2;
+};
+
+__device__ void control_update(const CtlArgs& a, DevState* st, const CtlSums& sums, double bnorm, double cnorm,
+                               double offset, double* hist) {
+    const double dx2 = sums.dx2, dxa2 = sums.dxa2, dy2 = sums.dy2, dya2 = sums.dya2;
+    const double pres2 = sums.pres2, dobj_r = sums.dobj_r, ywrong2 = sums.ywrong2, maxrel = sums.maxrel;
+    const double dres2 = sums.dres2, dobj_c = sums.dobj_c, pobj_c = sums.pobj_c, xviol2 = sums.xviol2;
 
     const long long it = st->iter + a.K;
     st->iter = it;
-    const double pobj = pobj_c + a.offset;
-    const double dobj = dobj_r + dobj_c + a.offset;
-    const double kp = sqrt(pres2 + xviol2) / (1.0 + a.bnorm);
-    const double kd = sqrt(dres2 + ywrong2) / (1.0 + a.cnorm);
+    const double pobj = pobj_c + offset;
+    const double dobj = dobj_r + dobj_c + offset;
+    const double kp = sqrt(pres2 + xviol2) / (1.0 + bnorm);
+    const double kd = sqrt(dres2 + ywrong2) / (1.0 + cnorm);
     const double kg = fabs(pobj - dobj) / (1.0 + fabs(pobj) + fabs(dobj));
     const double kkt = fmax(kp, fmax(kd, kg));
     const double omega = st->omega;
@@ -558,8 +552,8 @@ __global__ void __launch_bounds__(kBlock) k_control(CtlArgs a, DevState* st) {
     st->res = res;
     st->kkt_iter = it;
     st->apply_restart = 0;
-    {
-        double* h = a.hist + 8 * ((it / a.K) % kHist);
+    if (hist) {
+        double* h = hist + 8 * ((it / a.K) % kHist);
         h[0] = double(it);
         h[1] = kkt;
         h[2] = kp;
@@ -643,6 +637,27 @@ __global__ void __launch_bounds__(kBlock) k_control(CtlArgs a, DevState* st) {
     } else {
         st->k_base = k_after;
     }
+}
+
+
+__global__ void __launch_bounds__(kBlock) k_control(CtlArgs a, DevState* st) {
+    __shared__ double sh[kWarps];
+    if (st->done || st->phase != a.phase) return;
+    const double dx2 = block_sum_array(a.partP, a.nP, sh);
+    const double dxa2 = block_sum_array(a.partP + a.nP, a.nP, sh);
+    const double dy2 = block_sum_array(a.partD, a.nD, sh);
+    const double dya2 = block_sum_array(a.partD + a.nD, a.nD, sh);
+    const double pres2 = block_sum_array(a.partKR, a.nKR, sh);
+    const double dobj_r = block_sum_array(a.partKR + a.nKR, a.nKR, sh);
+    const double ywrong2 = block_sum_array(a.partKR + 2 * a.nKR, a.nKR, sh);
+    const double maxrel = block_max_array(a.partKR + 3 * a.nKR, a.nKR, sh);
+    const double dres2 = block_sum_array(a.partKC, a.nKC, sh);
+    const double dobj_c = block_sum_array(a.partKC + a.nKC, a.nKC, sh);
+    const double pobj_c = block_sum_array(a.partKC + 2 * a.nKC, a.nKC, sh);
+    const double xviol2 = block_sum_array(a.partKC + 3 * a.nKC, a.nKC, sh);
+    if (threadIdx.x != 0) return;
+    const CtlSums sums{dx2, dxa2, dy2, dya2, pres2, dobj_r, ywrong2, maxrel, dres2, dobj_c, pobj_c, xviol2};
+    control_update(a, st, sums, a.bnorm, a.cnorm, a.offset, a.hist);
 }
 
 // Restart: the anchor and the iterate become (x+, y+).

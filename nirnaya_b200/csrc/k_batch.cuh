@@ -1,0 +1,297 @@
+// Batched PDLP: many LPs of uneven sizes in one launch per half-iteration.
+//
+// The instances are laid out block-diagonally in one handle: instance i
+// owns rows [row_off[i], row_off[i+1]) and columns [col_off[i],
+// col_off[i+1]), and its warp row blocks (which never cross an instance)
+// are contiguous.  Every instance keeps its own DevState on the device:
+// step sizes, primal weight, Halpern counter, restart anchor, precision
+// phase and convergence flag.  The iteration kernels look up the instance
+// of each warp row block, skip converged instances, and in a check launch
+// leave one partial sum per quantity and block; the controller then runs
+// one CTA per instance, reducing that instance's block range in a fixed
+// order (deterministic) and applying the same update as the single-LP
+// controller.
+#pragma once
+
+#include "k_adaptive.cuh"
+
+namespace nir {
+
+struct BatchArgs {
+    const int2* blk;
+    int nblk;
+    int cap;
+    const int* rp;
+    const int* ci;
+    const int* blk_inst;  // instance of each warp row block
+    double* part;         // per-block partials: part[q * nblk + block]
+    const DevState* inst;
+    int i_in_chunk;
+    int halpern;
+    int phase;
+    double rho;
+};
+
+__device__ __forceinline__ bool inst_active(const DevState& s, int phase) { return !s.done && s.phase == phase; }
+
+template <class Epi>
+__device__ __forceinline__ void flush_block_partials(Epi& epi, double* __restrict__ part, int nblk, int b) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int q = 0; q < Epi::NQ; ++q) {
+        const double v = (Epi::kLastIsMax && q == Epi::NQ - 1) ? warp_max(epi.q[q]) : warp_sum(epi.q[q]);
+        if (lane == 0) part[q * nblk + b] = v;
+        epi.q[q] = 0.0;
+    }
+}
+
+// rowblock_spmv over the batch: per block, the instance decides whether the
+// block runs and with which scalars (SetFn(epi, DevState&)).
+template <typename TA, typename TV, typename TX, class Epi, class SetFn>
+__device__ __forceinline__ void rowblock_spmv_batch(const BatchArgs& a, const TV* __restrict__ val,
+                                                    const TX* __restrict__ x, Epi& epi, SetFn set) {
+    extern __shared__ __align__(16) unsigned char nir_smem[];
+    const int w = threadIdx.x >> 5;
+    TA* s_prod = reinterpret_cast<TA*>(nir_smem) + w * kWarpCapMax;
+    const int G = gridDim.x * kWarps;
+    int b = blockIdx.x * kWarps + w;
+    if (b >= a.nblk) return;
+    int2 d0 = __ldg(a.blk + b), d1 = __ldg(a.blk + b + 1);
+    int inst = __ldg(a.blk_inst + b);
+    bool act = inst_active(a.inst[inst], a.phase);
+    int c[kWarpU];
+    TV v[kWarpU];
+    stream_load<TV>(d0, d1, act ? a.cap : -1, a.ci, val, c, v);
+    for (;;) {
+        const int bn = b + G;
+        const bool has_next = bn < a.nblk;
+        int2 n0 = make_int2(0, 0), n1 = make_int2(0, 0);
+        int inst_n = 0;
+        bool act_n = false;
+        if (has_next) {
+            n0 = __ldg(a.blk + bn);
+            n1 = __ldg(a.blk + bn + 1);
+            inst_n = __ldg(a.blk_inst + bn);
+            act_n = inst_active(a.inst[inst_n], a.phase);
+        }
+        int cn[kWarpU];
+        TV vn[kWarpU];
+        stream_load<TV>(n0, n1, act_n ? a.cap : -1, a.ci, val, cn, vn);
+        if (act) {
+            set(epi, a.inst[inst]);
+            warp_process<TA, TV, TX>(d0, d1, a.cap, a.rp, a.ci, val, x, epi, s_prod, c, v);
+            if (Epi::NQ > 0) flush_block_partials(epi, a.part, a.nblk, b);
+        }
+        if (!has_next) break;
+#pragma unroll
+        for (int q = 0; q < kWarpU; ++q) {
+            c[q] = cn[q];
+            v[q] = vn[q];
+        }
+        d0 = n0;
+        d1 = n1;
+        inst = inst_n;
+        act = act_n;
+        b = bn;
+    }
+}
+
+template <typename T, bool CHECK>
+__global__ void __launch_bounds__(kBlock) k_bprimal(BatchArgs a, const T* __restrict__ val, const T* __restrict__ y,
+                                                    T* __restrict__ x, T* __restrict__ xbar, T* __restrict__ xplus,
+                                                    const T* __restrict__ c, const T* __restrict__ lo,
+                                                    const T* __restrict__ up, const T* __restrict__ x0) {
+    PrimalEpi<T, CHECK> epi;
+    epi.x = x;
+    epi.xbar = xbar;
+    epi.xplus = xplus;
+    epi.c = c;
+    epi.lo = lo;
+    epi.up = up;
+    epi.x0 = x0;
+    epi.halpern = a.halpern;
+    rowblock_spmv_batch<T, T, T>(a, val, y, epi, [&](PrimalEpi<T, CHECK>& e, const DevState& s) {
+        e.s = step_scalars<T>(&s, a.i_in_chunk, a.halpern, a.rho);
+    });
+}
+
+template <typename T, bool CHECK>
+__global__ void __launch_bounds__(kBlock) k_bdual(BatchArgs a, const T* __restrict__ val, const T* __restrict__ xbar,
+                                                  T* __restrict__ y, T* __restrict__ yplus, const T* __restrict__ rl,
+                                                  const T* __restrict__ ru, const T* __restrict__ y0) {
+    DualEpi<T, CHECK> epi;
+    epi.y = y;
+    epi.yplus = yplus;
+    epi.rl = rl;
+    epi.ru = ru;
+    epi.y0 = y0;
+    epi.halpern = a.halpern;
+    rowblock_spmv_batch<T, T, T>(a, val, xbar, epi, [&](DualEpi<T, CHECK>& e, const DevState& s) {
+        e.s = step_scalars<T>(&s, a.i_in_chunk, a.halpern, a.rho);
+    });
+}
+
+template <typename TX>
+__global__ void __launch_bounds__(kBlock) k_bkkt_rows(BatchArgs a, const double* __restrict__ val,
+                                                      const TX* __restrict__ xplus, const TX* __restrict__ yplus,
+                                                      const double* __restrict__ dr, const double* __restrict__ rl,
+                                                      const double* __restrict__ ru) {
+    KktRowEpi<TX> epi;
+    epi.dr = dr;
+    epi.rl = rl;
+    epi.ru = ru;
+    epi.yplus = yplus;
+    rowblock_spmv_batch<double, double, TX>(a, val, xplus, epi, [](KktRowEpi<TX>&, const DevState&) {});
+}
+
+template <typename TX>
+__global__ void __launch_bounds__(kBlock) k_bkkt_cols(BatchArgs a, const double* __restrict__ val,
+                                                      const TX* __restrict__ xplus, const TX* __restrict__ yplus,
+                                                      const double* __restrict__ dc, const double* __restrict__ c,
+                                                      const double* __restrict__ l, const double* __restrict__ u) {
+    KktColEpi<TX> epi;
+    epi.dc = dc;
+    epi.c = c;
+    epi.l = l;
+    epi.u = u;
+    epi.xplus = xplus;
+    rowblock_spmv_batch<double, double, TX>(a, val, yplus, epi, [](KktColEpi<TX>&, const DevState&) {});
+}
+
+struct BatchCtlArgs {
+    const double* partP;   // 2 x nP (A' blocks)
+    const double* partD;   // 2 x nD (A blocks)
+    const double* partKR;  // 4 x nD
+    const double* partKC;  // 4 x nP
+    int nP, nD;
+    const int* at_lo;      // instance i's A' blocks: [at_lo[i], at_lo[i+1])
+    const int* a_lo;       // instance i's A blocks:  [a_lo[i], a_lo[i+1])
+    const double* bnorm;   // per instance, original space
+    const double* cnorm;
+    const double* offset;
+};
+
+__device__ inline double range_sum(const double* __restrict__ p, int lo, int hi, double* sh) {
+    double s = 0.0;
+    for (int i = lo + threadIdx.x; i < hi; i += kBlock) s += p[i];
+    return block_sum(s, sh);
+}
+
+__device__ inline double range_max(const double* __restrict__ p, int lo, int hi, double* sh) {
+    double s = 0.0;
+    for (int i = lo + threadIdx.x; i < hi; i += kBlock) s = fmax(s, p[i]);
+    return block_max(s, sh);
+}
+
+// One CTA per instance.
+__global__ void __launch_bounds__(kBlock) k_bcontrol(CtlArgs a, BatchCtlArgs b, DevState* insts) {
+    __shared__ double sh[kWarps];
+    const int i = blockIdx.x;
+    DevState* st = insts + i;
+    if (st->done || st->phase != a.phase) return;
+    const int p0 = b.at_lo[i], p1 = b.at_lo[i + 1], d0 = b.a_lo[i], d1 = b.a_lo[i + 1];
+    CtlSums s;
+    s.dx2 = range_sum(b.partP, p0, p1, sh);
+    s.dxa2 = range_sum(b.partP + b.nP, p0, p1, sh);
+    s.dy2 = range_sum(b.partD, d0, d1, sh);
+    s.dya2 = range_sum(b.partD + b.nD, d0, d1, sh);
+    s.pres2 = range_sum(b.partKR, d0, d1, sh);
+    s.dobj_r = range_sum(b.partKR + b.nD, d0, d1, sh);
+    s.ywrong2 = range_sum(b.partKR + 2 * b.nD, d0, d1, sh);
+    s.maxrel = range_max(b.partKR + 3 * b.nD, d0, d1, sh);
+    s.dres2 = range_sum(b.partKC, p0, p1, sh);
+    s.dobj_c = range_sum(b.partKC + b.nP, p0, p1, sh);
+    s.pobj_c = range_sum(b.partKC + 2 * b.nP, p0, p1, sh);
+    s.xviol2 = range_sum(b.partKC + 3 * b.nP, p0, p1, sh);
+    if (threadIdx.x != 0) return;
+    control_update(a, st, s, b.bnorm[i], b.cnorm[i], b.offset[i], nullptr);
+}
+
+template <typename T>
+__global__ void k_bapply_restart(int n, int m, const int* __restrict__ col_inst, const int* __restrict__ row_inst,
+                                 const DevState* __restrict__ insts, int phase, T* __restrict__ x, T* __restrict__ x0,
+                                 const T* __restrict__ xplus, T* __restrict__ y, T* __restrict__ y0,
+                                 const T* __restrict__ yplus) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) {
+        const DevState& s = insts[col_inst[t]];
+        if (s.apply_restart && !s.done && s.phase == phase) {
+            const T v = xplus[t];
+            x[t] = v;
+            x0[t] = v;
+        }
+    }
+    if (t < m) {
+        const DevState& s = insts[row_inst[t]];
+        if (s.apply_restart && !s.done && s.phase == phase) {
+            const T v = yplus[t];
+            y[t] = v;
+            y0[t] = v;
+        }
+    }
+}
+
+// Batch status for the host: done = every instance finished, phase = 1
+// once no instance is still running in phase 0.
+__global__ void k_bsnap(int count, const DevState* __restrict__ insts, HostSnap* __restrict__ ring,
+                        long long* __restrict__ seq) {
+    __shared__ double sh[kWarps];
+    double ndone = 0.0, nphase0 = 0.0, maxit = 0.0;
+    for (int i = threadIdx.x; i < count; i += kBlock) {
+        const DevState& s = insts[i];
+        ndone += s.done ? 1.0 : 0.0;
+        nphase0 += (!s.done && s.phase == 0) ? 1.0 : 0.0;
+        maxit = fmax(maxit, double(s.iter));
+    }
+    ndone = block_sum(ndone, sh);
+    nphase0 = block_sum(nphase0, sh);
+    maxit = block_max(maxit, sh);
+    if (threadIdx.x != 0) return;
+    const long long s = *seq + 1;
+    *seq = s;
+    HostSnap h{};
+    h.seq = s;
+    h.iter = (long long)maxit;
+    h.done = (int(ndone) == count) ? 1 : 0;
+    h.phase = (int(nphase0) == 0) ? 1 : 0;
+    h.restarts = int(ndone);
+    ring[s % kSnapRing] = h;
+    __threadfence_system();
+}
+
+// Per-instance norms over contiguous ranges (power iteration).
+__global__ void k_seg_norm(const int* __restrict__ off, const double* __restrict__ w, double* __restrict__ norm) {
+    __shared__ double sh[kWarps];
+    const int i = blockIdx.x;
+    double s = 0.0;
+    for (int j = off[i] + threadIdx.x; j < off[i + 1]; j += kBlock) s += w[j] * w[j];
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) norm[i] = sqrt(s);
+}
+
+__global__ void k_seg_scale(int n, const int* __restrict__ inst_of, const double* __restrict__ norm,
+                            double* __restrict__ w) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const double d = norm[inst_of[j]];
+    w[j] = d > 0.0 ? w[j] / d : 0.0;
+}
+
+// Output of a batch: each instance from the precision it ended in.
+__global__ void k_bunscale_out(int n, int m, const int* __restrict__ col_inst, const int* __restrict__ row_inst,
+                               const DevState* __restrict__ insts, const float* __restrict__ xp32,
+                               const float* __restrict__ yp32, const double* __restrict__ xp64,
+                               const double* __restrict__ yp64, int all64, const double* __restrict__ dc,
+                               const double* __restrict__ dr, double* __restrict__ xo, double* __restrict__ yo) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) {
+        const bool f64 = all64 || insts[col_inst[t]].phase == 1;
+        xo[t] = (f64 ? xp64[t] : double(xp32[t])) * dc[t];
+    }
+    if (t < m) {
+        const bool f64 = all64 || insts[row_inst[t]].phase == 1;
+        yo[t] = (f64 ? yp64[t] : double(yp32[t])) * dr[t];
+    }
+}
+
+}  // namespace nir

@@ -152,15 +152,28 @@ __global__ void k_scale_vectors(int n, int m, const double* __restrict__ c, cons
 
 // ---------------------------------------------------------------- power iteration
 
-// Deterministic pseudo-random start in [0.5, 1.5).
-__global__ void k_power_start(int n, double* __restrict__ u) {
-    int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n) return;
-    unsigned long long z = (unsigned long long)j * 0x9e3779b97f4a7c15ULL + 0x632be59bd9b4e019ULL;
+// Deterministic pseudo-random start in [0.5, 1.5) (splitmix64 of the index).
+__device__ __forceinline__ double power_start_value(unsigned long long j) {
+    unsigned long long z = j * 0x9e3779b97f4a7c15ULL + 0x632be59bd9b4e019ULL;
     z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
     z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
     z ^= z >> 31;
-    u[j] = 0.5 + double(z >> 11) * 0x1.0p-53;
+    return 0.5 + double(z >> 11) * 0x1.0p-53;
+}
+
+__global__ void k_power_start(int n, double* __restrict__ u) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    u[j] = power_start_value(j);
+}
+
+// Batch start: each instance's columns from its own index 0, so an
+// instance's estimate does not depend on the batch around it.
+__global__ void k_power_start_batch(int n, const int* __restrict__ col_inst, const int* __restrict__ col_off,
+                                    double* __restrict__ u) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    u[j] = power_start_value(j - col_off[col_inst[j]]);
 }
 
 // One warp per row FP64 SpMV (setup only).

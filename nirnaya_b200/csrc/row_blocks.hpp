@@ -1,0 +1,93 @@
+// Warp row-block layout of a CSR orientation (host only).
+//
+// A descriptor list blk[0..nblk] holds (first row, first nonzero) of every
+// warp row block plus an end entry (rows, nnz).  A block either packs at
+// most kRowsPerWarpBlock consecutive rows whose nonzeros total at most
+// `cap` (<= kWarpCapMax), or holds one row of any length.  The iteration
+// kernels stage a packed block's products in a kWarpCapMax-entry shared
+// slice per warp, so these invariants are what keeps them in bounds:
+// check_row_blocks verifies them before any list is uploaded.
+#pragma once
+
+#include <vector_types.h>
+
+#include <algorithm>
+#include <stdexcept>
+#include <vector>
+
+namespace nir {
+
+constexpr int kWarpU = 8;                    // nonzeros per lane per round
+constexpr int kWarpCapMax = 32 * kWarpU;     // largest warp row block (256)
+constexpr int kRowsPerWarpBlock = 32;        // rows in one warp row block
+
+// Greedy packing of consecutive rows; rp[0] may be any offset.
+inline std::vector<int2> build_row_blocks(const std::vector<int>& rp, int cap) {
+    const int rows = int(rp.size()) - 1;
+    std::vector<int2> blk;
+    if (rows <= 0) {
+        const int p = rp.empty() ? 0 : rp[0];
+        blk.push_back(int2{0, p});
+        blk.push_back(int2{0, p});
+        return blk;
+    }
+    blk.push_back(int2{0, rp[0]});
+    int s = 0;
+    while (s < rows) {
+        int r = s + 1;
+        if (rp[s + 1] - rp[s] <= cap) {
+            while (r < rows && rp[r + 1] - rp[s] <= cap && r - s < kRowsPerWarpBlock) ++r;
+        }
+        blk.push_back(int2{r, rp[r]});
+        s = r;
+    }
+    return blk;
+}
+
+inline void check_row_blocks(const std::vector<int2>& b, const std::vector<int>& rp, int cap) {
+    const int rows = int(rp.size()) - 1;
+    if (cap < 1 || cap > kWarpCapMax) throw std::runtime_error("internal: row block capacity out of range");
+    if (b.size() < 2 || b.front().x != 0 || b.back().x != std::max(rows, 0))
+        throw std::runtime_error("internal: row blocks do not cover the rows");
+    for (size_t k = 0; k + 1 < b.size(); ++k) {
+        const int r0 = b[k].x, r1 = b[k + 1].x, p0 = b[k].y, p1 = b[k + 1].y;
+        if (rows <= 0) {
+            if (r0 != 0 || r1 != 0 || p0 != p1) throw std::runtime_error("internal: malformed empty row block");
+            continue;
+        }
+        if (!(r0 < r1 && r1 <= rows) || p0 != rp[r0] || p1 != rp[r1])
+            throw std::runtime_error("internal: malformed row block descriptor");
+        if (!(r1 - r0 == 1 || (p1 - p0 <= cap && r1 - r0 <= kRowsPerWarpBlock)))
+            throw std::runtime_error("internal: row block exceeds its capacity");
+    }
+}
+
+// Row blocks of a block-diagonal batch: instance i owns rows
+// [off[i], off[i+1]) of rp, and no block crosses an instance.  Also returns
+// the instance of every block (owner) and each instance's first block
+// (lo[i], with lo[count] = number of blocks).
+inline std::vector<int2> build_batch_row_blocks(const std::vector<int>& rp, const std::vector<int>& off, int cap,
+                                                std::vector<int>* owner, std::vector<int>* lo) {
+    const int count = int(off.size()) - 1;
+    std::vector<int2> all;
+    owner->clear();
+    lo->clear();
+    for (int i = 0; i < count; ++i) {
+        lo->push_back(int(all.size()));
+        if (off[i + 1] == off[i]) continue;  // no rows of this orientation
+        std::vector<int> seg(rp.begin() + off[i], rp.begin() + off[i + 1] + 1);
+        const std::vector<int2> b = build_row_blocks(seg, cap);  // rows relative to the instance
+        for (size_t k = 0; k + 1 < b.size(); ++k) {
+            all.push_back(int2{b[k].x + off[i], b[k].y});
+            owner->push_back(i);
+        }
+    }
+    lo->push_back(int(all.size()));
+    const int rows = int(rp.size()) - 1;
+    if (all.empty()) all.push_back(int2{0, rp.empty() ? 0 : rp[0]});  // one empty block, as for a single LP
+    all.push_back(int2{std::max(rows, 0), rows >= 0 ? rp[rows] : 0});
+    check_row_blocks(all, rp, cap);
+    return all;
+}
+
+}  // namespace nir

@@ -84,7 +84,7 @@ EXPORTED = [
     "nir_pdhg_default_params", "nir_pdhg_create", "nir_pdhg_update_vectors", "nir_pdhg_solve",
     "nir_pdhg_solve_lp", "nir_pdhg_free", "nir_pdhg_last_error", "nir_pdhg_spmv", "nir_pdhg_time_spmv",
     "nir_pdhg_set_profiling", "nir_pdhg_kernel_times", "nir_pdhg_get_layout", "nir_pdhg_history",
-    "nir_pdhg_reference_solve_noalloc",
+    "nir_pdhg_reference_solve_noalloc", "nir_pdhg_batch_create", "nir_pdhg_batch_solve", "nir_pdhg_batch_free",
 ]
 
 _lib = None
