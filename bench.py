@@ -160,17 +160,20 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def fused_primal_bytes(lp, nblk):
-    """Algorithmic bytes of one launch of the fused A'y SpMV + primal update
-    in FP32: index+value per nonzero, row pointers and row-block starts, y read
-    once, x/c/l/u/x0 read and x/xbar written once."""
+def primal_bytes(lp, w):
+    """Algorithmic bytes of one fused A'y + primal-update launch, counted
+    unfused: the CSR SpMV of A' (n rows; w-byte values, 4-byte indices and
+    row pointers, y read once, A'y written once) plus the primal update
+    (x, c, l, u, A'y read, x and x-bar written), w = 4 (FP32) or 8 (FP64)."""
     n, m, nnz = lp.ncol, lp.nrow, lp.nnz
-    return 8 * nnz + 4 * (n + 1) + 4 * (nblk + 1) + 4 * m + 4 * 5 * n + 4 * 2 * n
+    return (4 + w) * nnz + 4 * (n + 1) + w * m + w * n + 7 * w * n
 
 
-def fused_dual_bytes(lp, nblk):
+def dual_bytes(lp, w):
+    """Same for the fused A x-bar + dual-update launch: SpMV of A (m rows)
+    plus the dual update (y, A x-bar, row bounds read, y written)."""
     n, m, nnz = lp.ncol, lp.nrow, lp.nnz
-    return 8 * nnz + 4 * (m + 1) + 4 * (nblk + 1) + 4 * n + 4 * 4 * m + 4 * 1 * m
+    return (4 + w) * nnz + 4 * (m + 1) + w * n + w * m + 5 * w * m
 
 
 def spmv_bytes(lp, transpose, word):
@@ -448,7 +451,10 @@ def main():
                     help="count the reference loop's iterations to its stopping rule (cap), then exit")
     ap.add_argument("--ref-seconds", type=float, default=600.0)
     ap.add_argument("--ncu-case", action="store_true",
-                    help="one short solve (2 checks) of the workload for an ncu capture, then exit")
+                    help="one short solve (--ncu-iters iterations) of the workload for an ncu capture, then exit")
+    ap.add_argument("--ncu-iters", type=int, default=1024)
+    ap.add_argument("--ncu-precision", choices=["fp64", "mixed", "fp32"], default=None,
+                    help="iterate precision of the ncu case (default: the workload's)")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     if args.ref_iterations > 0:
@@ -458,15 +464,18 @@ def main():
         from nirnaya_b200 import lp as L
         from nirnaya_b200 import pdhg
 
+        if args.ncu_precision:
+            wl = dict(wl, precision={"fp64": 0, "mixed": 1, "fp32": 2}[args.ncu_precision])
+
         if wl.get("batch"):
             from nirnaya_b200 import batch as B
 
             with B.BatchEngine(batch_instances(wl)[:32], 0) as eng:
-                eng.solve(pdhg.default_params(precision=wl["precision"], max_iters=128, tol=0.0))
+                eng.solve(pdhg.default_params(precision=wl["precision"], max_iters=args.ncu_iters, tol=0.0))
             return
         lp = L.generate(wl["kind"], wl["seed"], **wl["kw"])
         with pdhg.Engine(lp, 0) as eng:
-            eng.solve(pdhg.default_params(precision=wl["precision"], max_iters=128, tol=0.0))
+            eng.solve(pdhg.default_params(precision=wl["precision"], max_iters=args.ncu_iters, tol=0.0))
         return
     rank, world, local = dist_setup(args.gpus)
 
@@ -530,9 +539,23 @@ def main():
     last = infos[-1]
     peak, peak_kind = peaks()
     kt, lay = r["kt"], r["lay"]
-    ach_bytes = fused_primal_bytes(lp, lay.blocks_at)
-    achieved = ach_bytes / (kt.primal_us * 1e-6) / 1e9 if kt.primal_us > 0 else None
-    traffic = committed_traffic(f"fused_primal_f32:{wl['label']}")
+    # dominant kernel of the solve: mean launch time x launches, per kernel
+    # and iterate precision (FP32 chunks, FP64 chunks)
+    it64 = last["iterations_fp64"]
+    it32 = last["iterations"] - it64
+    kernels = {}
+    for q, (tag, w, its) in enumerate((("f32", 4, it32), ("f64", 8, it64))):
+        if kt.samples[q] == 0 or its == 0:
+            continue
+        for kname, us, alg in (("k_primal", kt.primal_us[q], primal_bytes(lp, w)),
+                               ("k_dual", kt.dual_us[q], dual_bytes(lp, w))):
+            kernels[f"{kname}<{'float' if w == 4 else 'double'}>"] = {
+                "launch_us": us, "launches": its, "share_s": us * its * 1e-6,
+                "algorithmic_bytes_per_launch": alg, "achieved_GBs": alg / (us * 1e-6) / 1e9,
+                "iteration_us": kt.iter_us[q], "tag": tag}
+    dom_name, dom = max(kernels.items(), key=lambda kv: kv[1]["share_s"])
+    achieved = dom["achieved_GBs"]
+    traffic = committed_traffic(f"{dom_name}:{wl['label']}")
     cpu = cpu_baseline(lp, wl["label"], seconds=args.cpu_seconds)
     line = {
         "metric": METRIC,
@@ -561,12 +584,12 @@ def main():
                 "d2h_bytes_per_step": 8 * (lp.ncol + lp.nrow)},
         "gpu_launches": r["launches"],
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                     "kernel": "k_primal<float> (fused A'y CSR-adaptive SpMV + primal update)",
-                     "algorithmic_bytes_per_launch": ach_bytes, "launch_us": kt.primal_us,
+                     "frac": achieved / peak, "traffic": traffic,
+                     "kernel": f"{dom_name} (fused CSR-adaptive SpMV + update), dominant by time in the solve",
+                     "algorithmic_bytes_per_launch": dom["algorithmic_bytes_per_launch"],
+                     "launch_us": dom["launch_us"],
                      "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
-                     "dual_kernel_us": kt.dual_us, "dual_algorithmic_bytes": fused_dual_bytes(lp, lay.blocks_a),
-                     "iteration_us": kt.iter_us,
+                     "kernels": kernels,
                      "spmv_fp32_cold_At_GBs": spmv_bytes(lp, True, 4) / (r["spmv_t_us"] * 1e-6) / 1e9,
                      "spmv_fp32_cold_A_GBs": spmv_bytes(lp, False, 4) / (r["spmv_a_us"] * 1e-6) / 1e9},
         "cpu_baseline": cpu,

@@ -165,10 +165,11 @@ int nir_pdhg_spmv(nir_pdhg* h, int transpose, int kernel, const double* x, doubl
 int nir_pdhg_time_spmv(nir_pdhg* h, int transpose, int kernel, int reps, int flush_l2, double* usec);
 
 typedef struct nir_pdhg_kernel_time {
-    double primal_us;   /* mean duration of the fused A'y + primal-update kernel */
-    double dual_us;     /* mean duration of the fused A x + dual-update kernel   */
-    double iter_us;     /* mean wall time of one iteration inside the graphs     */
-    int64_t samples;
+    /* index 0: chunks iterating in FP32, index 1: chunks iterating in FP64 */
+    double primal_us[2]; /* mean duration of the fused A'y + primal-update kernel */
+    double dual_us[2];   /* mean duration of the fused A x + dual-update kernel   */
+    double iter_us[2];   /* mean time of one iteration (kernels + check share)    */
+    int64_t samples[2];  /* timed chunks                                           */
 } nir_pdhg_kernel_time;
 
 /* Event timing of the hot kernels during the last solve (when enabled by

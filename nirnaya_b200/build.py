@@ -46,7 +46,7 @@ def _sources(pattern_dir: str, exts) -> list:
 
 def build_engine(force: bool = False, verbose: bool = False) -> str:
     target = os.path.join(HERE, "libnir_pdhg.so")
-    srcs = _sources(CSRC, (".cu", ".cuh", ".h"))
+    srcs = _sources(CSRC, (".cu", ".cuh", ".h", ".hpp"))
     if force or _stale(target, srcs):
         cmd = [_nvcc(), *NVCC_FLAGS, os.path.join(CSRC, "engine.cu"), "-o", target]
         if verbose:

@@ -534,10 +534,12 @@ struct ChunkTimer {
     cudaEvent_t e[4] = {nullptr, nullptr, nullptr, nullptr};
     bool armed = false;
     int K = 1;
+    int prec = 0;  // 0: the timed chunk iterates in FP32, 1: FP64
 };
 
 template <typename T>
 void launch_fast_chunk(nir_pdhg* h, const SolveCfg& cfg, int phase, ChunkTimer* tm) {
+    if (tm) tm->prec = (sizeof(T) == 8) ? 1 : 0;
     cudaStream_t s = h->stream;
     const PartLayout L = part_layout(h);
     const int K = cfg.K;
@@ -753,10 +755,11 @@ LoopResult run_chunks(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*),
                 if (cudaEventElapsedTime(&a, tm->e[0], tm->e[1]) == cudaSuccess &&
                     cudaEventElapsedTime(&b, tm->e[1], tm->e[2]) == cudaSuccess &&
                     cudaEventElapsedTime(&c, tm->e[0], tm->e[3]) == cudaSuccess) {
-                    h->ktime.primal_us += 1000.0 * a;
-                    h->ktime.dual_us += 1000.0 * b;
-                    h->ktime.iter_us += 1000.0 * c / std::max(1, tm->K);
-                    h->ktime.samples += 1;
+                    const int q = tm->prec;
+                    h->ktime.primal_us[q] += 1000.0 * a;
+                    h->ktime.dual_us[q] += 1000.0 * b;
+                    h->ktime.iter_us[q] += 1000.0 * c / std::max(1, tm->K);
+                    h->ktime.samples[q] += 1;
                 }
             }
             const nir::HostSnap snap = h->snap.ring[(seq0 + completed) % nir::kSnapRing];
@@ -1021,6 +1024,7 @@ int pick_cap(nir_pdhg* h, const nir_pdhg_params& p) {
     double best = 1e300;
     int arg = auto_cap(h->nnz, std::max(h->m, h->n));
     for (int cap : {32, 64, 128, 256}) {
+        if (cap > nir::kWarpCapMax) continue;
         const double t = f64 ? time_layout<double>(h, cap) : time_layout<float>(h, cap);
         if (t <= best * 1.02) {  // near-ties go to the larger capacity
             arg = cap;
@@ -1039,7 +1043,8 @@ int solve_fast(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), void* 
     const double t0 = now_sec();
     const int n = h->n, m = h->m;
     const bool pdlp = p.algorithm == NIR_ALGO_PDLP;
-    if (p.spmv_block_nnz > nir::kWarpCapMax) throw std::invalid_argument("spmv_block_nnz must be in [1, 256]");
+    if (p.spmv_block_nnz > nir::kWarpCapMax)
+        throw std::invalid_argument("spmv_block_nnz must be at most " + std::to_string(nir::kWarpCapMax));
     const int cap = pick_cap(h, p);
     set_blocks(h, h->A, cap);
     set_blocks(h, h->At, cap);
@@ -1499,10 +1504,12 @@ int nir_pdhg_set_profiling(nir_pdhg* h, int on) {
 int nir_pdhg_kernel_times(nir_pdhg* h, nir_pdhg_kernel_time* out) {
     if (!h || !out) return NIR_STATUS_INPUT_ERROR;
     *out = h->ktime;
-    if (out->samples > 0) {
-        out->primal_us /= double(out->samples);
-        out->dual_us /= double(out->samples);
-        out->iter_us /= double(out->samples);
+    for (int q = 0; q < 2; ++q) {
+        if (out->samples[q] > 0) {
+            out->primal_us[q] /= double(out->samples[q]);
+            out->dual_us[q] /= double(out->samples[q]);
+            out->iter_us[q] /= double(out->samples[q]);
+        }
     }
     return 0;
 }

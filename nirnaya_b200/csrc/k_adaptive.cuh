@@ -31,6 +31,21 @@ namespace nir {
 
 // kWarpU, kWarpCapMax and kRowsPerWarpBlock: row_blocks.hpp
 
+// Minimum resident CTAs per SM the iteration kernels are compiled for
+// (register budget 65536 / (kBlock * n)): 3 (80 registers) with 4-byte
+// values, 2 (128) with 8-byte values, both without spills.  Forcing 4 / 3
+// spilled and measured no faster on the 5M-nonzero power-law workload.
+#ifndef NIR_ITER_MINB32
+#define NIR_ITER_MINB32 3
+#endif
+#ifndef NIR_ITER_MINB64
+#define NIR_ITER_MINB64 2
+#endif
+template <typename T>
+constexpr int iter_min_blocks() {
+    return sizeof(T) == 4 ? NIR_ITER_MINB32 : NIR_ITER_MINB64;
+}
+
 // Dynamic shared memory of an iteration kernel: one product slice per warp.
 template <typename TA>
 __host__ __device__ constexpr int warp_smem_bytes() {
@@ -44,11 +59,13 @@ __device__ __forceinline__ void stream_load(int2 d0, int2 d1, int cap, const int
                                             const TV* __restrict__ val, int (&c)[kWarpU], TV (&v)[kWarpU]) {
     const int lane = threadIdx.x & 31;
     const int p0 = d0.y, nnzb = d1.y - d0.y;
-    const bool packed = nnzb <= cap;
+    // a packed block whole, or the first round of a long row; nothing for
+    // cap < 0 (a block that will not run)
+    const int lim = (cap < 0) ? 0 : min(nnzb, 32 * kWarpU);
 #pragma unroll
     for (int q = 0; q < kWarpU; ++q) {
         const int k = lane + 32 * q;
-        const bool ok = packed && k < nnzb;
+        const bool ok = k < lim;
         c[q] = ok ? __ldg(ci + p0 + k) : 0;
         v[q] = ok ? __ldg(val + p0 + k) : TV(0);
     }
@@ -75,22 +92,52 @@ __device__ __forceinline__ void warp_process(int2 d0, int2 d1, int cap, const in
     constexpr int U = kWarpU;
     typename Epi::Pre pre{};
     if (nnzb > cap) {
+        // one long row in rounds of 32*U nonzeros; the first round's stream
+        // is already in (c, v).  With 4-byte values each round's stream is
+        // requested before the previous round's gathers are consumed; with
+        // 8-byte values the extra live registers cost more occupancy than
+        // the overlap gains, so the rounds stay sequential.  Per lane the
+        // products are summed in the same order either way.
         if (lane == 0) pre = epi.prefetch(r0);
         TA s = TA(0);
+        int cc[U];
+        TV vv[U];
+#pragma unroll
+        for (int q = 0; q < U; ++q) {
+            cc[q] = c[q];
+            vv[q] = v[q];
+        }
+        constexpr bool kPipe = sizeof(TV) == 4;
         for (int base = p0 + lane; base < p1; base += 32 * U) {
-            int cc[U];
-            TV vv[U];
             TX xv[U];
 #pragma unroll
-            for (int q = 0; q < U; ++q) {
-                const int k = base + 32 * q;
-                cc[q] = (k < p1) ? __ldg(ci + k) : 0;
-                vv[q] = (k < p1) ? __ldg(val + k) : TV(0);
+            for (int q = 0; q < U; ++q) xv[q] = (base + 32 * q < p1) ? __ldg(x + cc[q]) : TX(0);
+            const int nb = base + 32 * U;
+            int cn[U];
+            TV vn[U];
+            if (kPipe) {
+#pragma unroll
+                for (int q = 0; q < U; ++q) {
+                    const int k = nb + 32 * q;
+                    cn[q] = (k < p1) ? __ldg(ci + k) : 0;
+                    vn[q] = (k < p1) ? __ldg(val + k) : TV(0);
+                }
             }
 #pragma unroll
-            for (int q = 0; q < U; ++q) xv[q] = (base + 32 * q < p1) ? __ldg(x + cc[q]) : TX(0);
-#pragma unroll
             for (int q = 0; q < U; ++q) s += TA(vv[q]) * TA(xv[q]);
+            if (!kPipe) {
+#pragma unroll
+                for (int q = 0; q < U; ++q) {
+                    const int k = nb + 32 * q;
+                    cn[q] = (k < p1) ? __ldg(ci + k) : 0;
+                    vn[q] = (k < p1) ? __ldg(val + k) : TV(0);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < U; ++q) {
+                cc[q] = cn[q];
+                vv[q] = vn[q];
+            }
         }
         s = warp_sum(s);
         if (lane == 0) epi.row(r0, s, pre);
@@ -107,8 +154,10 @@ __device__ __forceinline__ void warp_process(int2 d0, int2 d1, int cap, const in
     if (mine && tl == 0) pre = epi.prefetch(r);
     int ra = 0, re = 0;
     if (mine) {
-        ra = __ldg(rp + r) - p0;
-        re = __ldg(rp + r + 1) - p0;
+        // clamped to the staged stream: a descriptor list that does not
+        // match rp can give wrong sums but never leaves the warp's slice
+        ra = max(__ldg(rp + r) - p0, 0);
+        re = min(__ldg(rp + r + 1) - p0, nnzb);
     }
 #pragma unroll
     for (int q = 0; q < U; ++q)
@@ -197,7 +246,7 @@ struct PlainEpi {
 };
 
 template <typename TA, typename TV, typename TX>
-__global__ void __launch_bounds__(kBlock) k_spmv_adaptive(const int2* __restrict__ blk, int nblk, int cap,
+__global__ void __launch_bounds__(kBlock, iter_min_blocks<TA>()) k_spmv_adaptive(const int2* __restrict__ blk, int nblk, int cap,
                                                           const int* __restrict__ rp, const int* __restrict__ ci,
                                                           const TV* __restrict__ val, const TX* __restrict__ x,
                                                           TA* __restrict__ y) {
@@ -331,7 +380,7 @@ struct IterArgs {
 };
 
 template <typename T, bool CHECK>
-__global__ void __launch_bounds__(kBlock) k_primal(IterArgs a, const T* __restrict__ val, const T* __restrict__ y,
+__global__ void __launch_bounds__(kBlock, iter_min_blocks<T>()) k_primal(IterArgs a, const T* __restrict__ val, const T* __restrict__ y,
                                                    T* __restrict__ x, T* __restrict__ xbar, T* __restrict__ xplus,
                                                    const T* __restrict__ c, const T* __restrict__ lo,
                                                    const T* __restrict__ up, const T* __restrict__ x0) {
@@ -352,7 +401,7 @@ __global__ void __launch_bounds__(kBlock) k_primal(IterArgs a, const T* __restri
 }
 
 template <typename T, bool CHECK>
-__global__ void __launch_bounds__(kBlock) k_dual(IterArgs a, const T* __restrict__ val, const T* __restrict__ xbar,
+__global__ void __launch_bounds__(kBlock, iter_min_blocks<T>()) k_dual(IterArgs a, const T* __restrict__ val, const T* __restrict__ xbar,
                                                  T* __restrict__ y, T* __restrict__ yplus, const T* __restrict__ rl,
                                                  const T* __restrict__ ru, const T* __restrict__ y0) {
     __shared__ double s_red[kWarps];

@@ -97,7 +97,7 @@ __device__ __forceinline__ void rowblock_spmv_batch(const BatchArgs& a, const TV
 }
 
 template <typename T, bool CHECK>
-__global__ void __launch_bounds__(kBlock) k_bprimal(BatchArgs a, const T* __restrict__ val, const T* __restrict__ y,
+__global__ void __launch_bounds__(kBlock, iter_min_blocks<T>()) k_bprimal(BatchArgs a, const T* __restrict__ val, const T* __restrict__ y,
                                                     T* __restrict__ x, T* __restrict__ xbar, T* __restrict__ xplus,
                                                     const T* __restrict__ c, const T* __restrict__ lo,
                                                     const T* __restrict__ up, const T* __restrict__ x0) {
@@ -116,7 +116,7 @@ __global__ void __launch_bounds__(kBlock) k_bprimal(BatchArgs a, const T* __rest
 }
 
 template <typename T, bool CHECK>
-__global__ void __launch_bounds__(kBlock) k_bdual(BatchArgs a, const T* __restrict__ val, const T* __restrict__ xbar,
+__global__ void __launch_bounds__(kBlock, iter_min_blocks<T>()) k_bdual(BatchArgs a, const T* __restrict__ val, const T* __restrict__ xbar,
                                                   T* __restrict__ y, T* __restrict__ yplus, const T* __restrict__ rl,
                                                   const T* __restrict__ ru, const T* __restrict__ y0) {
     DualEpi<T, CHECK> epi;

@@ -17,8 +17,11 @@
 
 namespace nir {
 
-constexpr int kWarpU = 8;                    // nonzeros per lane per round
-constexpr int kWarpCapMax = 32 * kWarpU;     // largest warp row block (256)
+#ifndef NIR_WARP_U
+#define NIR_WARP_U 8
+#endif
+constexpr int kWarpU = NIR_WARP_U;           // nonzeros per lane per round
+constexpr int kWarpCapMax = 32 * kWarpU;     // largest warp row block (256 for 8 per lane)
 constexpr int kRowsPerWarpBlock = 32;        // rows in one warp row block
 
 // Greedy packing of consecutive rows; rp[0] may be any offset.

@@ -69,8 +69,9 @@ class Info(C.Structure):
 
 
 class KernelTime(C.Structure):
-    _fields_ = [("primal_us", C.c_double), ("dual_us", C.c_double), ("iter_us", C.c_double),
-                ("samples", C.c_int64)]
+    """Mean event times of the fused kernels; index 0 = FP32 chunks, 1 = FP64."""
+    _fields_ = [("primal_us", C.c_double * 2), ("dual_us", C.c_double * 2), ("iter_us", C.c_double * 2),
+                ("samples", C.c_int64 * 2)]
 
 
 class Layout(C.Structure):

@@ -124,3 +124,4 @@ def test_corrupted_descriptor_is_rejected(harness):
         msg = run(harness, rp, off, 32, corrupt=k)
         assert isinstance(msg, str) and "internal" in msg
     assert "capacity" in run(harness, [0, 10, 20], [0, 2], 0)
+
