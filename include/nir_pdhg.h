@@ -116,6 +116,12 @@ typedef struct nir_pdhg_info {
     double solve_seconds;         /* iterations until the returned point                 */
     double time_to_fp64_seconds;  /* when the FP64 polish began (MIXED), else 0          */
     int32_t kernel_launches;      /* engine kernels launched by this solve               */
+    int32_t pad_;
+    int64_t iterations_to_tol;    /* NIR_ALGO_REFERENCE with tol > 0: first iteration (a
+                                     multiple of 32) whose iterate has rel KKT <= tol,
+                                     -1 if none; the iterates are not changed by the probe.
+                                     Other algorithms: the iterations when they stopped at
+                                     tol, else -1                                         */
 } nir_pdhg_info;
 
 typedef struct nir_pdhg nir_pdhg;

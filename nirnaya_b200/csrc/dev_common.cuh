@@ -55,6 +55,7 @@ struct DevState {
     long long ref_iterations;
     int ref_stopped;
     int pad_;
+    long long probe_hit;   // reference loop: first probed iteration with rel KKT <= tol (-1: none yet)
 };
 
 // Deterministic block-wide sum / max over kBlock threads: a fixed shuffle

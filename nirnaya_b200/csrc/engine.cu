@@ -662,7 +662,16 @@ unsigned long long chunk_key(const nir_pdhg* h, const SolveCfg& c, int phase, bo
     return k.h;
 }
 
-void launch_ref_chunk(nir_pdhg* h, int K) {
+void precondition(nir_pdhg* h, const nir_pdhg_params& p, bool enable);
+double rhs_norm(const nir_pdhg* h);
+double norm2(const std::vector<double>& v);
+
+// Relative-KKT probe of the reference loop: norms of the original b and c.
+struct RefProbe {
+    double bnorm, cnorm, tol;
+};
+
+void launch_ref_chunk(nir_pdhg* h, int K, const RefProbe* probe) {
     cudaStream_t s = h->stream;
     const PartLayout L = part_layout(h);
     const unsigned gm = grid_for(h->m), gn = grid_for(h->n);
@@ -674,6 +683,19 @@ void launch_ref_chunk(nir_pdhg* h, int K) {
                                                                   h->ru, h->y64, L.misc, h->st, i);
         NIR_LAUNCHED();
         nir::k_ref_stop<<<1, nir::kBlock, 0, s>>>(L.misc, std::max<int>(gm, 1), h->st, i, K);
+        NIR_LAUNCHED();
+        h->launches += 3;
+    }
+    if (probe) {
+        // KKT of (x, y) on the unscaled matrix (dr = dc = 1): reads only
+        const LaunchCfg ckr = warp_cfg<double>(h, nir::k_kkt_rows<double>, h->A.nblk);
+        const LaunchCfg ckc = warp_cfg<double>(h, nir::k_kkt_cols<double>, h->At.nblk);
+        nir::KktArgs kr{h->A.blk, h->A.nblk, h->A.cap, h->A.rp, h->A.ci, h->A.v64, L.KR, h->st, 0};
+        nir::k_kkt_rows<double><<<ckr.grid, nir::kBlock, ckr.smem, s>>>(kr, h->x64, h->y64, h->dr, h->rl, h->ru);
+        nir::KktArgs kc{h->At.blk, h->At.nblk, h->At.cap, h->At.rp, h->At.ci, h->At.v64, L.KC, h->st, 0};
+        nir::k_kkt_cols<double><<<ckc.grid, nir::kBlock, ckc.smem, s>>>(kc, h->x64, h->y64, h->dc, h->c, h->l, h->u);
+        nir::k_ref_probe<<<1, nir::kBlock, 0, s>>>(L.KR, ckr.grid, L.KC, ckc.grid, probe->bnorm, probe->cnorm,
+                                                   h->offset, probe->tol, h->st);
         NIR_LAUNCHED();
         h->launches += 3;
     }
@@ -816,7 +838,23 @@ int solve_reference(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), v
     nir::DevState st0{};
     st0.max_iters = p.max_iters;
     st0.best_kkt = INFINITY;
+    st0.kkt = st0.kp = st0.kd = st0.kg = st0.max_rel_row = NAN;
+    st0.probe_hit = -1;
     NIR_CUDA(cudaMemcpyAsync(h->st, &st0, sizeof(st0), cudaMemcpyHostToDevice, s));
+    // optional relative-KKT probe every chunk (tol > 0): unscaled FP64 copy
+    // of the values and warp row blocks for the KKT kernels
+    const bool probing = p.tol > 0.0;
+    RefProbe probe{0.0, 0.0, p.tol};
+    if (probing) {
+        precondition(h, p, false);
+        const int cap = auto_cap(h->nnz, std::max(h->m, h->n));
+        set_blocks(h, h->A, cap);
+        set_blocks(h, h->At, cap);
+        warp_cfg<double>(h, nir::k_kkt_rows<double>, h->A.nblk);
+        warp_cfg<double>(h, nir::k_kkt_cols<double>, h->At.nblk);
+        probe.bnorm = rhs_norm(h);
+        probe.cnorm = norm2(h->h_c);
+    }
     // power iteration, src/gpu/pdhg_solver.hpp:33-45
     nir::k_fill<<<grid_for(n), nir::kBlock, 0, s>>>(n, 1.0, h->tmp_n);
     NIR_LAUNCHED();
@@ -836,13 +874,17 @@ int solve_reference(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), v
     const double t_setup = now_sec();
     LoopResult R;
     if (p.max_iters > 0) {
-        auto launch = [&]() { launch_ref_chunk(h, K); };
+        const RefProbe* pr = probing ? &probe : nullptr;
+        auto launch = [&]() { launch_ref_chunk(h, K, pr); };
         if (p.use_graphs) {
-            cudaGraphExec_t ge = chunk_graph(h, 0, 1000, launch);
-            R = run_chunks(h, p, poll, ctx, t0, 0, launches_per_chunk(K, true), [&]() { NIR_CUDA(cudaGraphLaunch(ge, s)); },
-                           nullptr);
+            KeyHash key;
+            key.add(1000).add(probing).add(probe.bnorm).add(probe.cnorm).add(probe.tol).add(h->offset);
+            key.add(h->A.blk).add(h->At.blk).add(h->A.cap).add(h->part);
+            cudaGraphExec_t ge = chunk_graph(h, 0, key.h, launch);
+            const int per = launches_per_chunk(K, true) + (probing ? 3 : 0);
+            R = run_chunks(h, p, poll, ctx, t0, 0, per, [&]() { NIR_CUDA(cudaGraphLaunch(ge, s)); }, nullptr);
         } else {
-            R = run_chunks(h, p, poll, ctx, t0, 0, 0, [&]() { launch_ref_chunk(h, K); }, nullptr);
+            R = run_chunks(h, p, poll, ctx, t0, 0, 0, launch, nullptr);
         }
     }
     nir::DevState st;
@@ -865,8 +907,13 @@ int solve_reference(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), v
     info->primal_weight = 1.0;
     info->setup_seconds = t_setup - t0;
     info->solve_seconds = now_sec() - t_setup;
-    info->rel_kkt = info->rel_primal = info->rel_dual = info->rel_gap = NAN;
-    info->max_rel_row_viol = NAN;
+    // probed KKT of the last full chunk (NaN without the probe)
+    info->rel_kkt = st.kkt;
+    info->rel_primal = st.kp;
+    info->rel_dual = st.kd;
+    info->rel_gap = st.kg;
+    info->max_rel_row_viol = st.max_rel_row;
+    info->iterations_to_tol = st.probe_hit;
     (void)R;
     return status;
 }
@@ -1242,6 +1289,7 @@ int solve_fast(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), void* 
     info->setup_seconds = t_setup - t0;
     info->solve_seconds = now_sec() - t_setup;
     info->time_to_fp64_seconds = t_switch;
+    info->iterations_to_tol = (status == NIR_STATUS_OPTIMAL) ? st.iter : -1;
     return status;
 }
 

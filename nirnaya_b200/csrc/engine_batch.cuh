@@ -376,6 +376,7 @@ int batch_solve_impl(nir_pdhg_batch* B, const nir_pdhg_params& p, int (*poll)(vo
         inf.objective = o.hi + o.lo;
         inf.setup_seconds = t_setup - t0;
         inf.solve_seconds = t_end - t_setup;
+        inf.iterations_to_tol = (inf.status == NIR_STATUS_OPTIMAL) ? inf.iterations : -1;
         if (infos) infos[i] = inf;
         if (inf.status != NIR_STATUS_OPTIMAL && worst == NIR_STATUS_OPTIMAL) worst = inf.status;
         iters = std::max<long long>(iters, d.iter);

@@ -575,20 +575,34 @@ struct CtlSums {
     double dx2, dxa2, dy2, dya2, pres2, dobj_r, ywrong2, maxrel, dres2, dobj_c, pobj_c, xviol2;
 };
 
+// Relative KKT error in the original space from the KKT kernels' sums:
+// primal residual (rows and column bounds) over 1 + ||b||, dual residual
+// (reduced costs of the wrong sign and row duals of the wrong sign) over
+// 1 + ||c||, and the relative duality gap.
+struct KktVal {
+    double kkt, kp, kd, kg, pobj, dobj;
+};
+
+__device__ inline KktVal kkt_from_sums(const CtlSums& s, double bnorm, double cnorm, double offset) {
+    KktVal k;
+    k.pobj = s.pobj_c + offset;
+    k.dobj = s.dobj_r + s.dobj_c + offset;
+    k.kp = sqrt(s.pres2 + s.xviol2) / (1.0 + bnorm);
+    k.kd = sqrt(s.dres2 + s.ywrong2) / (1.0 + cnorm);
+    k.kg = fabs(k.pobj - k.dobj) / (1.0 + fabs(k.pobj) + fabs(k.dobj));
+    k.kkt = fmax(k.kp, fmax(k.kd, k.kg));
+    return k;
+}
+
 __device__ void control_update(const CtlArgs& a, DevState* st, const CtlSums& sums, double bnorm, double cnorm,
                                double offset, double* hist) {
     const double dx2 = sums.dx2, dxa2 = sums.dxa2, dy2 = sums.dy2, dya2 = sums.dya2;
-    const double pres2 = sums.pres2, dobj_r = sums.dobj_r, ywrong2 = sums.ywrong2, maxrel = sums.maxrel;
-    const double dres2 = sums.dres2, dobj_c = sums.dobj_c, pobj_c = sums.pobj_c, xviol2 = sums.xviol2;
+    const double maxrel = sums.maxrel;
 
     const long long it = st->iter + a.K;
     st->iter = it;
-    const double pobj = pobj_c + offset;
-    const double dobj = dobj_r + dobj_c + offset;
-    const double kp = sqrt(pres2 + xviol2) / (1.0 + bnorm);
-    const double kd = sqrt(dres2 + ywrong2) / (1.0 + cnorm);
-    const double kg = fabs(pobj - dobj) / (1.0 + fabs(pobj) + fabs(dobj));
-    const double kkt = fmax(kp, fmax(kd, kg));
+    const KktVal kv = kkt_from_sums(sums, bnorm, cnorm, offset);
+    const double pobj = kv.pobj, dobj = kv.dobj, kp = kv.kp, kd = kv.kd, kg = kv.kg, kkt = kv.kkt;
     const double omega = st->omega;
     const double res = sqrt(omega * dx2 + dy2 / omega);
     st->kkt = kkt;
@@ -707,6 +721,36 @@ __global__ void __launch_bounds__(kBlock) k_control(CtlArgs a, DevState* st) {
     if (threadIdx.x != 0) return;
     const CtlSums sums{dx2, dxa2, dy2, dya2, pres2, dobj_r, ywrong2, maxrel, dres2, dobj_c, pobj_c, xviol2};
     control_update(a, st, sums, a.bnorm, a.cnorm, a.offset, a.hist);
+}
+
+// KKT probe of the reference loop (after a chunk's KKT kernels): records
+// the relative KKT of the current iterate and the first iteration at which
+// it is at most tol.  Reads the iterate only.
+__global__ void __launch_bounds__(kBlock) k_ref_probe(const double* __restrict__ partKR, int nKR,
+                                                      const double* __restrict__ partKC, int nKC, double bnorm,
+                                                      double cnorm, double offset, double tol, DevState* st) {
+    __shared__ double sh[kWarps];
+    if (st->done) return;  // the KKT kernels skipped this chunk
+    CtlSums s{};
+    s.pres2 = block_sum_array(partKR, nKR, sh);
+    s.dobj_r = block_sum_array(partKR + nKR, nKR, sh);
+    s.ywrong2 = block_sum_array(partKR + 2 * nKR, nKR, sh);
+    s.maxrel = block_max_array(partKR + 3 * nKR, nKR, sh);
+    s.dres2 = block_sum_array(partKC, nKC, sh);
+    s.dobj_c = block_sum_array(partKC + nKC, nKC, sh);
+    s.pobj_c = block_sum_array(partKC + 2 * nKC, nKC, sh);
+    s.xviol2 = block_sum_array(partKC + 3 * nKC, nKC, sh);
+    if (threadIdx.x != 0) return;
+    const KktVal k = kkt_from_sums(s, bnorm, cnorm, offset);
+    st->kkt = k.kkt;
+    st->kp = k.kp;
+    st->kd = k.kd;
+    st->kg = k.kg;
+    st->pobj = k.pobj;
+    st->dobj = k.dobj;
+    st->max_rel_row = s.maxrel;
+    st->kkt_iter = st->iter;
+    if (st->probe_hit < 0 && k.kkt <= tol) st->probe_hit = st->iter;
 }
 
 // Restart: the anchor and the iterate become (x+, y+).

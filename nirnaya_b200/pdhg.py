@@ -61,7 +61,7 @@ class Info(C.Structure):
         ("rel_primal", C.c_double), ("rel_dual", C.c_double), ("rel_gap", C.c_double),
         ("max_rel_row_viol", C.c_double), ("primal_weight", C.c_double), ("step_size", C.c_double),
         ("setup_seconds", C.c_double), ("solve_seconds", C.c_double), ("time_to_fp64_seconds", C.c_double),
-        ("kernel_launches", C.c_int32),
+        ("kernel_launches", C.c_int32), ("pad_", C.c_int32), ("iterations_to_tol", C.c_int64),
     ]
 
     def as_dict(self):

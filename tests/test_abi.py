@@ -48,7 +48,35 @@ def test_structs_match_header_sizes():
     # nir_pdhg_params: 2 int32, 2 double, int64, double, 3 int32, 5 double,
     # double, 2 int32, double, 5 int32 (+pad), 2 pointers, 2 double
     assert C.sizeof(pdhg.Params) == 176
-    assert C.sizeof(pdhg.Info) == 4 + 4 + 8 + 8 + 8 * 11 + 4 + 4
+    assert C.sizeof(pdhg.Info) == 4 + 4 + 8 + 8 + 8 * 11 + 4 + 4 + 8
+
+
+def test_ctypes_layouts_match_the_c_compiler(tmp_path):
+    """sizeof and field offsets of every struct in include/*.h as gcc sees
+    them, against the ctypes mirrors."""
+    import subprocess
+
+    from nirnaya_b200 import pdhg
+    from nirnaya_b200.lp import NirLpView
+
+    mirrors = {"nir_pdhg_params": pdhg.Params, "nir_pdhg_info": pdhg.Info, "nir_pdhg_kernel_time": pdhg.KernelTime,
+               "nir_pdhg_layout": pdhg.Layout, "nir_lp_view": NirLpView}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "nir_pdhg.h"', "int main(void) {"]
+    for cname, py in mirrors.items():
+        lines.append(f'printf("{cname} sizeof %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for cname, py in mirrors.items():
+        assert got[(cname, "sizeof")] == C.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
 
 
 @pytest.mark.skipif(has_gpu(), reason="checks the no-GPU failure mode")

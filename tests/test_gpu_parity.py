@@ -282,3 +282,23 @@ def test_reference_shaped_api():
     d.interrupt()
     r = pdhg.PdhgSolver.solve(L.generate(L.RANDOM_EQ, 1), pdhg.Options(pdhg_tol=0.0), d)
     assert r.status == pdhg.TIME_LIMIT
+
+
+def test_reference_loop_kkt_probe_matches_oracle():
+    # the probe reads the iterates only (bit-identical loop) and finds the
+    # first 32-iteration boundary at which the reference iterate has rel KKT
+    # <= tol, as the oracle's restatement probing at the same interval does
+    lp = L.generate(L.RANDOM_EQ, 5, m=200, n=500)
+    tol = 1e-4
+    cap = 60016  # the chunk that ends the loop is not probed; the one before is
+    with pdhg.Engine(lp) as eng:
+        x, y, info = eng.solve(pdhg.default_params(algorithm=pdhg.ALGO_REFERENCE, max_iters=cap, tol=tol))
+    xo, yo, out = ffi.ref_pdhg_restated(lp, cap, probe_every=32, probe_tol=tol)
+    assert np.array_equal(G.bits(x), G.bits(xo)) and info.iterations == out.iterations
+    assert out.first_hit > 0
+    assert info.iterations_to_tol == out.first_hit
+    # same iterate at the last probe: FP64 device sums vs double-double
+    assert abs(info.rel_kkt - out.last_kkt) <= 1e-9 * out.last_kkt
+    with pdhg.Engine(lp) as eng:
+        _, _, off = eng.solve(pdhg.default_params(algorithm=pdhg.ALGO_REFERENCE, max_iters=60000, tol=0.0))
+    assert off.iterations_to_tol == -1 and np.isnan(off.rel_kkt)
