@@ -9,6 +9,12 @@ instances of include/nir_lpgen.h; the reference publishes no dataset):
   c2  ZIPF 200,000 x 500,000, ~5M nonzeros, mixed precision (default)
   c1  RANDOM_EQ 2,000 x 5,000, 40,000 nonzeros
   c5  BADLY_SCALED 50,000 x 120,000, ~1M nonzeros
+  c4  learned warm start on the fixed-matrix blending family (m 20,000,
+      n 50,000, 400k nonzeros): PDLP solves --c4-train instances, the
+      network (3 x 512, hand-written BF16 tensor-core kernels) trains on
+      them, and --c4-test held-out instances are solved cold and warm to
+      1e-6; also plain FP64 PDHG on --c4-pdhg of them.  Time per held-out
+      instance (mean).
   c3  256 MULTIPERIOD instances, m log-uniform in [500, 20,000], n = 2.5 m
       (~1.3M rows, ~3.3M columns, ~33M nonzeros in total), solved as one
       batch (nir_pdhg_batch_solve); with --gpus N the instances are sharded
@@ -50,6 +56,8 @@ WORKLOADS = {
     "c1": dict(kind=1, seed=1, kw={}, label="random_eq_2000x5000_nnz40000", precision=1),
     "c5": dict(kind=5, seed=1, kw={}, label="badly_scaled_50000x120000_nnz1M", precision=1),
     "c3": dict(kind=3, seed=1000, kw={}, label="multiperiod_batch256_m500-20000", precision=1, batch=256),
+    "c4": dict(kind=4, seed=0, kw={}, label="blend_family_20000x50000_nnz400k_learned_warm", precision=1,
+               learned=True),
 }
 
 
@@ -417,6 +425,85 @@ def batch_line(args, r, world):
     }
 
 
+def run_learned(args, world):
+    """c4: the learned warm start pipeline on one GPU (replicas only)."""
+    import numpy as np
+
+    from nirnaya_b200 import learned as LW
+    from nirnaya_b200 import pdhg
+
+    fam = LW.BlendFamily(m=20000, n=50000, nnz=400000, family_seed=0)
+    p = pdhg.default_params(tol=1e-6, max_iters=1000000)
+    eng = pdhg.Engine(fam.base, 0)
+    t0 = time.perf_counter()
+    train = LW.solve_family(fam, range(100000, 100000 + args.c4_train), p, engine=eng)
+    t_gen = time.perf_counter() - t0
+    model = LW.WarmStart(fam, width=512, depth=3, seed=0, lr=1e-3)
+    t0 = time.perf_counter()
+    fit = model.fit(train, epochs=args.c4_epochs, batch=8192, cols_per_instance=1024, rows_per_instance=512)
+    t_fit = time.perf_counter() - t0
+    losses = fit["col_loss"]
+    us_step, flops_step = model.col_net.step_stats()
+    held = list(range(900000, 900000 + args.c4_test))
+    with ClockSampler(0) as clk:
+        ev = LW.evaluate(fam, model, held, p, engine=eng)
+    summ = ev.summary()
+    # baselines on a subset: cold FP64 PDLP and plain (unrestarted) FP64 PDHG
+    sub = held[: args.c4_pdhg]
+    p64 = pdhg.default_params(tol=1e-6, max_iters=1000000, precision=pdhg.PREC_FP64)
+    pp = pdhg.default_params(tol=1e-6, max_iters=args.c4_pdhg_iters, precision=pdhg.PREC_FP64,
+                             algorithm=pdhg.ALGO_PDHG)
+    t64, tpl, itpl, stpl = [], [], [], []
+    for sd in sub:
+        rowlo, cost = fam.vectors(*fam.factors(sd))
+        eng.update_vectors(cost=cost, rowlo=rowlo)
+        t1 = time.perf_counter()
+        eng.solve(p64)
+        t64.append(time.perf_counter() - t1)
+        t1 = time.perf_counter()
+        _, _, ip = eng.solve(pp)
+        tpl.append(time.perf_counter() - t1)
+        itpl.append(ip.iterations)
+        stpl.append(ip.status)
+    eng.close()
+    model.close()
+    warm_s = summ["warm_seconds_mean"]
+    peak_tf = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak_tf = float(json.load(f)["bf16_tflops"])
+    except Exception:
+        peak_tf = 1590.0
+    tf = flops_step / (us_step * 1e-6) / 1e12 if us_step > 0 else None
+    pdhg_reached = all(s_ == pdhg.OPTIMAL for s_ in stpl)
+    line = {
+        "metric": METRIC, "value": warm_s, "unit": "s", "n_gpus": world, "steps": args.c4_test, "warmup": 0,
+        "ms_per_step": 1000 * warm_s, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64 (PDLP), bf16 x fp32 (network)", "data": "synthetic (seeded blending family)",
+        "config": {"workload": WORKLOADS["c4"]["label"], "m": fam.m, "n": fam.n, "nnz": fam.base.nnz,
+                   "train_instances": args.c4_train, "test_instances": args.c4_test, "network": "per-column and per-row 3 x 512 ReLU MLPs (shared weights)",
+                   "tol": 1e-6, "parallelism": "single gpu"},
+        "learned": {**summ, "train_generation_s": t_gen, "train_fit_s": t_fit,
+                    "train_loss_first_last": [float(losses[0]), float(losses[-1])],
+                    "row_loss_first_last": [float(fit["row_loss"][0]), float(fit["row_loss"][-1])],
+                    "col_samples": fit["col_samples"], "row_samples": fit["row_samples"],
+                    "train_solutions_optimal": int((train.status == pdhg.OPTIMAL).sum())},
+        "baselines": {"cold_mixed_pdlp_s": summ["cold_seconds_mean"], "cold_fp64_pdlp_s": float(np.mean(t64)),
+                      "plain_fp64_pdhg_s": float(np.mean(tpl)), "plain_fp64_pdhg_iterations": float(np.mean(itpl)),
+                      "plain_fp64_pdhg_reached_tol": pdhg_reached, "subset": len(sub),
+                      "plain_fp64_pdhg_over_learned_warm": float(np.mean(tpl)) / warm_s,
+                      "note": None if pdhg_reached else
+                      "plain PDHG hit its iteration cap on some instances: its time is a lower bound"},
+        "roofline": {"bound": "tensor", "achieved": tf, "peak": peak_tf, "unit": "TFLOP/s",
+                     "frac": (tf / peak_tf) if tf else None, "traffic": None,
+                     "kernel": "column network training step (k_gemm mma.sync BF16, FP32 accumulate), 8192-sample batch",
+                     "us_per_step": us_step, "flops_per_step": flops_step},
+        "cpu_baseline": None,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line))
+
+
 def reference_iterations(args):
     """Counts the reference PDHG's iterations to 1e-6 relative KKT on the
     workload: the bit-identical GPU restatement of its loop
@@ -450,6 +537,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--max-iters", type=int, default=1000000)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--c4-train", type=int, default=4096)
+    ap.add_argument("--c4-test", type=int, default=512)
+    ap.add_argument("--c4-pdhg", type=int, default=16)
+    ap.add_argument("--c4-pdhg-iters", type=int, default=400000)
+    ap.add_argument("--c4-epochs", type=int, default=4)
     ap.add_argument("--ref-iterations", type=int, default=0,
                     help="count the reference loop's iterations to its stopping rule (cap), then exit")
     ap.add_argument("--ref-seconds", type=float, default=600.0)
@@ -534,6 +626,10 @@ def main():
         print(json.dumps(line))
         return
 
+    if wl.get("learned"):
+        if rank == 0:
+            run_learned(args, world)
+        return
     if wl.get("batch"):
         r = run_batch_ours(args, rank, world, local)
         if rank == 0:

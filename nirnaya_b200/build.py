@@ -2,6 +2,7 @@
 
   nirnaya_b200/libnir_pdhg.so   CUDA engine + C ABI (nvcc, sm_100a only)
   nirnaya_b200/libnir_lpgen.so  seeded instance generator (g++)
+  nirnaya_b200/libnir_mlp.so    warm-start network (nvcc, sm_100a)
 
 Run `python -m nirnaya_b200.build` or call build_all().
 """
@@ -55,6 +56,17 @@ def build_engine(force: bool = False, verbose: bool = False) -> str:
     return target
 
 
+def build_mlp(force: bool = False, verbose: bool = False) -> str:
+    target = os.path.join(HERE, "libnir_mlp.so")
+    srcs = [os.path.join(CSRC, "mlp.cu"), os.path.join(INC, "nir_mlp.h")]
+    if force or _stale(target, srcs):
+        cmd = [_nvcc(), *NVCC_FLAGS, srcs[0], "-o", target]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+    return target
+
+
 def build_lpgen(force: bool = False, verbose: bool = False) -> str:
     target = os.path.join(HERE, "libnir_lpgen.so")
     srcs = [os.path.join(CSRC, "lpgen.cpp"), os.path.join(INC, "nir_lpgen.h"), os.path.join(INC, "nir_lp.h")]
@@ -70,6 +82,7 @@ def build_lpgen(force: bool = False, verbose: bool = False) -> str:
 def build_all(force: bool = False, verbose: bool = False) -> None:
     build_lpgen(force, verbose)
     build_engine(force, verbose)
+    build_mlp(force, verbose)
 
 
 if __name__ == "__main__":

@@ -1,0 +1,151 @@
+"""ctypes binding of libnir_mlp.so (include/nir_mlp.h): the warm-start
+network's hand-written tensor-core training and inference."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libnir_mlp.so")
+
+EXPORTED = [
+    "nir_mlp_create", "nir_mlp_free", "nir_mlp_last_error", "nir_mlp_param_count", "nir_mlp_get_params",
+    "nir_mlp_set_params", "nir_mlp_set_output_weights", "nir_mlp_set_data", "nir_mlp_train", "nir_mlp_predict",
+    "nir_mlp_gradients", "nir_mlp_gemm_check", "nir_mlp_step_stats",
+]
+
+
+class Config(C.Structure):
+    _fields_ = [("d_in", C.c_int32), ("width", C.c_int32), ("depth", C.c_int32), ("d_out", C.c_int32),
+                ("seed", C.c_uint64), ("lr", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float),
+                ("eps", C.c_float)]
+
+
+_lib = None
+F = C.POINTER(C.c_float)
+
+
+def lib():
+    """Loads libnir_mlp.so (raises if it is missing: no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing; build it with `python -m nirnaya_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        VP = C.c_void_p
+        L.nir_mlp_create.argtypes = [C.POINTER(Config), C.c_int, C.POINTER(VP)]
+        L.nir_mlp_free.argtypes = [VP]
+        L.nir_mlp_last_error.restype = C.c_char_p
+        L.nir_mlp_param_count.argtypes = [VP]
+        L.nir_mlp_param_count.restype = C.c_int64
+        L.nir_mlp_get_params.argtypes = [VP, F]
+        L.nir_mlp_set_params.argtypes = [VP, F]
+        L.nir_mlp_set_output_weights.argtypes = [VP, F]
+        L.nir_mlp_set_data.argtypes = [VP, F, F, C.c_int32]
+        L.nir_mlp_train.argtypes = [VP, C.c_int32, C.c_int32, F]
+        L.nir_mlp_predict.argtypes = [VP, F, C.c_int32, F]
+        L.nir_mlp_gradients.argtypes = [VP, F, F, C.c_int32, F, F]
+        L.nir_mlp_gemm_check.argtypes = [VP, C.c_int, C.c_int, C.c_int32, C.c_int32, C.c_int32, F, C.c_int32, F,
+                                         C.c_int32, F]
+        L.nir_mlp_step_stats.argtypes = [VP, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        _lib = L
+    return _lib
+
+
+def _f(a):
+    return a.ctypes.data_as(F)
+
+
+def _c32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+class Mlp:
+    """d_in -> width x depth (ReLU) -> d_out on one GPU."""
+
+    def __init__(self, d_in, d_out, width=512, depth=3, seed=0, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8,
+                 device=0):
+        self.cfg = Config(d_in, width, depth, d_out, seed, lr, beta1, beta2, eps)
+        self.dims = [d_in] + [width] * depth + [d_out]
+        self._h = C.c_void_p()
+        rc = lib().nir_mlp_create(C.byref(self.cfg), device, C.byref(self._h))
+        if rc != 0:
+            raise RuntimeError(f"nir_mlp_create failed: {lib().nir_mlp_last_error().decode()}")
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise RuntimeError(f"{what} failed: {lib().nir_mlp_last_error().decode()}")
+
+    def close(self):
+        if self._h:
+            lib().nir_mlp_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def param_count(self) -> int:
+        return int(lib().nir_mlp_param_count(self._h))
+
+    def get_params(self) -> np.ndarray:
+        out = np.zeros(self.param_count(), np.float32)
+        self._check(lib().nir_mlp_get_params(self._h, _f(out)), "get_params")
+        return out
+
+    def set_params(self, p):
+        p = _c32(p)
+        assert p.size == self.param_count()
+        self._check(lib().nir_mlp_set_params(self._h, _f(p)), "set_params")
+
+    def set_output_weights(self, w):
+        w = _c32(w)
+        self._check(lib().nir_mlp_set_output_weights(self._h, _f(w)), "set_output_weights")
+
+    def set_data(self, X, T):
+        X, T = _c32(X), _c32(T)
+        self._check(lib().nir_mlp_set_data(self._h, _f(X), _f(T), X.shape[0]), "set_data")
+
+    def train(self, epochs, batch) -> np.ndarray:
+        losses = np.zeros(max(epochs, 1), np.float32)
+        self._check(lib().nir_mlp_train(self._h, epochs, batch, _f(losses)), "train")
+        return losses[:epochs]
+
+    def predict(self, X) -> np.ndarray:
+        X = _c32(X)
+        n = X.shape[0]
+        pad = (-n) % 8
+        if pad:
+            X = np.vstack([X, np.zeros((pad, X.shape[1]), np.float32)])
+        Y = np.zeros((X.shape[0], self.dims[-1]), np.float32)
+        self._check(lib().nir_mlp_predict(self._h, _f(X), X.shape[0], _f(Y)), "predict")
+        return Y[:n]
+
+    def gradients(self, X, T):
+        X, T = _c32(X), _c32(T)
+        g = np.zeros(self.param_count(), np.float32)
+        loss = C.c_float()
+        self._check(lib().nir_mlp_gradients(self._h, _f(X), _f(T), X.shape[0], C.byref(loss), _f(g)), "gradients")
+        return float(loss.value), g
+
+    def gemm(self, a_kmaj, b_kmaj, M, N, K, A, lda, B, ldb) -> np.ndarray:
+        A, B = _c32(A), _c32(B)
+        Cm = np.zeros((M, N), np.float32)
+        self._check(lib().nir_mlp_gemm_check(self._h, int(a_kmaj), int(b_kmaj), M, N, K, _f(A), lda, _f(B), ldb,
+                                             _f(Cm)), "gemm_check")
+        return Cm
+
+    def step_stats(self):
+        us, fl = C.c_double(), C.c_double()
+        lib().nir_mlp_step_stats(self._h, C.byref(us), C.byref(fl))
+        return us.value, fl.value

@@ -172,7 +172,8 @@ class Engine:
         self.lp._view = None
 
     def solve(self, params: Params | None = None, poll=None, x_init=None, y_init=None, omega_init=None):
-        p = params if params is not None else default_params()
+        # a copy: the warm-start pointers must not outlive this call in the caller's params
+        p = Params.from_buffer_copy(params) if params is not None else default_params()
         keep = []
         if x_init is not None:
             xa = np.ascontiguousarray(x_init, np.float64)

@@ -1,0 +1,44 @@
+"""The learned warm start on a small member of the blending family, end to
+end on the GPU: PDLP generates the training solutions, the per-column and
+per-row networks train on the GPU with their own kernels, and on held-out
+instances the warm-started PDLP reaches the same 1e-6 relative KKT as the
+cold start (checked by the oracle) in fewer iterations on average.
+
+The SpMV layout is pinned (spmv_block_nnz) so that the iteration counts do
+not depend on the autotuner's timing-based choice: the whole pipeline is
+then deterministic."""
+import numpy as np
+import pytest
+
+from conftest import has_gpu
+from nirnaya_b200 import learned as LW
+from nirnaya_b200 import pdhg
+from oracle import ffi
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not has_gpu(), reason="needs a CUDA device")]
+
+
+def test_warm_start_reaches_the_same_tolerance_in_fewer_iterations():
+    fam = LW.BlendFamily(m=2000, n=5000, nnz=40000, family_seed=0)
+    p = pdhg.default_params(tol=1e-6, max_iters=200000, spmv_block_nnz=64)
+    with pdhg.Engine(fam.base) as eng:
+        train = LW.solve_family(fam, range(1000, 1512), p, engine=eng)
+        assert (train.status == pdhg.OPTIMAL).all()
+        model = LW.WarmStart(fam, width=256, depth=3, seed=0, lr=1e-3)
+        fit = model.fit(train, epochs=8, batch=8192)
+        assert fit["col_loss"][-1] < fit["col_loss"][0] and fit["row_loss"][-1] < fit["row_loss"][0]
+        held = list(range(5000, 5048))
+        ev = LW.evaluate(fam, model, held, p, engine=eng)
+        # the warm result is judged by the oracle too
+        lp = fam.instance(held[0])
+        x0, y0, w0 = model.predict(*fam.factors(held[0]))
+        eng.update_vectors(cost=lp.cost, rowlo=lp.rowlo)
+        x, y, info = eng.solve(p, x_init=x0, y_init=y0, omega_init=w0)
+    model.close()
+    s = ev.summary()
+    assert s["accepted"] == s["instances"], s
+    assert info.status == pdhg.OPTIMAL and ffi.rel_kkt(lp, x, y).rel_kkt <= 1.05e-6
+    assert s["max_rel_objective_gap"] <= 2e-5, s
+    # restarted PDLP's iteration count depends only logarithmically on the
+    # starting distance: the gain is real but modest (about 8% measured)
+    assert s["warm_iterations_mean"] <= 0.97 * s["cold_iterations_mean"], s
