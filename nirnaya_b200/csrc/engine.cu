@@ -872,7 +872,7 @@ int solve_reference(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), v
     h->launches += 3;
     const int K = 32;
     const double t_setup = now_sec();
-    LoopResult R;
+    [[maybe_unused]] LoopResult R;
     if (p.max_iters > 0) {
         const RefProbe* pr = probing ? &probe : nullptr;
         auto launch = [&]() { launch_ref_chunk(h, K, pr); };

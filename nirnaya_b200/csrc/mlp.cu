@@ -803,7 +803,7 @@ int nir_mlp_predict(nir_mlp* h, const float* x, int32_t n, float* y) {
     }
     try {
         MLP_CUDA(cudaSetDevice(h->device));
-        const int chunk = std::min(n, 1024);
+        const int chunk = std::min(n, 16384);
         ensure_rows(h, chunk);
         for (int r = 0; r < n; r += chunk) {
             const int k = std::min(chunk, n - r);  // a multiple of 8
