@@ -504,6 +504,33 @@ def run_learned(args, world):
     print(json.dumps(line))
 
 
+def mlp_perf(args):
+    """Throughput of the warm-start network's hand-written GEMM on a few
+    shapes and of one per-variable training step (16 -> 3 x 512 -> 8,
+    8192-sample batches); one JSON line."""
+    import numpy as np
+
+    from nirnaya_b200 import mlp
+
+    peak = 1590.0
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak = float(json.load(f)["bf16_tflops"])
+    except Exception:
+        pass
+    out = {"peak_bf16_tflops": peak, "gemm": {}}
+    with mlp.Mlp(16, 8, width=512, depth=3, seed=0) as net:
+        for shape in ((8192, 8192, 8192), (4096, 4096, 4096), (8192, 512, 512), (256, 512, 52000)):
+            tf = net.gemm_tflops(*shape, reps=10)
+            out["gemm"]["x".join(map(str, shape))] = {"tflops": tf, "frac": tf / peak}
+        rng = np.random.default_rng(0)
+        net.set_data(rng.normal(size=(262144, 16)).astype(np.float32), rng.normal(size=(262144, 8)).astype(np.float32))
+        net.train(2, 8192)
+        us, fl = net.step_stats()
+    out["train_step"] = {"us": us, "gflop": fl / 1e9, "tflops": fl / (us * 1e-6) / 1e12}
+    print(json.dumps(out))
+
+
 def reference_iterations(args):
     """Counts the reference PDHG's iterations to 1e-6 relative KKT on the
     workload: the bit-identical GPU restatement of its loop
@@ -545,6 +572,8 @@ def main():
     ap.add_argument("--ref-iterations", type=int, default=0,
                     help="count the reference loop's iterations to its stopping rule (cap), then exit")
     ap.add_argument("--ref-seconds", type=float, default=600.0)
+    ap.add_argument("--mlp-perf", action="store_true",
+                    help="throughput of the warm-start network's GEMM and training step, then exit")
     ap.add_argument("--ncu-case", action="store_true",
                     help="one short solve (--ncu-iters iterations) of the workload for an ncu capture, then exit")
     ap.add_argument("--ncu-iters", type=int, default=1024)
@@ -557,6 +586,9 @@ def main():
     wl = WORKLOADS[args.workload]
     if args.ref_iterations > 0:
         reference_iterations(args)
+        return
+    if args.mlp_perf:
+        mlp_perf(args)
         return
     if args.ncu_case:
         from nirnaya_b200 import lp as L

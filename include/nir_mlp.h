@@ -86,6 +86,11 @@ int nir_mlp_gradients(nir_mlp* h, const float* x, const float* targets, int32_t 
 int nir_mlp_gemm_check(nir_mlp* h, int a_kmaj, int b_kmaj, int32_t M, int32_t N, int32_t K, const float* A,
                        int32_t lda, const float* B, int32_t ldb, float* C);
 
+/* Mean device time (microseconds, CUDA events, after one warm-up) of the
+ * forward-layer GEMM (bias + ReLU epilogue) on M x K and N x K BF16
+ * operands, for throughput measurements: 2*M*N*K FLOP per call. */
+int nir_mlp_gemm_time(nir_mlp* h, int32_t M, int32_t N, int32_t K, int32_t reps, double* us);
+
 /* Event timing of the last nir_mlp_train: mean microseconds per minibatch
  * step (forward, loss, backward, Adam) and the tensor-core FLOPs of one
  * step (2 * batch * sum of in_l * out_l, forward plus both backward

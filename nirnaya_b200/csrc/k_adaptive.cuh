@@ -40,6 +40,20 @@ namespace nir {
 #ifndef NIR_STREAM_LOAD
 #define NIR_STREAM_LOAD 2
 #endif
+// Same choice for the per-row operands of the iteration epilogues (cost,
+// bounds, Halpern anchor), also read once per launch; streaming them
+// measured 2% slower than __ldg, so the default keeps the read-only path.
+#ifndef NIR_VEC_LOAD
+#define NIR_VEC_LOAD 0
+#endif
+template <typename T>
+__device__ __forceinline__ T vec_ld(const T* p) {
+#if NIR_VEC_LOAD == 2
+    return __ldcs(p);
+#else
+    return __ldg(p);
+#endif
+}
 template <typename T>
 __device__ __forceinline__ T stream_ld(const T* p) {
 #if NIR_STREAM_LOAD == 1
@@ -322,10 +336,10 @@ struct PrimalEpi {
     __device__ Pre prefetch(int j) const {
         Pre p;
         p.x = x[j];
-        p.c = __ldg(c + j);
-        p.lo = __ldg(lo + j);
-        p.up = __ldg(up + j);
-        p.x0 = (halpern || CHECK) ? x0[j] : T(0);
+        p.c = vec_ld(c + j);
+        p.lo = vec_ld(lo + j);
+        p.up = vec_ld(up + j);
+        p.x0 = (halpern || CHECK) ? vec_ld(x0 + j) : T(0);
         return p;
     }
     __device__ void row(int j, T aty, const Pre& p) {
@@ -363,9 +377,9 @@ struct DualEpi {
     __device__ Pre prefetch(int i) const {
         Pre p;
         p.y = y[i];
-        p.rl = __ldg(rl + i);
-        p.ru = __ldg(ru + i);
-        p.y0 = (halpern || CHECK) ? y0[i] : T(0);
+        p.rl = vec_ld(rl + i);
+        p.ru = vec_ld(ru + i);
+        p.y0 = (halpern || CHECK) ? vec_ld(y0 + i) : T(0);
         return p;
     }
     __device__ void row(int i, T ax, const Pre& p) {

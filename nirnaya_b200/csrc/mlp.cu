@@ -298,12 +298,25 @@ __global__ void k_sum_partials(int n, const float* __restrict__ part, float mul,
     if (threadIdx.x == 0) out[slot] = s * mul;
 }
 
-// db[c] = sum over rows of dY[r][c], rows in order.
-__global__ void k_colsum(int rows, int cols, const bf16* __restrict__ dy, float* __restrict__ db) {
+// db[c] = sum over rows of dY[r][c] in two deterministic passes: chunk z
+// of kColChunkRows rows -> part[z][c] (rows in order), then the chunks in
+// order.
+constexpr int kColChunkRows = 128;
+
+__global__ void k_colsum_part(int rows, int cols, const bf16* __restrict__ dy, float* __restrict__ part) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cols) return;
+    const int r0 = blockIdx.y * kColChunkRows, r1 = min(rows, r0 + kColChunkRows);
+    float s = 0.f;
+    for (int r = r0; r < r1; ++r) s += __bfloat162float(dy[(size_t)r * cols + c]);
+    part[(size_t)blockIdx.y * cols + c] = s;
+}
+
+__global__ void k_colsum_final(int chunks, int cols, const float* __restrict__ part, float* __restrict__ db) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= cols) return;
     float s = 0.f;
-    for (int r = 0; r < rows; ++r) s += __bfloat162float(dy[(size_t)r * cols + c]);
+    for (int z = 0; z < chunks; ++z) s += part[(size_t)z * cols + c];
     db[c] = s;
 }
 
@@ -370,6 +383,8 @@ struct nir_mlp {
     bf16 *g0 = nullptr, *g1 = nullptr;  // hidden-size gradient ping-pong
     float* ws = nullptr;
     size_t ws_len = 0;
+    float* colsum_ws = nullptr;
+    size_t colsum_len = 0;
     float* part = nullptr;
     float* losses = nullptr;  // device loss per step
     int losses_len = 0;
@@ -516,8 +531,18 @@ void backward(nir_mlp* h, int rows, int loss_slot) {
         // dW = g^T in   (out x in), contraction over the rows
         gemm(h, false, false, g, ly.out, in, ly.in, ly.out, ly.in, rows, EPI_F32, nullptr, nullptr, ly.gW, ly.in,
              nullptr, 0);
-        k_colsum<<<(ly.out + 255) / 256, 256, 0, h->stream>>>(rows, ly.out, g, ly.gb);
-        MLP_LAUNCHED();
+        {
+            const int chunks = (rows + kColChunkRows - 1) / kColChunkRows;
+            const size_t need = (size_t)chunks * ly.out;
+            if (need > h->colsum_len) {
+                h->release(h->colsum_ws);
+                h->colsum_ws = h->alloc<float>(need);
+                h->colsum_len = need;
+            }
+            k_colsum_part<<<dim3((ly.out + 255) / 256, chunks), 256, 0, h->stream>>>(rows, ly.out, g, h->colsum_ws);
+            k_colsum_final<<<(ly.out + 255) / 256, 256, 0, h->stream>>>(chunks, ly.out, h->colsum_ws, ly.gb);
+            MLP_LAUNCHED();
+        }
         if (l > 0) {
             bf16* gn = (g == h->g0) ? h->g1 : h->g0;
             // d(in) = g W, masked by the ReLU of the layer below
@@ -877,6 +902,41 @@ int nir_mlp_gemm_check(nir_mlp* h, int a_kmaj, int b_kmaj, int32_t M, int32_t N,
         h->release(dc);
     } catch (const std::invalid_argument& e) {
         return fail(e, true);
+    } catch (const std::exception& e) {
+        return fail(e, false);
+    }
+    return 0;
+}
+
+int nir_mlp_gemm_time(nir_mlp* h, int32_t M, int32_t N, int32_t K, int32_t reps, double* us) {
+    if (!h || !us || M < 8 || N < 8 || K < 8 || M % 8 || N % 8 || K % 8 || reps < 1) {
+        g_err = "invalid arguments";
+        return 2;
+    }
+    try {
+        MLP_CUDA(cudaSetDevice(h->device));
+        bf16* a = h->alloc<bf16>((size_t)M * K);
+        bf16* b = h->alloc<bf16>((size_t)N * K);
+        bf16* c = h->alloc<bf16>((size_t)M * N);
+        float* bias = h->alloc<float>(N);
+        cudaEvent_t e0, e1;
+        MLP_CUDA(cudaEventCreate(&e0));
+        MLP_CUDA(cudaEventCreate(&e1));
+        gemm(h, true, true, a, K, b, K, M, N, K, EPI_BIAS_RELU_BF16, bias, c, nullptr, N, nullptr, 0);  // warm-up
+        MLP_CUDA(cudaEventRecord(e0, h->stream));
+        for (int r = 0; r < reps; ++r)
+            gemm(h, true, true, a, K, b, K, M, N, K, EPI_BIAS_RELU_BF16, bias, c, nullptr, N, nullptr, 0);
+        MLP_CUDA(cudaEventRecord(e1, h->stream));
+        MLP_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        MLP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        *us = 1000.0 * ms / reps;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        h->release(a);
+        h->release(b);
+        h->release(c);
+        h->release(bias);
     } catch (const std::exception& e) {
         return fail(e, false);
     }

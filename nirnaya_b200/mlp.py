@@ -13,7 +13,7 @@ LIB_PATH = os.path.join(_HERE, "libnir_mlp.so")
 EXPORTED = [
     "nir_mlp_create", "nir_mlp_free", "nir_mlp_last_error", "nir_mlp_param_count", "nir_mlp_get_params",
     "nir_mlp_set_params", "nir_mlp_set_output_weights", "nir_mlp_set_data", "nir_mlp_train", "nir_mlp_predict",
-    "nir_mlp_gradients", "nir_mlp_gemm_check", "nir_mlp_step_stats",
+    "nir_mlp_gradients", "nir_mlp_gemm_check", "nir_mlp_gemm_time", "nir_mlp_step_stats",
 ]
 
 
@@ -50,6 +50,7 @@ def lib():
         L.nir_mlp_gemm_check.argtypes = [VP, C.c_int, C.c_int, C.c_int32, C.c_int32, C.c_int32, F, C.c_int32, F,
                                          C.c_int32, F]
         L.nir_mlp_step_stats.argtypes = [VP, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.nir_mlp_gemm_time.argtypes = [VP, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_double)]
         _lib = L
     return _lib
 
@@ -144,6 +145,12 @@ class Mlp:
         self._check(lib().nir_mlp_gemm_check(self._h, int(a_kmaj), int(b_kmaj), M, N, K, _f(A), lda, _f(B), ldb,
                                              _f(Cm)), "gemm_check")
         return Cm
+
+    def gemm_tflops(self, M, N, K, reps=20) -> float:
+        """Throughput of the forward GEMM on an M x N x K problem."""
+        us = C.c_double()
+        self._check(lib().nir_mlp_gemm_time(self._h, M, N, K, reps, C.byref(us)), "gemm_time")
+        return 2.0 * M * N * K / (us.value * 1e-6) / 1e12
 
     def step_stats(self):
         us, fl = C.c_double(), C.c_double()
