@@ -27,6 +27,7 @@
 
 #include "dev_common.cuh"
 #include "k_adaptive.cuh"
+#include "k_persistent.cuh"
 #include "k_reference.cuh"
 #include "k_setup.cuh"
 #include "k_batch.cuh"
@@ -170,6 +171,9 @@ struct nir_pdhg {
     std::vector<Occ> occ;
     bool profiling = false;
     nir_pdhg_kernel_time ktime{};
+    unsigned* gs_count = nullptr;  // grid barrier of the persistent chunk kernel
+    unsigned* gs_gen = nullptr;
+    int* gs_err = nullptr;
     int launches = 0;
 
     // zero-filled allocation with `pad` spare elements past the end (the
@@ -424,6 +428,9 @@ void create_impl(nir_pdhg* h, const nir_lp_view* lp, int device) {
     h->st = h->alloc<nir::DevState>(1);
     h->hist = h->alloc<double>(8 * nir::kHist);
     h->snap.d_seq = h->alloc<long long>(1);
+    h->gs_count = h->allocz<unsigned>(1);
+    h->gs_gen = h->allocz<unsigned>(1);
+    h->gs_err = h->allocz<int>(1);
     NIR_CUDA(cudaMemsetAsync(h->snap.d_seq, 0, sizeof(long long), s));
     NIR_CUDA(cudaHostAlloc((void**)&h->snap.ring, sizeof(nir::HostSnap) * nir::kSnapRing, cudaHostAllocMapped));
     std::memset(h->snap.ring, 0, sizeof(nir::HostSnap) * nir::kSnapRing);
@@ -527,6 +534,8 @@ struct SolveCfg {
     int restarts = 1;
     int mixed = 0;
     double bnorm = 0.0, cnorm = 0.0;
+    int persistent = 0;    // non-check iterations in one cooperative launch per chunk
+    int barrier_test = 0;  // persistent launch whose barrier cannot complete (bounded-wait test)
 };
 
 // Optional event timing of the first iteration of a chunk.
@@ -551,13 +560,44 @@ void launch_fast_chunk(nir_pdhg* h, const SolveCfg& cfg, int phase, ChunkTimer* 
     const LaunchCfg ckr = warp_cfg<double>(h, nir::k_kkt_rows<T>, h->A.nblk);
     const LaunchCfg ckc = warp_cfg<double>(h, nir::k_kkt_cols<T>, h->At.nblk);
     const size_t smem = cp1.smem, smem64 = ckr.smem;
-    for (int i = 0; i < K; ++i) {
+    int i_first = 0;
+    if (cfg.persistent && K > 1) {
+        // iterations 0..K-2 in one cooperative launch; the check pair below
+        const LaunchCfg pc = warp_cfg<T>(h, nir::k_chunk<T>, std::max(h->A.nblk, h->At.nblk));
+        nir::IterArgs ap{h->At.blk, h->At.nblk, cap, h->At.rp, h->At.ci, L.P, h->st, 0, cfg.halpern, phase,
+                         cfg.p.reflection};
+        nir::IterArgs ad{h->A.blk, h->A.nblk, cap, h->A.rp, h->A.ci, L.D, h->st, 0, cfg.halpern, phase,
+                         cfg.p.reflection};
+        nir::ChunkPtrs<T> v{View<T>::valAt(h), View<T>::valA(h), View<T>::x(h), View<T>::xb(h), View<T>::xp(h),
+                            View<T>::y(h),     View<T>::yp(h),   View<T>::c(h), View<T>::l(h),  View<T>::u(h),
+                            View<T>::x0(h),    View<T>::rl(h),   View<T>::ru(h), View<T>::y0(h)};
+        // ~1 s of SM clock per wait; 0.1 s and one CTA too many in the test
+        nir::GridSync gs{h->gs_count, h->gs_gen, h->gs_err, unsigned(pc.grid) + (cfg.barrier_test ? 1u : 0u),
+                         cfg.barrier_test ? 200000000LL : 2000000000LL};
+        nir::DevState* st = h->st;
+#ifdef NIR_DEBUG_CHUNK_ONE_ITER
+        for (int it = 0; it < K - 1; ++it) {
+            int i0 = it, iters = 1;
+            void* args[] = {&ap, &ad, &v, &i0, &iters, &gs, &st};
+            NIR_CUDA(cudaLaunchCooperativeKernel((const void*)nir::k_chunk<T>, dim3(pc.grid), dim3(nir::kBlock), args,
+                                                 pc.smem, s));
+        }
+#else
+        int i0 = 0, iters = K - 1;
+        void* args[] = {&ap, &ad, &v, &i0, &iters, &gs, &st};
+        NIR_CUDA(cudaLaunchCooperativeKernel((const void*)nir::k_chunk<T>, dim3(pc.grid), dim3(nir::kBlock), args,
+                                             pc.smem, s));
+#endif
+        h->launches += 1;
+        i_first = K - 1;
+    }
+    for (int i = i_first; i < K; ++i) {
         const bool check = (i == K - 1);
         nir::IterArgs ap{h->At.blk, h->At.nblk, cap, h->At.rp, h->At.ci, L.P, h->st, i, cfg.halpern, phase,
                          cfg.p.reflection};
         nir::IterArgs ad{h->A.blk, h->A.nblk, cap, h->A.rp, h->A.ci, L.D, h->st, i, cfg.halpern, phase,
                          cfg.p.reflection};
-        const bool timed = tm && tm->armed && i == 0;
+        const bool timed = tm && tm->armed && i == 0 && !cfg.persistent;
         if (timed) NIR_CUDA(cudaEventRecord(tm->e[0], s));
         if (check)
             nir::k_primal<T, true><<<cp1.grid, nir::kBlock, smem, s>>>(
@@ -659,6 +699,7 @@ unsigned long long chunk_key(const nir_pdhg* h, const SolveCfg& c, int phase, bo
     k.add(c.p.reflection).add(c.p.restart_sufficient).add(c.p.restart_necessary).add(c.p.restart_artificial);
     k.add(c.p.primal_weight_smoothing).add(c.p.polish_stall_checks).add(c.p.polish_switch_kkt).add(c.p.tol);
     k.add(c.p.feas_tol).add(c.p.restart_anchor).add(c.p.primal_weight_decades).add(c.p.polish_fresh).add(h->offset).add(h->A.cap).add(h->A.blk).add(h->At.blk).add(h->part).add(h->hist);
+    k.add(c.persistent).add(c.barrier_test);
     return k.h;
 }
 
@@ -1104,6 +1145,21 @@ int solve_fast(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), void* 
     cfg.halpern = pdlp ? 1 : 0;
     cfg.restarts = pdlp ? 1 : 0;
     cfg.mixed = (p.precision == NIR_PREC_MIXED) ? 1 : 0;
+    {
+        // persistent chunks on request (not while profiling, whose per-kernel
+        // events need the two-kernel path)
+        int coop = 0;
+        NIR_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, h->device));
+        const bool want = p.persistent == 1 || p.persistent == 2;
+        if (want && !coop) throw std::invalid_argument("persistent chunks need cooperative launch support");
+        cfg.persistent = (want && coop && !h->profiling) ? 1 : 0;
+        cfg.barrier_test = (cfg.persistent && p.persistent == 2) ? 1 : 0;
+        if (cfg.persistent) {
+            NIR_CUDA(cudaMemsetAsync(h->gs_count, 0, sizeof(unsigned), s));
+            NIR_CUDA(cudaMemsetAsync(h->gs_gen, 0, sizeof(unsigned), s));
+            NIR_CUDA(cudaMemsetAsync(h->gs_err, 0, sizeof(int), s));
+        }
+    }
     cfg.bnorm = rhs_norm(h);
     cfg.cnorm = norm2(h->h_c);
     h->ktime = nir_pdhg_kernel_time{};
@@ -1203,7 +1259,7 @@ int solve_fast(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), void* 
                 else launch_fast_chunk<float>(h, cfg, phase, h->profiling ? &tm : nullptr);
             };
             const int per = launches_per_chunk(cfg.K, false);
-            if (p.use_graphs && !h->profiling) {
+            if (p.use_graphs && !h->profiling && !cfg.persistent) {
                 cudaGraphExec_t ge = chunk_graph(h, 1 + phase, chunk_key(h, cfg, phase, f64), launch);
                 return run_chunks(h, p, poll, ctx, t0, phase, per, [&]() { NIR_CUDA(cudaGraphLaunch(ge, s)); }, nullptr);
             }
@@ -1290,6 +1346,7 @@ int solve_fast(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), void* 
     info->solve_seconds = now_sec() - t_setup;
     info->time_to_fp64_seconds = t_switch;
     info->iterations_to_tol = (status == NIR_STATUS_OPTIMAL) ? st.iter : -1;
+    if (status == NIR_STATUS_INTERNAL_ERROR) g_err = "a grid barrier of the persistent chunk kernel exceeded its wait bound";
     return status;
 }
 
@@ -1329,6 +1386,7 @@ int nir_pdhg_default_params(nir_pdhg_params* p) {
     p->y_init = nullptr;
     p->omega_init = 0.0;
     p->primal_weight_decades = 1.0;
+    p->persistent = 0;
     return 0;
 }
 

@@ -40,6 +40,16 @@ namespace nir {
 #ifndef NIR_STREAM_LOAD
 #define NIR_STREAM_LOAD 2
 #endif
+// Gathers of the multiplied vector.  A kernel that runs several
+// iterations (the persistent chunk kernel) rewrites that vector between
+// its grid barriers, so it must gather through L2 (coherent, ld.global.cg)
+// rather than through the read-only path, which may serve a stale line.
+template <bool COH, typename T>
+__device__ __forceinline__ T gather_ld(const T* p) {
+    if (COH) return __ldcg(p);
+    return __ldg(p);
+}
+
 // Same choice for the per-row operands of the iteration epilogues (cost,
 // bounds, Halpern anchor), also read once per launch; streaming them
 // measured 2% slower than __ldg, so the default keeps the read-only path.
@@ -115,7 +125,7 @@ __device__ __forceinline__ void stream_load(int2 d0, int2 d1, int cap, const int
 //    leader applies the epilogue.
 //  * One long row: the warp strides over it from global memory, 256
 //    nonzeros per round.
-template <typename TA, typename TV, typename TX, class Epi>
+template <typename TA, typename TV, typename TX, class Epi, bool COH = false>
 __device__ __forceinline__ void warp_process(int2 d0, int2 d1, int cap, const int* __restrict__ rp,
                                              const int* __restrict__ ci, const TV* __restrict__ val,
                                              const TX* __restrict__ x, Epi& epi, TA* s_prod, const int (&c)[kWarpU],
@@ -145,7 +155,7 @@ __device__ __forceinline__ void warp_process(int2 d0, int2 d1, int cap, const in
         for (int base = p0 + lane; base < p1; base += 32 * U) {
             TX xv[U];
 #pragma unroll
-            for (int q = 0; q < U; ++q) xv[q] = (base + 32 * q < p1) ? __ldg(x + cc[q]) : TX(0);
+            for (int q = 0; q < U; ++q) xv[q] = (base + 32 * q < p1) ? gather_ld<COH>(x + cc[q]) : TX(0);
             const int nb = base + 32 * U;
             int cn[U];
             TV vn[U];
@@ -184,7 +194,7 @@ __device__ __forceinline__ void warp_process(int2 d0, int2 d1, int cap, const in
     const bool mine = r < r1;
     TX xv[U];
 #pragma unroll
-    for (int q = 0; q < U; ++q) xv[q] = (lane + 32 * q < nnzb) ? __ldg(x + c[q]) : TX(0);
+    for (int q = 0; q < U; ++q) xv[q] = (lane + 32 * q < nnzb) ? gather_ld<COH>(x + c[q]) : TX(0);
     if (mine && tl == 0) pre = epi.prefetch(r);
     int ra = 0, re = 0;
     if (mine) {
@@ -209,7 +219,7 @@ __device__ __forceinline__ void warp_process(int2 d0, int2 d1, int cap, const in
 // stream and the descriptor after that are already in flight (register
 // double buffering).  The per-row reduction order depends only on the
 // layout, so results do not depend on the grid.
-template <typename TA, typename TV, typename TX, class Epi>
+template <typename TA, typename TV, typename TX, class Epi, bool COH = false>
 __device__ __forceinline__ void rowblock_spmv(const int2* __restrict__ blk, int nblk, int cap,
                                               const int* __restrict__ rp, const int* __restrict__ ci,
                                               const TV* __restrict__ val, const TX* __restrict__ x, Epi& epi,
@@ -239,7 +249,7 @@ __device__ __forceinline__ void rowblock_spmv(const int2* __restrict__ blk, int 
             m0 = __ldg(blk + b + 2 * G);
             m1 = __ldg(blk + b + 2 * G + 1);
         }
-        warp_process<TA, TV, TX>(d0, d1, cap, rp, ci, val, x, epi, s_prod, c, v);
+        warp_process<TA, TV, TX, Epi, COH>(d0, d1, cap, rp, ci, val, x, epi, s_prod, c, v);
         if (!has_next) break;
 #pragma unroll
         for (int q = 0; q < kWarpU; ++q) {
@@ -413,13 +423,13 @@ struct IterArgs {
     double rho;
 };
 
-template <typename T, bool CHECK>
-__global__ void __launch_bounds__(kBlock, iter_min_blocks<T>()) k_primal(IterArgs a, const T* __restrict__ val, const T* __restrict__ y,
-                                                   T* __restrict__ x, T* __restrict__ xbar, T* __restrict__ xplus,
-                                                   const T* __restrict__ c, const T* __restrict__ lo,
-                                                   const T* __restrict__ up, const T* __restrict__ x0) {
-    __shared__ double s_red[kWarps];
-    if (a.st->done || a.st->phase != a.phase) return;
+// One primal / dual half-iteration over all warp row blocks (the body of
+// k_primal / k_dual and of the persistent chunk kernel's phases).
+template <typename T, bool CHECK, bool COH>
+__device__ __forceinline__ void primal_phase(const IterArgs& a, const T* __restrict__ val, const T* __restrict__ y,
+                                             T* __restrict__ x, T* __restrict__ xbar, T* __restrict__ xplus,
+                                             const T* __restrict__ c, const T* __restrict__ lo,
+                                             const T* __restrict__ up, const T* __restrict__ x0, double* s_red) {
     PrimalEpi<T, CHECK> epi;
     epi.x = x;
     epi.xbar = xbar;
@@ -430,16 +440,15 @@ __global__ void __launch_bounds__(kBlock, iter_min_blocks<T>()) k_primal(IterArg
     epi.x0 = x0;
     epi.s = step_scalars<T>(a.st, a.i_in_chunk, a.halpern, a.rho);
     epi.halpern = a.halpern;
-    rowblock_spmv<T, T, T>(a.blk, a.nblk, a.cap, a.rp, a.ci, val, y, epi, reinterpret_cast<T*>(s_red));
+    rowblock_spmv<T, T, T, PrimalEpi<T, CHECK>, COH>(a.blk, a.nblk, a.cap, a.rp, a.ci, val, y, epi,
+                                                       reinterpret_cast<T*>(s_red));
     if (CHECK) write_partials(epi, a.part, s_red);
 }
 
-template <typename T, bool CHECK>
-__global__ void __launch_bounds__(kBlock, iter_min_blocks<T>()) k_dual(IterArgs a, const T* __restrict__ val, const T* __restrict__ xbar,
-                                                 T* __restrict__ y, T* __restrict__ yplus, const T* __restrict__ rl,
-                                                 const T* __restrict__ ru, const T* __restrict__ y0) {
-    __shared__ double s_red[kWarps];
-    if (a.st->done || a.st->phase != a.phase) return;
+template <typename T, bool CHECK, bool COH>
+__device__ __forceinline__ void dual_phase(const IterArgs& a, const T* __restrict__ val, const T* __restrict__ xbar,
+                                           T* __restrict__ y, T* __restrict__ yplus, const T* __restrict__ rl,
+                                           const T* __restrict__ ru, const T* __restrict__ y0, double* s_red) {
     DualEpi<T, CHECK> epi;
     epi.y = y;
     epi.yplus = yplus;
@@ -448,8 +457,28 @@ __global__ void __launch_bounds__(kBlock, iter_min_blocks<T>()) k_dual(IterArgs 
     epi.y0 = y0;
     epi.s = step_scalars<T>(a.st, a.i_in_chunk, a.halpern, a.rho);
     epi.halpern = a.halpern;
-    rowblock_spmv<T, T, T>(a.blk, a.nblk, a.cap, a.rp, a.ci, val, xbar, epi, reinterpret_cast<T*>(s_red));
+    rowblock_spmv<T, T, T, DualEpi<T, CHECK>, COH>(a.blk, a.nblk, a.cap, a.rp, a.ci, val, xbar, epi,
+                                                     reinterpret_cast<T*>(s_red));
     if (CHECK) write_partials(epi, a.part, s_red);
+}
+
+template <typename T, bool CHECK>
+__global__ void __launch_bounds__(kBlock, iter_min_blocks<T>()) k_primal(IterArgs a, const T* __restrict__ val, const T* __restrict__ y,
+                                                   T* __restrict__ x, T* __restrict__ xbar, T* __restrict__ xplus,
+                                                   const T* __restrict__ c, const T* __restrict__ lo,
+                                                   const T* __restrict__ up, const T* __restrict__ x0) {
+    __shared__ double s_red[kWarps];
+    if (a.st->done || a.st->phase != a.phase) return;
+    primal_phase<T, CHECK, false>(a, val, y, x, xbar, xplus, c, lo, up, x0, s_red);
+}
+
+template <typename T, bool CHECK>
+__global__ void __launch_bounds__(kBlock, iter_min_blocks<T>()) k_dual(IterArgs a, const T* __restrict__ val, const T* __restrict__ xbar,
+                                                 T* __restrict__ y, T* __restrict__ yplus, const T* __restrict__ rl,
+                                                 const T* __restrict__ ru, const T* __restrict__ y0) {
+    __shared__ double s_red[kWarps];
+    if (a.st->done || a.st->phase != a.phase) return;
+    dual_phase<T, CHECK, false>(a, val, xbar, y, yplus, rl, ru, y0, s_red);
 }
 
 // ---------------------------------------------------------------- KKT (FP64)

@@ -50,7 +50,8 @@ class Params(C.Structure):
         ("polish_switch_kkt", C.c_double), ("spmv_block_nnz", C.c_int32), ("use_graphs", C.c_int32),
         ("verbose", C.c_int32), ("restart_anchor", C.c_int32), ("polish_fresh", C.c_int32),
         ("x_init", C.POINTER(C.c_double)), ("y_init", C.POINTER(C.c_double)),
-        ("omega_init", C.c_double), ("primal_weight_decades", C.c_double),
+        ("omega_init", C.c_double), ("primal_weight_decades", C.c_double), ("persistent", C.c_int32),
+        ("pad_", C.c_int32),
     ]
 
 

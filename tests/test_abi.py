@@ -47,7 +47,7 @@ def test_structs_match_header_sizes():
     assert C.sizeof(NirLpView) == 4 + 4 + 8 + 8 * 8 + 8
     # nir_pdhg_params: 2 int32, 2 double, int64, double, 3 int32, 5 double,
     # double, 2 int32, double, 5 int32 (+pad), 2 pointers, 2 double
-    assert C.sizeof(pdhg.Params) == 176
+    assert C.sizeof(pdhg.Params) == 184
     assert C.sizeof(pdhg.Info) == 4 + 4 + 8 + 8 + 8 * 11 + 4 + 4 + 8
 
 

@@ -302,3 +302,39 @@ def test_reference_loop_kkt_probe_matches_oracle():
     with pdhg.Engine(lp) as eng:
         _, _, off = eng.solve(pdhg.default_params(algorithm=pdhg.ALGO_REFERENCE, max_iters=60000, tol=0.0))
     assert off.iterations_to_tol == -1 and np.isnan(off.rel_kkt)
+
+
+@pytest.mark.parametrize("prec", [pdhg.PREC_FP64, pdhg.PREC_MIXED])
+def test_persistent_chunks_are_bit_identical_to_two_kernel_path(prec):
+    # one cooperative launch per chunk with grid barriers runs the same row
+    # blocks in the same order as the per-iteration kernels
+    # the third LP (a 9000-nonzero row, empty rows) exercises the long-row
+    # path over a fixed number of iterations; the first two are solved
+    cases = [(L.generate(L.RANDOM_EQ, 3, m=500, n=1250), 200000),
+             (L.generate(L.BLEND_FAMILY, 3, m=1000, n=2500, target_nnz=20000), 200000),
+             (dense_row_lp(), 3200)]
+    for lp, cap in cases:
+        with pdhg.Engine(lp) as eng:
+            base = dict(precision=prec, tol=1e-6, max_iters=cap, spmv_block_nnz=64)
+            x0, y0, i0 = eng.solve(pdhg.default_params(persistent=0, **base))
+            x1, y1, i1 = eng.solve(pdhg.default_params(persistent=1, **base))
+        assert i1.status == i0.status
+        assert i0.status == (pdhg.OPTIMAL if cap > 3200 else pdhg.ITERATION_LIMIT)
+        assert i1.iterations == i0.iterations
+        assert np.array_equal(G.bits(x0), G.bits(x1)) and np.array_equal(G.bits(y0), G.bits(y1))
+        assert i1.kernel_launches < i0.kernel_launches
+
+
+def test_persistent_barrier_wait_is_bounded():
+    # persistent=2 launches one CTA fewer than the barrier waits for: every
+    # wait must give up after its bound, the solve must end with an internal
+    # error, and the handle (and the CUDA context) must stay usable
+    lp = L.generate(L.RANDOM_EQ, 4, m=300, n=700)
+    with pdhg.Engine(lp) as eng:
+        t = time.perf_counter()
+        with pytest.raises(RuntimeError, match="internal_error"):
+            eng.solve(pdhg.default_params(persistent=2, max_iters=5000))
+        assert time.perf_counter() - t < 10.0
+        x, y, info = eng.solve(pdhg.default_params(persistent=1))
+        assert info.status == pdhg.OPTIMAL
+        assert ffi.rel_kkt(lp, x, y).rel_kkt <= 1.05e-6
