@@ -575,19 +575,10 @@ void launch_fast_chunk(nir_pdhg* h, const SolveCfg& cfg, int phase, ChunkTimer* 
         nir::GridSync gs{h->gs_count, h->gs_gen, h->gs_err, unsigned(pc.grid) + (cfg.barrier_test ? 1u : 0u),
                          cfg.barrier_test ? 200000000LL : 2000000000LL};
         nir::DevState* st = h->st;
-#ifdef NIR_DEBUG_CHUNK_ONE_ITER
-        for (int it = 0; it < K - 1; ++it) {
-            int i0 = it, iters = 1;
-            void* args[] = {&ap, &ad, &v, &i0, &iters, &gs, &st};
-            NIR_CUDA(cudaLaunchCooperativeKernel((const void*)nir::k_chunk<T>, dim3(pc.grid), dim3(nir::kBlock), args,
-                                                 pc.smem, s));
-        }
-#else
         int i0 = 0, iters = K - 1;
         void* args[] = {&ap, &ad, &v, &i0, &iters, &gs, &st};
         NIR_CUDA(cudaLaunchCooperativeKernel((const void*)nir::k_chunk<T>, dim3(pc.grid), dim3(nir::kBlock), args,
                                              pc.smem, s));
-#endif
         h->launches += 1;
         i_first = K - 1;
     }

@@ -74,10 +74,6 @@ struct ChunkPtrs {
     const T *c, *l, *u, *x0, *rl, *ru, *y0;
 };
 
-#ifndef NIR_CHUNK_COH
-#define NIR_CHUNK_COH true
-#endif
-
 template <typename T>
 __global__ void __launch_bounds__(kBlock, iter_min_blocks<T>()) k_chunk(IterArgs ap, IterArgs ad, ChunkPtrs<T> v,
                                                                         int i0, int iters, GridSync gs, DevState* st) {
@@ -87,9 +83,9 @@ __global__ void __launch_bounds__(kBlock, iter_min_blocks<T>()) k_chunk(IterArgs
     for (int i = i0; i < i0 + iters; ++i) {
         ap.i_in_chunk = i;
         ad.i_in_chunk = i;
-        primal_phase<T, false, NIR_CHUNK_COH>(ap, v.valAt, v.y, v.x, v.xb, v.xp, v.c, v.l, v.u, v.x0, s_red);
+        primal_phase<T, false, true>(ap, v.valAt, v.y, v.x, v.xb, v.xp, v.c, v.l, v.u, v.x0, s_red);
         if (!grid_sync(gs)) break;
-        dual_phase<T, false, NIR_CHUNK_COH>(ad, v.valA, v.xb, v.y, v.yp, v.rl, v.ru, v.y0, s_red);
+        dual_phase<T, false, true>(ad, v.valA, v.xb, v.y, v.yp, v.rl, v.ru, v.y0, s_red);
         if (!grid_sync(gs)) break;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0 && *(volatile int*)gs.err) {
