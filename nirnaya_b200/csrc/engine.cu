@@ -115,6 +115,11 @@ struct Orient {
     int cap = 0;
     int nblk = 0;
     int2* blk = nullptr;  // (first row, first nonzero) of each row block, plus an end entry
+    struct Layout {
+        int cap, nblk;
+        int2* blk;
+    };
+    std::vector<Layout> layouts;  // every layout built so far, one per capacity used
 };
 
 struct Snapshot {
@@ -229,12 +234,22 @@ using nir::check_row_blocks;
 
 void set_blocks(nir_pdhg* h, Orient& o, int cap) {
     if (o.cap == cap && o.blk) return;
+    // a capacity used before keeps its device copy: switching back and forth
+    // (the autotuner, or solves with different spmv_block_nnz) allocates once
+    for (const auto& l : o.layouts)
+        if (l.cap == cap) {
+            o.blk = l.blk;
+            o.nblk = l.nblk;
+            o.cap = cap;
+            return;
+        }
     std::vector<int2> b = build_row_blocks(o.h_rp, cap);
     check_row_blocks(b, o.h_rp, cap);
     o.nblk = int(b.size()) - 1;
     o.blk = h->alloc<int2>(b.size());
     h2d(h, o.blk, b.data(), b.size() * sizeof(int2));
     o.cap = cap;
+    o.layouts.push_back({cap, o.nblk, o.blk});
 }
 
 // Warp row-block capacity: 256 nonzeros (8 per lane) when the matrix gives
