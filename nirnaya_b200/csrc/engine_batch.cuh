@@ -20,6 +20,15 @@ struct nir_pdhg_batch {
     int nblkA = 0, nblkAt = 0;
     int *d_a_lo = nullptr, *d_at_lo = nullptr;
     double* part = nullptr;
+    struct Layout {
+        int cap;
+        int2 *blkA, *blkAt;
+        int *instA, *instAt;
+        int nblkA, nblkAt;
+        int *a_lo, *at_lo;
+        double* part;
+    };
+    std::vector<Layout> layouts;  // one per capacity used, built once each
     nir::DevState* insts = nullptr;
     double *d_bnorm = nullptr, *d_cnorm = nullptr, *d_offset = nullptr, *d_norm = nullptr;
     ChunkGraph graphs[2];
@@ -218,9 +227,27 @@ int batch_solve_impl(nir_pdhg_batch* B, const nir_pdhg_params& p, int (*poll)(vo
         throw std::invalid_argument("invalid parameters");
     const int cap = pick_cap(h, p);  // timed on the block-diagonal matrix
     if (B->cap != cap) {
-        batch_blocks(B, h->A.h_rp, B->row_off, cap, &B->blkA, &B->instA, &B->nblkA, &B->d_a_lo);
-        batch_blocks(B, h->At.h_rp, B->col_off, cap, &B->blkAt, &B->instAt, &B->nblkAt, &B->d_at_lo);
-        B->part = h->alloc<double>(6 * size_t(std::max(B->nblkA, 1)) + 6 * size_t(std::max(B->nblkAt, 1)));
+        bool found = false;
+        for (const auto& l : B->layouts)
+            if (l.cap == cap) {
+                B->blkA = l.blkA;
+                B->blkAt = l.blkAt;
+                B->instA = l.instA;
+                B->instAt = l.instAt;
+                B->nblkA = l.nblkA;
+                B->nblkAt = l.nblkAt;
+                B->d_a_lo = l.a_lo;
+                B->d_at_lo = l.at_lo;
+                B->part = l.part;
+                found = true;
+            }
+        if (!found) {
+            batch_blocks(B, h->A.h_rp, B->row_off, cap, &B->blkA, &B->instA, &B->nblkA, &B->d_a_lo);
+            batch_blocks(B, h->At.h_rp, B->col_off, cap, &B->blkAt, &B->instAt, &B->nblkAt, &B->d_at_lo);
+            B->part = h->alloc<double>(6 * size_t(std::max(B->nblkA, 1)) + 6 * size_t(std::max(B->nblkAt, 1)));
+            B->layouts.push_back({cap, B->blkA, B->blkAt, B->instA, B->instAt, B->nblkA, B->nblkAt, B->d_a_lo,
+                                  B->d_at_lo, B->part});
+        }
         B->cap = cap;
     }
     SolveCfg cfg;
