@@ -246,7 +246,8 @@ class Options:
     pdhg_precision: int = PREC_MIXED
     pdhg_tol: float = 1e-6
     pdhg_feas_tol: float = 0.0
-    pdhg_max_iters: int = 0            # 0 = the reference's max(5000, simplex_iter_limit // 10)
+    pdhg_max_iters: int = 0            # 0 = the reference's max(5000, simplex_iter_limit // 10),
+                                       # times 10 for the restarted methods (as the C++ drop-in)
     device: int = 0
     extra: dict = field(default_factory=dict)
 
@@ -281,7 +282,8 @@ class PdhgSolver:
 
     @staticmethod
     def params_from(options: Options) -> Params:
-        cap = options.pdhg_max_iters or max(5000, options.simplex_iter_limit // 10)
+        ref_cap = max(5000, options.simplex_iter_limit // 10)
+        cap = options.pdhg_max_iters or (ref_cap if options.pdhg_algorithm == ALGO_REFERENCE else 10 * ref_cap)
         p = default_params(algorithm=options.pdhg_algorithm, precision=options.pdhg_precision,
                            tol=options.pdhg_tol, feas_tol=options.pdhg_feas_tol, max_iters=cap)
         for k, v in options.extra.items():

@@ -99,3 +99,17 @@ def test_params_defaults_roundtrip():
     p = pdhg.default_params()
     assert p.algorithm == pdhg.ALGO_PDLP and p.precision == pdhg.PREC_MIXED and p.tol == 1e-6
     assert p.check_every == 64 and p.reflection == 1.0 and p.use_graphs == 1
+
+
+def test_python_solver_mirror_uses_the_dropin_iteration_cap():
+    # as nirnaya_b200/sov/pdhg_solver.hpp: the reference's cap
+    # max(5000, simplex_iter_limit / 10) for its own loop, ten times that
+    # for the restarted methods, whose iterations replace many plain ones
+    from nirnaya_b200 import pdhg
+
+    p = pdhg.PdhgSolver.params_from(pdhg.Options(simplex_iter_limit=500000))
+    assert p.max_iters == 500000 and p.algorithm == pdhg.ALGO_PDLP
+    p = pdhg.PdhgSolver.params_from(pdhg.Options(simplex_iter_limit=1000, pdhg_algorithm=pdhg.ALGO_REFERENCE))
+    assert p.max_iters == 5000
+    p = pdhg.PdhgSolver.params_from(pdhg.Options(pdhg_max_iters=123, extra={"check_every": 32}))
+    assert p.max_iters == 123 and p.check_every == 32
