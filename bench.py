@@ -615,10 +615,10 @@ def main():
             eng.solve(pdhg.default_params(precision=wl["precision"], max_iters=args.ncu_iters, tol=0.0,
                                           spmv_block_nnz=args.ncu_cap))
         return
-    rank, world, local = dist_setup(args.gpus)
-
     if args.impl == "reference":
-        if rank != 0:
+        # the reference runs on the host cores of rank 0; the other ranks of a
+        # torchrun launch have nothing to do and open no process group
+        if int(os.environ.get("RANK", "0")) != 0:
             return
         from nirnaya_b200 import lp as L
 
@@ -665,6 +665,19 @@ def main():
         print(json.dumps(line))
         return
 
+    rank, world, local = dist_setup(args.gpus)
+    try:
+        run_arm(args, wl, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            if dist.is_initialized():
+                dist.destroy_process_group()
+
+
+def run_arm(args, wl, rank, world, local):
+    """Our arm: one JSON line from rank 0."""
     if wl.get("learned"):
         if rank == 0:
             run_learned(args, world)
@@ -695,7 +708,10 @@ def main():
                 "launch_us": us, "launches": its, "share_s": us * its * 1e-6,
                 "algorithmic_bytes_per_launch": alg, "achieved_GBs": alg / (us * 1e-6) / 1e9,
                 "iteration_us": kt.iter_us[q], "tag": tag}
-    dom_name, dom = max(kernels.items(), key=lambda kv: kv[1]["share_s"])
+    if kernels:
+        dom_name, dom = max(kernels.items(), key=lambda kv: kv[1]["share_s"])
+    else:  # no timed chunk (a solve that ended inside its first chunk)
+        dom_name, dom = "none", {"achieved_GBs": None, "algorithmic_bytes_per_launch": None, "launch_us": None}
     achieved = dom["achieved_GBs"]
     traffic = committed_traffic(f"{dom_name}:{wl['label']}")
     cpu = cpu_baseline(lp, wl["label"], seconds=args.cpu_seconds)
@@ -726,7 +742,7 @@ def main():
                 "d2h_bytes_per_step": 8 * (lp.ncol + lp.nrow)},
         "gpu_launches": r["launches"],
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic,
+                     "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                      "kernel": f"{dom_name} (fused CSR-adaptive SpMV + update), dominant by time in the solve",
                      "algorithmic_bytes_per_launch": dom["algorithmic_bytes_per_launch"],
                      "launch_us": dom["launch_us"],
