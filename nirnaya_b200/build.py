@@ -3,6 +3,7 @@
   nirnaya_b200/libnir_pdhg.so   CUDA engine + C ABI (nvcc, sm_100a only)
   nirnaya_b200/libnir_lpgen.so  seeded instance generator (g++)
   nirnaya_b200/libnir_mlp.so    warm-start network (nvcc, sm_100a)
+  nirnaya_b200/libnir_mps.so    multi-threaded MPS reader (g++, host only)
 
 Run `python -m nirnaya_b200.build` or call build_all().
 """
@@ -79,8 +80,21 @@ def build_lpgen(force: bool = False, verbose: bool = False) -> str:
     return target
 
 
+def build_mps(force: bool = False, verbose: bool = False) -> str:
+    target = os.path.join(HERE, "libnir_mps.so")
+    srcs = [os.path.join(CSRC, "mps.cpp"), os.path.join(INC, "nir_mps.h"), os.path.join(INC, "nir_lp.h")]
+    if force or _stale(target, srcs):
+        cxx = os.environ.get("CXX", "g++")
+        cmd = [cxx, "-std=c++17", "-O3", "-fPIC", "-shared", "-pthread", "-I" + INC, srcs[0], "-o", target]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+    return target
+
+
 def build_all(force: bool = False, verbose: bool = False) -> None:
     build_lpgen(force, verbose)
+    build_mps(force, verbose)
     build_engine(force, verbose)
     build_mlp(force, verbose)
 

@@ -101,6 +101,12 @@ def ref_lib():
         lib.ref_read_mps.argtypes = [C.c_char_p]
         lib.ref_model_view.argtypes = [C.c_void_p, _VP, C.POINTER(C.c_int)]
         lib.ref_model_free.argtypes = [C.c_void_p]
+        lib.ref_last_status.restype = C.c_int
+        lib.ref_model_vartypes.argtypes = [C.c_void_p, C.POINTER(C.c_int8)]
+        lib.ref_model_qnnz.restype = C.c_int64
+        lib.ref_model_qnnz.argtypes = [C.c_void_p]
+        lib.ref_model_q.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int32), _D]
+        lib.ref_write_mps.argtypes = [_VP, C.POINTER(C.c_int8), C.c_int, C.c_char_p]
         _ref = lib
     return _ref
 
@@ -216,6 +222,21 @@ def ref_dd_probe(a, b, c):
     return d.value, nsum.value
 
 
+def _ref_model_lp(lib, h):
+    v = NirLpView()
+    sense = C.c_int()
+    lib.ref_model_view(h, C.byref(v), C.byref(sense))
+
+    def cp(p, n, dt):
+        return np.ctypeslib.as_array(p, shape=(n,)).astype(dt, copy=True) if n else np.zeros(0, dt)
+
+    lp = LP(v.nrow, v.ncol, cp(v.col_start, v.ncol + 1, np.int64), cp(v.row_index, v.nnz, np.int32),
+            cp(v.value, v.nnz, np.float64), cp(v.cost, v.ncol, np.float64), cp(v.collo, v.ncol, np.float64),
+            cp(v.colup, v.ncol, np.float64), cp(v.rowlo, v.nrow, np.float64), cp(v.rowup, v.nrow, np.float64),
+            v.obj_offset)
+    return lp, sense.value
+
+
 def ref_read_mps(path: str):
     """MpsReader::read + to_internal_min; returns (LP, sense)."""
     lib = ref_lib()
@@ -223,17 +244,48 @@ def ref_read_mps(path: str):
     if not h:
         raise RuntimeError(lib.ref_last_error().decode())
     try:
-        v = NirLpView()
-        sense = C.c_int()
-        lib.ref_model_view(h, C.byref(v), C.byref(sense))
-
-        def cp(p, n, dt):
-            return np.ctypeslib.as_array(p, shape=(n,)).astype(dt, copy=True) if n else np.zeros(0, dt)
-
-        lp = LP(v.nrow, v.ncol, cp(v.col_start, v.ncol + 1, np.int64), cp(v.row_index, v.nnz, np.int32),
-                cp(v.value, v.nnz, np.float64), cp(v.cost, v.ncol, np.float64), cp(v.collo, v.ncol, np.float64),
-                cp(v.colup, v.ncol, np.float64), cp(v.rowlo, v.nrow, np.float64), cp(v.rowup, v.nrow, np.float64),
-                v.obj_offset)
-        return lp, sense.value
+        return _ref_model_lp(lib, h)
     finally:
         lib.ref_model_free(h)
+
+
+class RefMpsError(RuntimeError):
+    """A failed MpsReader::read: status is the sov::Status code, or -1 when
+    the reader let an exception escape (std::stod on a bad number)."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"status {status}: {message}")
+        self.status = status
+        self.message = message
+
+
+def ref_read_mps_full(path: str):
+    """MpsReader::read + to_internal_min: (LP, sense, vartype, (q_start,
+    q_index, q_value)); raises RefMpsError on failure."""
+    lib = ref_lib()
+    h = lib.ref_read_mps(path.encode())
+    if not h:
+        raise RefMpsError(lib.ref_last_status(), lib.ref_last_error().decode(errors="replace"))
+    try:
+        lp, sense = _ref_model_lp(lib, h)
+        vt = np.zeros(lp.ncol, np.int8)
+        lib.ref_model_vartypes(h, vt.ctypes.data_as(C.POINTER(C.c_int8)))
+        qn = lib.ref_model_qnnz(h)
+        qs = np.zeros(lp.ncol + 1, np.int64)
+        qi = np.zeros(qn, np.int32)
+        qv = np.zeros(qn, np.float64)
+        lib.ref_model_q(h, qs.ctypes.data_as(C.POINTER(C.c_int64)), qi.ctypes.data_as(C.POINTER(C.c_int32)),
+                        _dptr(qv))
+        return lp, sense, vt, (qs, qi, qv)
+    finally:
+        lib.ref_model_free(h)
+
+
+def ref_write_mps(lp: LP, path: str, vartype=None, sense: int = 1) -> None:
+    """MpsReader::write of an LP (names C<j> / R<i>, objective row OBJ)."""
+    vt = None if vartype is None else np.ascontiguousarray(vartype, np.int8)
+    rc = ref_lib().ref_write_mps(C.byref(lp.view()),
+                                 None if vt is None else vt.ctypes.data_as(C.POINTER(C.c_int8)), int(sense),
+                                 path.encode())
+    if rc != 0:
+        raise RuntimeError(f"MpsReader::write failed on {path}")

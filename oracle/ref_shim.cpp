@@ -12,6 +12,7 @@
 //   ref_spmv(_t)        sov::CscMatrix::spmv(_transpose) src/core/csc_matrix.hpp:99-120
 //   ref_from_triplets   sov::CscMatrix::from_triplets src/core/csc_matrix.hpp:30-96
 //   ref_read_mps        sov::MpsReader::read          src/io/mps_reader.hpp:15-304
+//   ref_write_mps       sov::MpsReader::write         src/io/mps_reader.hpp:306-412
 //   ref_dd_probe        sov::dd_real / NeumaierSum    src/core/dd_real.hpp:27-104
 
 #include "include/sov/solver.hpp"
@@ -25,6 +26,7 @@
 namespace {
 
 thread_local std::string g_err;
+thread_local int g_status = 0;
 
 sov::Model to_model(const nir_lp_view* v) {
     sov::Model m;
@@ -171,14 +173,55 @@ void ref_dd_probe(double a, double b, double c, double* dd_out, double* neumaier
 ref_model* ref_read_mps(const char* path) {
     auto h = std::make_unique<ref_model>();
     std::string err;
-    sov::Status st = sov::MpsReader::read(path, h->m, err);
-    if (st != sov::Status::Optimal) {
-        g_err = err;
+    sov::Status st;
+    try {
+        st = sov::MpsReader::read(path, h->m, err);
+    } catch (const std::exception& e) {
+        // the reader lets std::stod's exceptions escape
+        g_err = std::string("exception: ") + e.what();
+        g_status = -1;
         return nullptr;
     }
+    if (st != sov::Status::Optimal) {
+        g_err = err;
+        g_status = static_cast<int>(st);
+        return nullptr;
+    }
+    g_status = 0;
     h->sense = (h->m.sense == sov::Sense::Maximize) ? -1 : 1;
     h->m = h->m.to_internal_min();
     return h.release();
+}
+
+int ref_last_status(void) { return g_status; }
+
+int ref_model_vartypes(const ref_model* h, int8_t* out) {
+    if (!h) return 1;
+    for (sov::Idx j = 0; j < h->m.ncol; ++j) out[j] = static_cast<int8_t>(h->m.vartype[j]);
+    return 0;
+}
+
+int64_t ref_model_qnnz(const ref_model* h) { return h ? h->m.Q.nnz() : 0; }
+
+int ref_model_q(const ref_model* h, int64_t* start, int32_t* index, double* value) {
+    if (!h) return 1;
+    const sov::CscMatrix& Q = h->m.Q;
+    for (sov::Idx j = 0; j <= h->m.ncol; ++j) start[j] = Q.start.empty() ? 0 : Q.start[j];
+    for (sov::Off k = 0; k < Q.nnz(); ++k) {
+        index[k] = Q.index[k];
+        value[k] = Q.value[k];
+    }
+    return 0;
+}
+
+// MPS writer over an LP view with variable types and a sense (+1 / -1).
+int ref_write_mps(const nir_lp_view* v, const int8_t* vartype, int sense, const char* path) {
+    sov::Model m = to_model(v);
+    m.name = "written";
+    m.sense = sense < 0 ? sov::Sense::Maximize : sov::Sense::Minimize;
+    if (vartype)
+        for (sov::Idx j = 0; j < v->ncol; ++j) m.vartype[j] = static_cast<sov::VarType>(vartype[j]);
+    return sov::MpsReader::write(path, m) ? 0 : 1;
 }
 
 int ref_model_view(const ref_model* h, nir_lp_view* v, int* sense) {

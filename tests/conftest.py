@@ -20,6 +20,7 @@ def _native_libs():
     from nirnaya_b200 import build
 
     build.build_lpgen()
+    build.build_mps()
     import subprocess
 
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "oracle"], check=True)
