@@ -538,6 +538,63 @@ def mlp_perf(args):
     print(json.dumps(out))
 
 
+def mps_read_bench(args):
+    """Reads the workload's LP from an MPS file: libnir_mps.so with all host
+    threads (W warm-up reads, K timed reads) and with one thread, against
+    the reference's MpsReader::read (oracle/_ref, one read) on the same
+    file, with a bit-for-bit comparison of the models.  The file is written
+    once by nir_mps_write (the reference writer's bytes) under --mps-dir.
+    One JSON line; wall-clock timing (host-only work)."""
+    import numpy as np
+
+    from nirnaya_b200 import lp as L
+    from nirnaya_b200 import mps
+    from oracle import ffi
+
+    wl = WORKLOADS[args.workload]
+    os.makedirs(args.mps_dir, exist_ok=True)
+    path = os.path.join(args.mps_dir, wl["label"] + ".mps")
+    lp = L.generate(wl["kind"], wl["seed"], **wl["kw"])
+    t0 = time.perf_counter()
+    mps.write_mps(path, lp, name=wl["label"])
+    t_write = time.perf_counter() - t0
+    size = os.path.getsize(path)
+    nproc = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        mps.read_mps(path)
+    times, phases = [], None
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        m = mps.read_mps(path)
+        times.append(time.perf_counter() - t0)
+        phases = m.timings
+    t = float(np.median(times))
+    t0 = time.perf_counter()
+    mps.read_mps(path, threads=1)
+    t1 = time.perf_counter() - t0
+    ref = None
+    if ffi.ref_available():
+        t0 = time.perf_counter()
+        rl, rs, rvt, _ = ffi.ref_read_mps_full(path)
+        tr = time.perf_counter() - t0
+        ours, _ = m.internal_min()
+        same = rs == m.sense and np.array_equal(rvt, m.vartype) and all(
+            np.array_equal(getattr(ours, k).view(np.uint8), getattr(rl, k).view(np.uint8))
+            for k in ("col_start", "row_index", "value", "cost", "collo", "colup", "rowlo", "rowup"))
+        ref = {"seconds": tr, "MB_per_s": size / tr / 1e6, "cores": 1, "kind": "reference",
+               "sample": "sov::MpsReader::read + Model::validate (+ to_internal_min) of the whole file, once",
+               "models_bit_identical": bool(same)}
+    line = {"metric": "mps_read_throughput", "value": size / t / 1e6, "unit": "MB/s", "higher_is_better": True,
+            "steps": args.steps, "warmup": args.warmup, "seconds": t,
+            "data": "synthetic (seeded generator, include/nir_lpgen.h), written as MPS",
+            "config": {"workload": wl["label"] + ".mps", "bytes": size, "rows": lp.nrow, "cols": lp.ncol,
+                       "nnz": lp.nnz, "threads": nproc},
+            "phases_s": phases, "single_thread": {"seconds": t1, "MB_per_s": size / t1 / 1e6},
+            "writer_seconds": t_write, "reference": ref,
+            "speedup_vs_reference": (ref["seconds"] / t) if ref else None}
+    print(json.dumps(line))
+
+
 def reference_iterations(args):
     """Counts the reference PDHG's iterations to 1e-6 relative KKT on the
     workload: the bit-identical GPU restatement of its loop
@@ -589,8 +646,15 @@ def main():
     ap.add_argument("--ncu-cap", type=int, default=0,
                     help="warp row-block capacity of the ncu case (0: autotuned; the tuner times launches, "
                          "which a profiler that serialises every launch perturbs)")
+    ap.add_argument("--mps-read", action="store_true",
+                    help="MPS reader throughput on the workload written as an MPS file, then exit")
+    ap.add_argument("--mps-dir", default=os.path.join(ROOT, "_bench_tmp"),
+                    help="where --mps-read writes its input file")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
+    if args.mps_read:
+        mps_read_bench(args)
+        return
     if args.ref_iterations > 0:
         reference_iterations(args)
         return

@@ -18,7 +18,10 @@
  * The COLUMNS section is tokenised and converted by `threads` threads in
  * parallel and replayed in file order; the CSC is built in parallel.
  * Status codes are sov::Status (src/core/status.hpp:7-24): 0 valid,
- * 1 infeasible bounds (as Model::validate), 12 input error.
+ * 1 infeasible bounds (as Model::validate), 12 input error, 14 internal
+ * (allocation) error.  Where the reference lets std::stod's exception
+ * escape (a token that is not a number, or out of double range), this
+ * reader returns 12 and names the token and its line.
  */
 #ifndef NIR_MPS_H
 #define NIR_MPS_H
@@ -46,6 +49,13 @@ int nir_mps_view(const nir_mps* m, nir_lp_view* view, int32_t* sense);
  * (sov::VarType). */
 const int8_t* nir_mps_vartypes(const nir_mps* m);
 
+/* The NAME line's model name ("mps_model" when there is none). */
+const char* nir_mps_model_name(const nir_mps* m);
+
+/* Column (of_rows = 0) or row (of_rows = 1) names, packed: name i is the
+ * bytes [offsets[i], offsets[i+1]) of chars (not NUL-terminated). */
+int nir_mps_names(const nir_mps* m, int32_t of_rows, const char** chars, const int64_t** offsets);
+
 /* The quadratic objective block (QUADOBJ / QMATRIX) as an ncol x ncol CSC
  * (upper triangle as the reference stores it); *nnz = 0 for an LP. */
 int nir_mps_quadratic(const nir_mps* m, int64_t* nnz, const int64_t** col_start, const int32_t** row_index,
@@ -57,6 +67,19 @@ int nir_mps_quadratic(const nir_mps* m, int64_t* nnz, const int64_t** col_start,
 int nir_mps_timings(double* out6);
 
 void nir_mps_free(nir_mps* m);
+
+/* Writes an MPS file byte for byte as sov::MpsReader::write
+ * (src/io/mps_reader.hpp:306-412) writes the same model: `sense` 1 / -1,
+ * `vartype` (ncol bytes, may be NULL: all continuous), names NUL-terminated
+ * (NULL: the reference's generated C<j> / R<i>), the quadratic block as an
+ * upper-triangle CSC (qnnz = 0: none).  Formatting runs on `threads`
+ * threads (<= 0: all).  Returns 0, 12 on a bad argument, 14 when the file
+ * cannot be written. */
+int nir_mps_write(const nir_lp_view* lp, const int8_t* vartype, int32_t sense, const char* model_name,
+                  const char* const* col_names, const char* const* row_names, int64_t qnnz, const int64_t* q_start,
+                  const int32_t* q_index, const double* q_value, int32_t threads, const char* path);
+
+/* The message of the last failed call on this thread. */
 const char* nir_mps_last_error(void);
 
 #ifdef __cplusplus

@@ -22,6 +22,7 @@
 //     sorted by row (stably) and merged, in parallel over columns.
 // Numbers: the exact fast conversion of decimal.hpp, with strtod (as
 // std::stod calls it) wherever that conversion declines.
+#include <emmintrin.h>
 #include <fcntl.h>
 #include <sys/stat.h>
 #include <unistd.h>
@@ -72,15 +73,40 @@ struct Tok {
     uint32_t n;
 };
 
+// Bit i set when p[i] is white space (' ' or 0x09-0x0D), 16 bytes at once.
+// Reads p[0..15]: the file buffer is padded so that this stays inside it.
+inline uint32_t space_mask16(const char* p) {
+    const __m128i v = _mm_loadu_si128(reinterpret_cast<const __m128i*>(p));
+    const __m128i sp = _mm_cmpeq_epi8(v, _mm_set1_epi8(' '));
+    const __m128i t = _mm_sub_epi8(v, _mm_set1_epi8(0x09));
+    const __m128i ctl = _mm_cmpeq_epi8(_mm_min_epu8(t, _mm_set1_epi8(4)), t);  // 0x09 <= c <= 0x0D
+    return uint32_t(_mm_movemask_epi8(_mm_or_si128(sp, ctl)));
+}
+
+// The tokens of [b, e), split on white space as istream >> splits them.
 inline void tokenize(const char* b, const char* e, std::vector<Tok>& out) {
     out.clear();
-    while (b < e) {
-        while (b < e && is_space(*b)) ++b;
-        if (b == e) break;
-        const char* s = b;
-        while (b < e && !is_space(*b)) ++b;
-        out.push_back({s, uint32_t(b - s)});
+    const char* tok = nullptr;  // start of a token still open
+    for (const char* p = b; p < e; p += 16) {
+        uint32_t sp = space_mask16(p);
+        const size_t lim = size_t(e - p);
+        if (lim < 16) sp |= (0xFFFFu << lim) & 0xFFFFu;  // bytes past the end count as space
+        uint32_t pos = 0;
+        for (;;) {
+            if (!tok) {
+                const uint32_t ns = ~sp & (0xFFFFu << pos) & 0xFFFFu;
+                if (!ns) break;
+                pos = uint32_t(__builtin_ctz(ns));
+                tok = p + pos;
+            }
+            const uint32_t s = sp & (0xFFFFu << pos);
+            if (!s) break;  // the token goes on in the next block
+            pos = uint32_t(__builtin_ctz(s));
+            out.push_back({tok, uint32_t(p + pos - tok)});
+            tok = nullptr;
+        }
     }
+    if (tok) out.push_back({tok, uint32_t(e - tok)});
 }
 
 std::string upper(const Tok& t) {
@@ -213,10 +239,11 @@ struct NameMap {
     void reserve(size_t n) {
         size_t want = slots.size();
         while (want < 2 * n + 2) want *= 2;
-        while (slots.size() < want) grow();
+        if (want > slots.size()) rehash(want);
     }
-    void grow() {
-        std::vector<Slot> old(slots.size() * 2);
+    void grow() { rehash(slots.size() * 2); }
+    void rehash(size_t size) {
+        std::vector<Slot> old(size);
         old.swap(slots);
         const size_t mask = slots.size() - 1;
         for (const Slot& s : old) {
@@ -271,6 +298,9 @@ struct nir_mps {
     std::vector<int64_t> qstart{0};
     std::vector<int32_t> qindex;
     std::vector<double> qvalue;
+    std::string name = "mps_model";
+    std::vector<char> col_chars, row_chars;  // names, packed
+    std::vector<int64_t> col_off{0}, row_off{0};
 };
 
 namespace {
@@ -282,24 +312,49 @@ namespace {
 void from_triplets(int32_t nrow, int32_t ncol, const Triplets& t, std::vector<int64_t>& start,
                    std::vector<int32_t>& index, std::vector<double>& value, int threads) {
     const size_t T = t.size();
-    std::vector<int64_t> cnt(size_t(ncol) + 1, 0);
     auto keep = [&](size_t k) {
         return t.row[k] >= 0 && t.row[k] < nrow && t.col[k] >= 0 && t.col[k] < ncol && t.val[k] != 0.0;
     };
-    for (size_t k = 0; k < T; ++k)
-        if (keep(k)) ++cnt[size_t(t.col[k]) + 1];
-    for (int32_t j = 0; j < ncol; ++j) cnt[j + 1] += cnt[j];
+    // stable counting sort by column: thread k counts its slice of the
+    // triplets per column, then writes them after the slices before it
+    const int ns = int(std::max<size_t>(1, std::min<size_t>(size_t(threads), T / 65536 + 1)));
+    std::vector<std::vector<int64_t>> pos(static_cast<size_t>(ns));
+    run_threads(ns, [&](int k) {
+        std::vector<int64_t>& c = pos[size_t(k)];
+        c.assign(size_t(ncol), 0);
+        for (size_t q = T * size_t(k) / size_t(ns); q < T * size_t(k + 1) / size_t(ns); ++q)
+            if (keep(q)) ++c[size_t(t.col[q])];
+    });
+    std::vector<int64_t> cnt(size_t(ncol) + 1, 0);
+    for (int32_t j = 0; j < ncol; ++j) {
+        int64_t s = 0;
+        for (int k = 0; k < ns; ++k) s += pos[size_t(k)][size_t(j)];
+        cnt[size_t(j) + 1] = cnt[size_t(j)] + s;
+    }
+    {
+        const int nc = std::max(1, std::min(threads, int(ncol / 4096) + 1));
+        run_threads(nc, [&](int q) {
+            for (int32_t j = int32_t(int64_t(ncol) * q / nc); j < int32_t(int64_t(ncol) * (q + 1) / nc); ++j) {
+                int64_t off = cnt[size_t(j)];
+                for (int k = 0; k < ns; ++k) {
+                    const int64_t c = pos[size_t(k)][size_t(j)];
+                    pos[size_t(k)][size_t(j)] = off;
+                    off += c;
+                }
+            }
+        });
+    }
     std::vector<int32_t> ri(size_t(cnt[ncol]));
     std::vector<double> rv(size_t(cnt[ncol]));
-    {
-        std::vector<int64_t> pos(cnt.begin(), cnt.end() - 1);
-        for (size_t k = 0; k < T; ++k)
-            if (keep(k)) {
-                const int64_t p = pos[t.col[k]]++;
-                ri[p] = t.row[k];
-                rv[p] = t.val[k];
+    run_threads(ns, [&](int k) {
+        std::vector<int64_t>& w = pos[size_t(k)];
+        for (size_t q = T * size_t(k) / size_t(ns); q < T * size_t(k + 1) / size_t(ns); ++q)
+            if (keep(q)) {
+                const int64_t p = w[size_t(t.col[q])]++;
+                ri[size_t(p)] = t.row[q];
+                rv[size_t(p)] = t.val[q];
             }
-    }
+    });
     // per column: sort (stable) and merge in place; merged count per column
     std::vector<int64_t> kept(size_t(ncol), 0);
     auto work = [&](int32_t j0, int32_t j1) {
@@ -350,6 +405,14 @@ void from_triplets(int32_t nrow, int32_t ncol, const Triplets& t, std::vector<in
         jb[k] = std::max(jb[k - 1], std::min(jb[k], ncol));
     }
     run_threads(nt, [&](int k) { work(jb[k], jb[k + 1]); });
+    bool merged = false;  // some column lost entries to merging
+    for (int32_t c = 0; c < ncol && !merged; ++c) merged = kept[c] != cnt[c + 1] - cnt[c];
+    if (!merged) {  // the usual case: the bucketed arrays are the CSC
+        start.swap(cnt);
+        index.swap(ri);
+        value.swap(rv);
+        return;
+    }
     start.assign(size_t(ncol) + 1, 0);
     for (int32_t c = 0; c < ncol; ++c) start[c + 1] = start[c] + kept[c];
     index.resize(size_t(start[ncol]));
@@ -414,6 +477,7 @@ struct Header {
 };
 
 struct Reader {
+    static constexpr size_t kPad = 64;
     std::unique_ptr<char[]> store;
     const char* buf = nullptr;
     size_t size = 0;  // bytes of the file; buf[size] == '\n'
@@ -500,9 +564,10 @@ struct Reader {
             throw InputError(std::string("Cannot open MPS file: ") + path);
         }
         size = size_t(st.st_size);
-        store.reset(new char[size + 1]);
+        // one '\n' after the file, then padding for the 16-byte loads
+        store.reset(new char[size + kPad]);
         char* dst = store.get();
-        dst[size] = '\n';
+        std::memset(dst + size, '\n', kPad);
         int nt = int(std::max<size_t>(1, std::min<size_t>(size_t(threads), size / (size_t(8) << 20) + 1)));
         std::vector<int> fail(size_t(nt), 0);
         run_threads(nt, [&](int k) {
@@ -590,9 +655,11 @@ struct Reader {
                 tokenize(buf + this_line, buf + le, tk);
                 if (tk.empty()) continue;
                 int marker = -1;
-                for (const Tok& t : tk) {
-                    if (contains(t, "INTORG", 6)) marker = 1;
-                    else if (contains(t, "INTEND", 6)) marker = 0;
+                if (memmem(buf + this_line, le - this_line, "INT", 3)) {
+                    for (const Tok& t : tk) {
+                        if (contains(t, "INTORG", 6)) marker = 1;
+                        else if (contains(t, "INTEND", 6)) marker = 0;
+                    }
                 }
                 if (marker >= 0) {
                     r.events.push_back(marker == 1 ? -2 : -1);
@@ -850,32 +917,65 @@ struct Reader {
         }
     }
 
-    // ---- ROWS (one thread: row numbers are the order of appearance)
+    // ---- ROWS: lines tokenised in parallel, rows numbered on one thread in
+    // order of appearance
+    struct RowRec {
+        uint64_t hash;
+        const char* p;
+        uint32_t n;
+        char type;  // upper-cased first letter of the type token
+        char key[16];
+        size_t line;
+    };
+
     void rows_section(size_t a, size_t b) {
-        std::vector<Tok> tk;
-        for (size_t lb = a; lb < b;) {
-            const size_t nl = line_end(lb);
-            const size_t le = trimmed(lb, nl);
-            const size_t this_line = lb;
-            lb = nl + 1;
-            if (skipped(this_line, le)) continue;
-            tokenize(buf + this_line, buf + le, tk);
-            if (tk.size() < 2) continue;
-            const char rt = char(std::toupper((unsigned char)tk[0].p[0]));
-            const Tok& rn = tk[1];
-            if (rt == 'N') {
-                if (obj_row.empty()) obj_row.assign(rn.p, rn.n);
-                continue;  // further free rows are dropped
+        int nt;
+        const std::vector<size_t> at = cut(a, b, nt);
+        std::vector<std::vector<RowRec>> run(static_cast<size_t>(nt));
+        run_threads(nt, [&](int k) {
+            std::vector<Tok> tk;
+            std::vector<RowRec>& r = run[size_t(k)];
+            r.reserve((at[k + 1] - at[k]) / 16 + 16);
+            for (size_t lb = at[k]; lb < at[k + 1];) {
+                const size_t nl = line_end(lb);
+                const size_t le = trimmed(lb, nl);
+                const size_t this_line = lb;
+                lb = nl + 1;
+                if (skipped(this_line, le)) continue;
+                tokenize(buf + this_line, buf + le, tk);
+                if (tk.size() < 2) continue;
+                RowRec q;
+                q.hash = hash_name(tk[1].p, tk[1].n);
+                q.p = tk[1].p;
+                q.n = tk[1].n;
+                q.type = char(std::toupper((unsigned char)tk[0].p[0]));
+                std::memcpy(q.key, tk[1].p, std::min<size_t>(tk[1].n, 16));
+                q.line = this_line;
+                r.push_back(q);
             }
-            const int32_t r = m->nrow;
-            if (rows.insert(rn.p, rn.n, r) >= 0)
-                throw InputError("Duplicate row name at line " + std::to_string(line_number(this_line)));
-            m->nrow++;
-            row_name.push_back(rn);
-            row_type.push_back(rt == 'L' ? kRowL : (rt == 'G' ? kRowG : kRowE));
-            rhs.push_back(0.0);
-            range.push_back(0.0);
-            has_range.push_back(0);
+        });
+        size_t total = 0;
+        for (const auto& r : run) total += r.size();
+        rows.reserve(rows.count + total);
+        row_name.reserve(row_name.size() + total);
+        for (const auto& r : run) {
+            for (size_t i = 0; i < r.size(); ++i) {
+                if (i + 8 < r.size()) __builtin_prefetch(rows.slot_for(r[i + 8].hash));
+                const RowRec& q = r[i];
+                if (q.type == 'N') {
+                    if (obj_row.empty()) obj_row.assign(q.p, q.n);
+                    continue;  // further free rows are dropped
+                }
+                const int32_t idx = m->nrow;
+                if (rows.insert_h(q.hash, q.n <= 16 ? q.key : q.p, q.p, q.n, idx) >= 0)
+                    throw InputError("Duplicate row name at line " + std::to_string(line_number(q.line)));
+                m->nrow++;
+                row_name.push_back({q.p, q.n});
+                row_type.push_back(q.type == 'L' ? kRowL : (q.type == 'G' ? kRowG : kRowE));
+                rhs.push_back(0.0);
+                range.push_back(0.0);
+                has_range.push_back(0);
+            }
         }
     }
 
@@ -938,6 +1038,7 @@ struct Reader {
             const Sec kind = Sec(hdr[h].kind);
             if (kind == END) break;
             if (kind == NAME) {
+                if (tk.size() >= 2) m->name.assign(tk[1].p, tk[1].n);
                 sec = NAME;
             } else if (kind == OBJSENSE) {
                 if (tk.size() >= 2) {
@@ -984,10 +1085,25 @@ struct Reader {
         t_csc = now() - t0;
         assemble_rows();
         validate();
+        pack_names(col_name, m->col_chars, m->col_off);
+        pack_names(row_name, m->row_chars, m->row_off);
         g_times[2] = t_parse;
         g_times[3] = t_apply;
         g_times[4] = t_csc;
         g_times[5] = (now() - t_all) - t_parse - t_apply - t_csc;
+    }
+
+    // names as one character array with offsets (n + 1), copied in parallel
+    void pack_names(const std::vector<Tok>& nm, std::vector<char>& chars, std::vector<int64_t>& off) const {
+        const size_t n = nm.size();
+        off.assign(n + 1, 0);
+        for (size_t i = 0; i < n; ++i) off[i + 1] = off[i] + nm[i].n;
+        chars.resize(size_t(off[n]));
+        const int nt = int(std::max<size_t>(1, std::min<size_t>(size_t(threads), n / 65536 + 1)));
+        run_threads(nt, [&](int k) {
+            for (size_t i = n * size_t(k) / size_t(nt); i < n * size_t(k + 1) / size_t(nt); ++i)
+                std::memcpy(chars.data() + off[i], nm[i].p, nm[i].n);
+        });
     }
 
     void assemble_rows() {
@@ -1073,6 +1189,10 @@ struct Reader {
 
 }  // namespace
 
+namespace nir {
+__attribute__((visibility("hidden"))) void set_mps_error(const std::string& msg) { g_err = msg; }
+}  // namespace nir
+
 extern "C" {
 
 int nir_mps_read(const char* path, int32_t threads, nir_mps** out) {
@@ -1121,6 +1241,15 @@ int nir_mps_view(const nir_mps* m, nir_lp_view* v, int32_t* sense) {
 }
 
 const int8_t* nir_mps_vartypes(const nir_mps* m) { return m ? m->vartype.data() : nullptr; }
+
+const char* nir_mps_model_name(const nir_mps* m) { return m ? m->name.c_str() : nullptr; }
+
+int nir_mps_names(const nir_mps* m, int32_t of_rows, const char** chars, const int64_t** offsets) {
+    if (!m) return 12;
+    if (chars) *chars = of_rows ? m->row_chars.data() : m->col_chars.data();
+    if (offsets) *offsets = of_rows ? m->row_off.data() : m->col_off.data();
+    return 0;
+}
 
 int nir_mps_quadratic(const nir_mps* m, int64_t* nnz, const int64_t** col_start, const int32_t** row_index,
                       const double** value) {

@@ -20,8 +20,8 @@ from .lp import LP, NirLpView
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
 
-EXPORTED = ["nir_mps_read", "nir_mps_view", "nir_mps_vartypes", "nir_mps_quadratic", "nir_mps_timings",
-            "nir_mps_free", "nir_mps_last_error"]
+EXPORTED = ["nir_mps_read", "nir_mps_view", "nir_mps_vartypes", "nir_mps_model_name", "nir_mps_names",
+            "nir_mps_quadratic", "nir_mps_timings", "nir_mps_free", "nir_mps_write", "nir_mps_last_error"]
 
 CONTINUOUS, INTEGER, BINARY = 0, 1, 2
 TIMING_PHASES = ("file_read", "line_scan", "columns_parse", "columns_replay", "csc_build", "other")
@@ -47,6 +47,16 @@ def lib() -> C.CDLL:
         L.nir_mps_view.argtypes = [C.c_void_p, C.POINTER(NirLpView), C.POINTER(C.c_int32)]
         L.nir_mps_vartypes.restype = C.POINTER(C.c_int8)
         L.nir_mps_vartypes.argtypes = [C.c_void_p]
+        L.nir_mps_model_name.restype = C.c_char_p
+        L.nir_mps_model_name.argtypes = [C.c_void_p]
+        L.nir_mps_names.restype = C.c_int
+        L.nir_mps_names.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.POINTER(C.c_char)),
+                                    C.POINTER(C.POINTER(C.c_int64))]
+        L.nir_mps_write.restype = C.c_int
+        L.nir_mps_write.argtypes = [C.POINTER(NirLpView), C.POINTER(C.c_int8), C.c_int32, C.c_char_p,
+                                    C.POINTER(C.c_char_p), C.POINTER(C.c_char_p), C.c_int64,
+                                    C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_double), C.c_int32,
+                                    C.c_char_p]
         L.nir_mps_quadratic.restype = C.c_int
         L.nir_mps_quadratic.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.POINTER(C.c_int64)),
                                         C.POINTER(C.POINTER(C.c_int32)), C.POINTER(C.POINTER(C.c_double))]
@@ -69,6 +79,9 @@ class MpsModel:
     q_index: np.ndarray         # int32[qnnz]
     q_value: np.ndarray         # float64[qnnz]
     timings: dict
+    name: str = "mps_model"
+    col_names: list | None = None
+    row_names: list | None = None
 
     def internal_min(self) -> tuple[LP, np.ndarray]:
         """Model::to_internal_min: for MAX, cost, offset and Q negated.
@@ -81,31 +94,97 @@ class MpsModel:
         return out, -self.q_value
 
 
-def _copy(p, n, dt):
-    return np.ctypeslib.as_array(p, shape=(n,)).astype(dt, copy=True) if n else np.zeros(0, dt)
+class _Handle:
+    """Owns one nir_mps model; freed when the last array viewing it goes."""
+
+    def __init__(self, h):
+        self.h = h
+
+    def __del__(self):
+        if self.h:
+            lib().nir_mps_free(self.h)
+            self.h = None
 
 
-def read_mps(path: str, threads: int = 0) -> MpsModel:
+class _View:
+    """An array interface over memory the handle owns, keeping it alive."""
+
+    def __init__(self, ptr, n, dt, owner):
+        self.__array_interface__ = {"data": (C.cast(ptr, C.c_void_p).value or 0, True), "shape": (n,),
+                                    "typestr": np.dtype(dt).str, "version": 3}
+        self.owner = owner
+
+
+def _view(p, n, dt, owner):
+    if not n:
+        return np.zeros(0, dt)
+    return np.asarray(_View(p, n, dt, owner))
+
+
+def _names(L, h, of_rows: int, n: int) -> list:
+    chars, off = C.POINTER(C.c_char)(), C.POINTER(C.c_int64)()
+    L.nir_mps_names(h, of_rows, C.byref(chars), C.byref(off))
+    o = np.ctypeslib.as_array(off, shape=(n + 1,)).copy()
+    blob = C.string_at(chars, int(o[-1])) if o[-1] else b""
+    return [blob[o[i]:o[i + 1]].decode(errors="surrogateescape") for i in range(n)]
+
+
+def read_mps(path: str, threads: int = 0, names: bool = False) -> MpsModel:
+    """Reads an MPS file (threads <= 0: all hardware threads); names=True
+    also returns the column and row names."""
     L = lib()
     h = C.c_void_p()
     st = L.nir_mps_read(os.fsencode(path), int(threads), C.byref(h))
     if st != 0:
         raise MpsError(st, L.nir_mps_last_error().decode(errors="replace"))
-    try:
-        v = NirLpView()
-        sense = C.c_int32()
-        L.nir_mps_view(h, C.byref(v), C.byref(sense))
-        lp = LP(v.nrow, v.ncol, _copy(v.col_start, v.ncol + 1, np.int64), _copy(v.row_index, v.nnz, np.int32),
-                _copy(v.value, v.nnz, np.float64), _copy(v.cost, v.ncol, np.float64),
-                _copy(v.collo, v.ncol, np.float64), _copy(v.colup, v.ncol, np.float64),
-                _copy(v.rowlo, v.nrow, np.float64), _copy(v.rowup, v.nrow, np.float64), v.obj_offset)
-        vt = _copy(L.nir_mps_vartypes(h), v.ncol, np.int8)
-        qn = C.c_int64()
-        qs, qi, qv = C.POINTER(C.c_int64)(), C.POINTER(C.c_int32)(), C.POINTER(C.c_double)()
-        L.nir_mps_quadratic(h, C.byref(qn), C.byref(qs), C.byref(qi), C.byref(qv))
-        t = (C.c_double * 6)()
-        L.nir_mps_timings(t)
-        return MpsModel(lp, int(sense.value), vt, _copy(qs, v.ncol + 1, np.int64), _copy(qi, qn.value, np.int32),
-                        _copy(qv, qn.value, np.float64), dict(zip(TIMING_PHASES, list(t))))
-    finally:
-        L.nir_mps_free(h)
+    owner = _Handle(h.value)
+    v = NirLpView()
+    sense = C.c_int32()
+    L.nir_mps_view(h, C.byref(v), C.byref(sense))
+    # the arrays are read-only views of the native model (no copy)
+    lp = LP(v.nrow, v.ncol, _view(v.col_start, v.ncol + 1, np.int64, owner),
+            _view(v.row_index, v.nnz, np.int32, owner), _view(v.value, v.nnz, np.float64, owner),
+            _view(v.cost, v.ncol, np.float64, owner), _view(v.collo, v.ncol, np.float64, owner),
+            _view(v.colup, v.ncol, np.float64, owner), _view(v.rowlo, v.nrow, np.float64, owner),
+            _view(v.rowup, v.nrow, np.float64, owner), v.obj_offset)
+    vt = _view(L.nir_mps_vartypes(h), v.ncol, np.int8, owner)
+    qn = C.c_int64()
+    qs, qi, qv = C.POINTER(C.c_int64)(), C.POINTER(C.c_int32)(), C.POINTER(C.c_double)()
+    L.nir_mps_quadratic(h, C.byref(qn), C.byref(qs), C.byref(qi), C.byref(qv))
+    t = (C.c_double * 6)()
+    L.nir_mps_timings(t)
+    model = MpsModel(lp, int(sense.value), vt, _view(qs, v.ncol + 1, np.int64, owner),
+                     _view(qi, qn.value, np.int32, owner), _view(qv, qn.value, np.float64, owner),
+                     dict(zip(TIMING_PHASES, list(t))), L.nir_mps_model_name(h).decode(errors="replace"))
+    if names:
+        model.col_names = _names(L, h, 0, v.ncol)
+        model.row_names = _names(L, h, 1, v.nrow)
+    return model
+
+
+def write_mps(path: str, lp: LP, vartype=None, sense: int = 1, name: str = "", col_names=None, row_names=None,
+              q=None, threads: int = 0) -> None:
+    """MpsReader::write's bytes for the LP (file-sense cost and offset);
+    q = (q_start, q_index, q_value) adds the QUADOBJ block."""
+    L = lib()
+    vt = None if vartype is None else np.ascontiguousarray(vartype, np.int8)
+
+    def cnames(ns):
+        if ns is None:
+            return None
+        arr = (C.c_char_p * len(ns))()
+        arr[:] = [s.encode() for s in ns]
+        return arr
+
+    cn, rn = cnames(col_names), cnames(row_names)
+    if q is not None:
+        qs, qi, qv = (np.ascontiguousarray(q[0], np.int64), np.ascontiguousarray(q[1], np.int32),
+                      np.ascontiguousarray(q[2], np.float64))
+        qargs = (int(qs[-1]), qs.ctypes.data_as(C.POINTER(C.c_int64)), qi.ctypes.data_as(C.POINTER(C.c_int32)),
+                 qv.ctypes.data_as(C.POINTER(C.c_double)))
+    else:
+        qargs = (0, None, None, None)
+    st = L.nir_mps_write(C.byref(lp.view()), None if vt is None else vt.ctypes.data_as(C.POINTER(C.c_int8)),
+                         int(sense), name.encode(), cn, rn, *qargs, int(threads), os.fsencode(path))
+    if st != 0:
+        raise MpsError(st, L.nir_mps_last_error().decode(errors="replace"))

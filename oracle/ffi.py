@@ -107,6 +107,7 @@ def ref_lib():
         lib.ref_model_qnnz.argtypes = [C.c_void_p]
         lib.ref_model_q.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int32), _D]
         lib.ref_write_mps.argtypes = [_VP, C.POINTER(C.c_int8), C.c_int, C.c_char_p]
+        lib.ref_mps_roundtrip.argtypes = [C.c_char_p, C.c_char_p]
         _ref = lib
     return _ref
 
@@ -289,3 +290,8 @@ def ref_write_mps(lp: LP, path: str, vartype=None, sense: int = 1) -> None:
                                  path.encode())
     if rc != 0:
         raise RuntimeError(f"MpsReader::write failed on {path}")
+
+
+def ref_mps_roundtrip(src: str, dst: str) -> int:
+    """MpsReader::read of src, then MpsReader::write of that model to dst."""
+    return ref_lib().ref_mps_roundtrip(src.encode(), dst.encode())

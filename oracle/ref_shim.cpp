@@ -13,6 +13,7 @@
 //   ref_from_triplets   sov::CscMatrix::from_triplets src/core/csc_matrix.hpp:30-96
 //   ref_read_mps        sov::MpsReader::read          src/io/mps_reader.hpp:15-304
 //   ref_write_mps       sov::MpsReader::write         src/io/mps_reader.hpp:306-412
+//   ref_mps_roundtrip   MpsReader::read then ::write  (names and all kept)
 //   ref_dd_probe        sov::dd_real / NeumaierSum    src/core/dd_real.hpp:27-104
 
 #include "include/sov/solver.hpp"
@@ -194,6 +195,24 @@ ref_model* ref_read_mps(const char* path) {
 }
 
 int ref_last_status(void) { return g_status; }
+
+// Reads `in` with the reference reader and writes the model back with the
+// reference writer; 0 on success, else the read status (-1: exception).
+int ref_mps_roundtrip(const char* in, const char* out) {
+    sov::Model m;
+    std::string err;
+    try {
+        const sov::Status st = sov::MpsReader::read(in, m, err);
+        if (st != sov::Status::Optimal) {
+            g_err = err;
+            return static_cast<int>(st);
+        }
+    } catch (const std::exception& e) {
+        g_err = std::string("exception: ") + e.what();
+        return -1;
+    }
+    return sov::MpsReader::write(out, m) ? 0 : 14;
+}
 
 int ref_model_vartypes(const ref_model* h, int8_t* out) {
     if (!h) return 1;

@@ -146,3 +146,90 @@ def test_cli_method_pdhg_on_crude_blending(tmp_path, args):
     obj = float(re.search(r"Objective:\s+([-0-9.eE+]+)", r.stdout).group(1))
     assert abs(obj - g["sol_objective"]) / g["sol_objective"] <= 1e-6
     assert "PASS=YES" in r.stdout
+
+
+# ---- the MPS reader drop-in (nirnaya_b200/sov/mps_reader.hpp): CPU only
+
+REF_DIR = os.environ.get("NIRNAYA_REF", "/root/reference")
+REFINERY = os.path.join(REF_DIR, "data", "refinery")
+REF_CHECKER = os.path.join(ROOT, "oracle", "_ref", "checker")
+
+
+def _refinery(ext):
+    if not os.path.isdir(REFINERY):
+        return []
+    return sorted(f[:-len(ext)] for f in os.listdir(REFINERY) if f.endswith(ext))
+
+
+def test_dropin_links_the_mps_reader():
+    for exe in ("sovsolve", "libsov.so", "checker"):
+        out = subprocess.run(["readelf", "-d", _need(exe)], capture_output=True, text=True).stdout
+        assert "libnir_mps.so" in out, exe
+
+
+@pytest.mark.parametrize("model", [m for m in _refinery(".sol") if m in _refinery(".mps")])
+def test_dropin_checker_matches_the_reference_checker(model):
+    """tools/checker.cpp built twice: on the drop-in reader and as it is."""
+    if not os.path.exists(REF_CHECKER):
+        pytest.skip("the reference checker (oracle/_ref/checker) is absent")
+    args = [os.path.join(REFINERY, model + ".mps"), os.path.join(REFINERY, model + ".sol")]
+    ours = subprocess.run([_need("checker"), *args], capture_output=True, text=True, timeout=120)
+    ref = subprocess.run([REF_CHECKER, *args], capture_output=True, text=True, timeout=120)
+    assert (ours.returncode, ours.stdout) == (ref.returncode, ref.stdout)
+
+
+def _c_api_roundtrip(lib, src, dst):
+    lib.sov_read_mps.argtypes = [C.c_void_p, C.c_char_p]
+    env = lib.sov_env_create()
+    m = lib.sov_model_create(env, b"rt")
+    try:
+        assert lib.sov_read_mps(m, src.encode()) == 0, lib.sov_error_message(m)
+        assert lib.sov_write_mps(m, dst.encode()) == 0
+    finally:
+        lib.sov_model_free(m)
+        lib.sov_env_free(env)
+
+
+def _roundtrip_cases(tmp_path):
+    from mps_cases import CASES, random_mps
+
+    from nirnaya_b200 import lp as L
+
+    paths = [os.path.join(REFINERY, f + ".mps") for f in _refinery(".mps")]
+    for name in ("basic", "ranges", "integers", "objname", "bound_rules", "quadobj", "layout"):
+        p = tmp_path / (name + ".mps")
+        with open(p, "w", newline="") as f:
+            f.write(CASES[name])
+        paths.append(str(p))
+    p = tmp_path / "random.mps"
+    with open(p, "w", newline="") as f:
+        f.write(random_mps(L.generate(L.ZIPF, 3, m=3000, n=8000, target_nnz=60000), 3, sense=-1))
+    paths.append(str(p))
+    return paths
+
+
+def test_dropin_c_api_read_then_write_is_the_reference_bytes(tmp_path):
+    """sov_read_mps + sov_write_mps (src/driver/c_api.cpp:101-120) on the
+    drop-in against MpsReader::read + MpsReader::write of the reference:
+    the files written must be identical, names and all."""
+    from oracle import ffi
+
+    if not ffi.ref_available():
+        pytest.skip("the reference build (oracle/_ref) is absent")
+    lib = _sov(_need("libsov.so"))
+    for src in _roundtrip_cases(tmp_path):
+        ours, ref = str(tmp_path / "ours.mps"), str(tmp_path / "ref.mps")
+        _c_api_roundtrip(lib, src, ours)
+        assert ffi.ref_mps_roundtrip(src, ref) == 0, src
+        with open(ours, "rb") as a, open(ref, "rb") as b:
+            assert a.read() == b.read(), src
+
+
+def test_dropin_cli_reports_a_bad_number_as_an_input_error(tmp_path):
+    # the reference's reader throws from std::stod here; the drop-in returns
+    # InputError, which the CLI reports (src/driver/cli_main.cpp:89-93)
+    p = tmp_path / "bad.mps"
+    p.write_text("NAME B\nROWS\n N o\n L r\nCOLUMNS\n x o 1 r 1\n y o abc r 1\nENDATA\n")
+    r = subprocess.run([_need("sovsolve"), str(p)], capture_output=True, text=True, timeout=120)
+    assert r.returncode != 0
+    assert "Input Error reading" in r.stderr and "invalid number 'abc' at line 7" in r.stderr
