@@ -99,10 +99,11 @@ class _Handle:
 
     def __init__(self, h):
         self.h = h
+        self._free = lib().nir_mps_free  # held so that teardown order does not matter
 
     def __del__(self):
         if self.h:
-            lib().nir_mps_free(self.h)
+            self._free(self.h)
             self.h = None
 
 
