@@ -605,6 +605,69 @@ def mps_read_bench(args):
     print(json.dumps(line))
 
 
+def host_path_bench(args):
+    """The host steps Solver::solve takes before PdhgSolver::solve on the CLI
+    path (include/sov/solver.hpp:135-181): read the MPS file, presolve, scale.
+    This build's libraries (all host threads) against the reference's own
+    code (oracle/_ref, one thread, as it runs), each step once after one
+    warm-up, with a bit-for-bit comparison of the scaled model handed to
+    PDHG.  One JSON line; wall-clock timing (host-only work)."""
+    import numpy as np
+
+    from nirnaya_b200 import facade
+    from nirnaya_b200 import lp as L
+    from nirnaya_b200 import mps
+    from oracle import ffi
+
+    wl = WORKLOADS[args.workload]
+    os.makedirs(args.mps_dir, exist_ok=True)
+    path = os.path.join(args.mps_dir, wl["label"] + ".mps")
+    lp = L.generate(wl["kind"], wl["seed"], **wl["kw"])
+    mps.write_mps(path, lp, name=wl["label"])
+
+    def ours():
+        t = {}
+        t0 = time.perf_counter()
+        m = mps.read_mps(path)
+        t["read"] = time.perf_counter() - t0
+        lpm, _ = m.internal_min()
+        t0 = time.perf_counter()
+        pre = facade.presolve(lpm, m.vartype)
+        t["presolve"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        sc = facade.scale(pre.reduced, pre.vartype)
+        t["scale"] = time.perf_counter() - t0
+        return t, sc
+
+    ours()
+    t_ours, sc = ours()
+    ref = None
+    if ffi.ref_available():
+        t = {}
+        t0 = time.perf_counter()
+        rl, _, rvt, _ = ffi.ref_read_mps_full(path)
+        t["read"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        rp = ffi.ref_presolve(rl, rvt)
+        t["presolve"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        rs = ffi.ref_scale(rp["reduced"], rp["vartype"])
+        t["scale"] = time.perf_counter() - t0
+        same = (sc.active == rs["active"] and np.array_equal(sc.R, rs["R"]) and np.array_equal(sc.C, rs["C"]) and
+                all(np.array_equal(getattr(sc.lp, k).view(np.uint8), rs[k].view(np.uint8))
+                    for k in ("cost", "collo", "colup", "value", "rowlo", "rowup")))
+        ref = {"seconds": t, "total": sum(t.values()), "cores": 1, "kind": "reference",
+               "sample": "MpsReader::read, Presolver::presolve (level 2), scale_model, once each",
+               "scaled_model_bit_identical": bool(same)}
+    total = sum(t_ours.values())
+    print(json.dumps({"metric": "host_path_seconds", "value": total, "unit": "s", "higher_is_better": False,
+                      "data": "synthetic (seeded generator, include/nir_lpgen.h), written as MPS",
+                      "config": {"workload": wl["label"] + ".mps", "bytes": os.path.getsize(path),
+                                 "threads": os.cpu_count(), "reduced": [sc.lp.nrow, sc.lp.ncol, sc.lp.nnz]},
+                      "seconds": t_ours, "reference": ref,
+                      "speedup_vs_reference": (ref["total"] / total) if ref else None}))
+
+
 def reference_iterations(args):
     """Counts the reference PDHG's iterations to 1e-6 relative KKT on the
     workload: the bit-identical GPU restatement of its loop
@@ -660,8 +723,13 @@ def main():
                     help="MPS reader throughput on the workload written as an MPS file, then exit")
     ap.add_argument("--mps-dir", default=os.path.join(ROOT, "_bench_tmp"),
                     help="where --mps-read writes its input file")
+    ap.add_argument("--host-path", action="store_true",
+                    help="MPS read + presolve + scale (the CLI's host steps before PDHG) against the reference's")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
+    if args.host_path:
+        host_path_bench(args)
+        return
     if args.mps_read:
         mps_read_bench(args)
         return

@@ -4,6 +4,7 @@
   nirnaya_b200/libnir_lpgen.so  seeded instance generator (g++)
   nirnaya_b200/libnir_mlp.so    warm-start network (nvcc, sm_100a)
   nirnaya_b200/libnir_mps.so    multi-threaded MPS reader (g++, host only)
+  nirnaya_b200/libnir_facade.so presolve and scaling before the path (g++, host only)
 
 Run `python -m nirnaya_b200.build` or call build_all().
 """
@@ -93,9 +94,24 @@ def build_mps(force: bool = False, verbose: bool = False) -> str:
     return target
 
 
+def build_facade(force: bool = False, verbose: bool = False) -> str:
+    target = os.path.join(HERE, "libnir_facade.so")
+    srcs = [os.path.join(CSRC, "facade.cpp"), os.path.join(INC, "nir_facade.h"), os.path.join(INC, "nir_lp.h")]
+    if force or _stale(target, srcs):
+        cxx = os.environ.get("CXX", "g++")
+        # no FMA contraction: the reference's x86-64 build has none
+        cmd = [cxx, "-std=c++17", "-O3", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared", "-pthread",
+               "-I" + INC, srcs[0], "-o", target]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+    return target
+
+
 def build_all(force: bool = False, verbose: bool = False) -> None:
     build_lpgen(force, verbose)
     build_mps(force, verbose)
+    build_facade(force, verbose)
     build_engine(force, verbose)
     build_mlp(force, verbose)
 

@@ -108,6 +108,18 @@ def ref_lib():
         lib.ref_model_q.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int32), _D]
         lib.ref_write_mps.argtypes = [_VP, C.POINTER(C.c_int8), C.c_int, C.c_char_p]
         lib.ref_mps_roundtrip.argtypes = [C.c_char_p, C.c_char_p]
+        lib.ref_presolve.restype = C.c_void_p
+        lib.ref_presolve.argtypes = [_VP, C.POINTER(C.c_int8), C.c_int, C.c_int]
+        lib.ref_presolved_status.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                             C.POINTER(C.c_int)]
+        lib.ref_presolved_reduced.argtypes = [C.c_void_p, _VP, C.POINTER(C.c_int8)]
+        lib.ref_presolved_maps.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), _D,
+                                           C.POINTER(C.c_uint8)]
+        lib.ref_presolved_map_sizes.restype = C.c_int64
+        lib.ref_presolved_map_sizes.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
+        lib.ref_presolved_free.argtypes = [C.c_void_p]
+        lib.ref_scale.argtypes = [_VP, C.POINTER(C.c_int8), C.c_int, C.c_int64, C.POINTER(C.c_int64),
+                                  C.POINTER(C.c_int32), _D, _D, _D, C.POINTER(C.c_int)] + [_D] * 7
         _ref = lib
     return _ref
 
@@ -295,3 +307,60 @@ def ref_write_mps(lp: LP, path: str, vartype=None, sense: int = 1) -> None:
 def ref_mps_roundtrip(src: str, dst: str) -> int:
     """MpsReader::read of src, then MpsReader::write of that model to dst."""
     return ref_lib().ref_mps_roundtrip(src.encode(), dst.encode())
+
+
+def ref_presolve(lp: LP, vartype=None, level: int = 2, rounds: int = 20) -> dict:
+    """Presolver::presolve on the LP (names C<j> / R<i>): status, counters,
+    the reduced LP and vartypes, the maps, fixed_x and is_col_fixed."""
+    lib = ref_lib()
+    vt = None if vartype is None else np.ascontiguousarray(vartype, np.int8)
+    h = lib.ref_presolve(C.byref(lp.view()), None if vt is None else vt.ctypes.data_as(C.POINTER(C.c_int8)),
+                         level, rounds)
+    try:
+        st, solved, cnt = C.c_int(), C.c_int(), (C.c_int * 3)()
+        lib.ref_presolved_status(h, C.byref(st), C.byref(solved), cnt)
+        v = NirLpView()
+        lib.ref_presolved_reduced(h, C.byref(v), None)
+        rvt = np.zeros(v.ncol, np.int8)
+        lib.ref_presolved_reduced(h, C.byref(v), rvt.ctypes.data_as(C.POINTER(C.c_int8)))
+
+        def cp(p, n, dt):
+            return np.ctypeslib.as_array(p, shape=(n,)).astype(dt, copy=True) if n else np.zeros(0, dt)
+
+        red = LP(v.nrow, v.ncol, cp(v.col_start, v.ncol + 1, np.int64) if v.col_start else np.zeros(1, np.int64),
+                 cp(v.row_index, v.nnz, np.int32), cp(v.value, v.nnz, np.float64), cp(v.cost, v.ncol, np.float64),
+                 cp(v.collo, v.ncol, np.float64), cp(v.colup, v.ncol, np.float64), cp(v.rowlo, v.nrow, np.float64),
+                 cp(v.rowup, v.nrow, np.float64), v.obj_offset)
+        nc = C.c_int64()
+        nr = lib.ref_presolved_map_sizes(h, C.byref(nc))
+        cm, rm = np.zeros(nc.value, np.int32), np.zeros(nr, np.int32)
+        fx, isf = np.zeros(lp.ncol), np.zeros(lp.ncol, np.uint8)
+        lib.ref_presolved_maps(h, cm.ctypes.data_as(C.POINTER(C.c_int32)), rm.ctypes.data_as(C.POINTER(C.c_int32)),
+                               _dptr(fx), isf.ctypes.data_as(C.POINTER(C.c_uint8)))
+        return dict(status=st.value, solved_in_presolve=bool(solved.value), rows_removed=cnt[0],
+                    cols_removed=cnt[1], bound_tightenings=cnt[2], reduced=red, vartype=rvt, orig_col_map=cm,
+                    orig_row_map=rm, fixed_x=fx, is_col_fixed=isf.astype(bool))
+    finally:
+        lib.ref_presolved_free(h)
+
+
+def ref_scale(lp: LP, vartype=None, enable: bool = True, q=None) -> dict:
+    """scale_model: active, R, C and the scaled arrays."""
+    lib = ref_lib()
+    vt = None if vartype is None else np.ascontiguousarray(vartype, np.int8)
+    R, Cs = np.zeros(lp.nrow), np.zeros(lp.ncol)
+    out = {k: np.empty_like(getattr(lp, k)) for k in ("cost", "collo", "colup", "value", "rowlo", "rowup")}
+    act = C.c_int()
+    if q is not None:
+        qs, qi, qv = (np.ascontiguousarray(q[0], np.int64), np.ascontiguousarray(q[1], np.int32),
+                      np.ascontiguousarray(q[2], np.float64))
+        qo = np.empty_like(qv)
+        qargs = (int(qs[-1]), qs.ctypes.data_as(C.POINTER(C.c_int64)), qi.ctypes.data_as(C.POINTER(C.c_int32)),
+                 _dptr(qv))
+    else:
+        qo, qargs = None, (0, None, None, None)
+    lib.ref_scale(C.byref(lp.view()), None if vt is None else vt.ctypes.data_as(C.POINTER(C.c_int8)), int(enable),
+                  *qargs, _dptr(R), _dptr(Cs), C.byref(act), _dptr(out["cost"]), _dptr(out["collo"]),
+                  _dptr(out["colup"]), _dptr(out["value"]), _dptr(out["rowlo"]), _dptr(out["rowup"]),
+                  None if qo is None else _dptr(qo))
+    return dict(active=bool(act.value), R=R, C=Cs, q_value=qo, **out)

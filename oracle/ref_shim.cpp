@@ -14,6 +14,8 @@
 //   ref_read_mps        sov::MpsReader::read          src/io/mps_reader.hpp:15-304
 //   ref_write_mps       sov::MpsReader::write         src/io/mps_reader.hpp:306-412
 //   ref_mps_roundtrip   MpsReader::read then ::write  (names and all kept)
+//   ref_presolve        sov::Presolver::presolve      src/presolve/presolve.hpp:32-345
+//   ref_scale           sov::scale_model              src/model/scaling.hpp:56-154
 //   ref_dd_probe        sov::dd_real / NeumaierSum    src/core/dd_real.hpp:27-104
 
 #include "include/sov/solver.hpp"
@@ -263,5 +265,89 @@ int ref_model_view(const ref_model* h, nir_lp_view* v, int* sense) {
 }
 
 void ref_model_free(ref_model* h) { delete h; }
+
+struct ref_presolved {
+    sov::PresolveResult r;
+};
+
+ref_presolved* ref_presolve(const nir_lp_view* v, const int8_t* vartype, int level, int rounds) {
+    sov::Model m = to_model(v);
+    if (vartype)
+        for (sov::Idx j = 0; j < v->ncol; ++j) m.vartype[size_t(j)] = static_cast<sov::VarType>(vartype[j]);
+    auto h = std::make_unique<ref_presolved>();
+    h->r = sov::Presolver::presolve(m, level, rounds);
+    return h.release();
+}
+
+int ref_presolved_status(const ref_presolved* h, int* status, int* solved, int* counters3) {
+    *status = static_cast<int>(h->r.status);
+    *solved = h->r.solved_in_presolve ? 1 : 0;
+    counters3[0] = h->r.rows_removed;
+    counters3[1] = h->r.cols_removed;
+    counters3[2] = h->r.bound_tightenings;
+    return 0;
+}
+
+int ref_presolved_reduced(const ref_presolved* h, nir_lp_view* v, int8_t* vartype) {
+    const sov::Model& m = h->r.reduced;
+    v->nrow = m.nrow;
+    v->ncol = m.ncol;
+    v->nnz = m.A.nnz();
+    v->col_start = m.A.start.data();
+    v->row_index = m.A.index.data();
+    v->value = m.A.value.data();
+    v->cost = m.cost.data();
+    v->collo = m.collo.data();
+    v->colup = m.colup.data();
+    v->rowlo = m.rowlo.data();
+    v->rowup = m.rowup.data();
+    v->obj_offset = m.obj_offset;
+    if (vartype)
+        for (sov::Idx j = 0; j < m.ncol; ++j) vartype[j] = static_cast<int8_t>(m.vartype[size_t(j)]);
+    return 0;
+}
+
+// sizes: col_map / row_map as the reduced model, fixed_x / is_fixed as the original
+int ref_presolved_maps(const ref_presolved* h, int32_t* col_map, int32_t* row_map, double* fixed_x, uint8_t* is_fixed) {
+    for (size_t j = 0; j < h->r.orig_col_map.size(); ++j) col_map[j] = h->r.orig_col_map[j];
+    for (size_t i = 0; i < h->r.orig_row_map.size(); ++i) row_map[i] = h->r.orig_row_map[i];
+    for (size_t j = 0; j < h->r.fixed_x.size(); ++j) fixed_x[j] = h->r.fixed_x[j];
+    for (size_t j = 0; j < h->r.is_col_fixed.size(); ++j) is_fixed[j] = h->r.is_col_fixed[j] ? 1 : 0;
+    return 0;
+}
+
+int64_t ref_presolved_map_sizes(const ref_presolved* h, int64_t* ncols) {
+    *ncols = int64_t(h->r.orig_col_map.size());
+    return int64_t(h->r.orig_row_map.size());
+}
+
+void ref_presolved_free(ref_presolved* h) { delete h; }
+
+// scale_model: scales and the scaled arrays (Q scaled when qnnz > 0)
+int ref_scale(const nir_lp_view* v, const int8_t* vartype, int enable, int64_t qnnz, const int64_t* q_start,
+              const int32_t* q_index, const double* q_value, double* R, double* C, int* active, double* cost,
+              double* collo, double* colup, double* value, double* rowlo, double* rowup, double* q_out) {
+    sov::Model m = to_model(v);
+    if (vartype)
+        for (sov::Idx j = 0; j < v->ncol; ++j) m.vartype[size_t(j)] = static_cast<sov::VarType>(vartype[j]);
+    if (qnnz > 0) {
+        m.Q.start.assign(q_start, q_start + v->ncol + 1);
+        m.Q.index.assign(q_index, q_index + qnnz);
+        m.Q.value.assign(q_value, q_value + qnnz);
+    }
+    sov::ScalingInfo info;
+    sov::Model s = sov::scale_model(m, enable != 0, info);
+    *active = info.active ? 1 : 0;
+    std::copy(info.R.begin(), info.R.end(), R);
+    std::copy(info.C.begin(), info.C.end(), C);
+    std::copy(s.cost.begin(), s.cost.end(), cost);
+    std::copy(s.collo.begin(), s.collo.end(), collo);
+    std::copy(s.colup.begin(), s.colup.end(), colup);
+    std::copy(s.A.value.begin(), s.A.value.end(), value);
+    std::copy(s.rowlo.begin(), s.rowlo.end(), rowlo);
+    std::copy(s.rowup.begin(), s.rowup.end(), rowup);
+    if (qnnz > 0) std::copy(s.Q.value.begin(), s.Q.value.end(), q_out);
+    return 0;
+}
 
 }  // extern "C"

@@ -21,6 +21,7 @@ def _native_libs():
 
     build.build_lpgen()
     build.build_mps()
+    build.build_facade()
     import subprocess
 
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "oracle"], check=True)
