@@ -557,11 +557,30 @@ struct Reader {
         const int fd = ::open(path, O_RDONLY);
         if (fd < 0) throw InputError(std::string("Cannot open MPS file: ") + path);
         struct stat st;
-        if (::fstat(fd, &st) != 0 || !S_ISREG(st.st_mode)) {
+        if (::fstat(fd, &st) != 0) {
             ::close(fd);
-            // not a regular file: the reference's ifstream would read it as
-            // a stream; this reader takes regular files only
             throw InputError(std::string("Cannot open MPS file: ") + path);
+        }
+        if (!S_ISREG(st.st_mode)) {
+            // a pipe or a device is read as a stream, as std::ifstream reads
+            // it; a directory opens but yields no line, so the model is empty
+            std::vector<char> v;
+            if (!S_ISDIR(st.st_mode)) {
+                std::vector<char> tmp(size_t(1) << 16);
+                for (;;) {
+                    const ssize_t r = ::read(fd, tmp.data(), tmp.size());
+                    if (r < 0 && errno == EINTR) continue;
+                    if (r <= 0) break;
+                    v.insert(v.end(), tmp.data(), tmp.data() + r);
+                }
+            }
+            ::close(fd);
+            size = v.size();
+            store.reset(new char[size + kPad]);
+            if (size) std::memcpy(store.get(), v.data(), size);
+            std::memset(store.get() + size, '\n', kPad);
+            buf = store.get();
+            return;
         }
         size = size_t(st.st_size);
         // one '\n' after the file, then padding for the 16-byte loads

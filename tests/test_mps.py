@@ -239,3 +239,28 @@ def test_decimal_conversion_matches_strtod(tmp_path):
     assert out.returncode == 0, out.stdout
     checked, accepted = int(out.stdout.split()[1]), int(out.stdout.split()[3])
     assert "mismatches 0" in out.stdout and accepted > 0.9 * checked, out.stdout
+
+
+def test_directory_reads_as_an_empty_model(tmp_path):
+    # std::ifstream opens a directory and getline yields nothing: an empty,
+    # valid model (status 0), which the reference reader returns too
+    from nirnaya_b200 import mps
+
+    m = mps.read_mps(str(tmp_path))
+    assert (m.lp.nrow, m.lp.ncol, m.lp.nnz, m.sense) == (0, 0, 0, 1)
+    if _ref_available():
+        _check_against_reference(_ours(str(tmp_path)), str(tmp_path), "directory")
+
+
+def test_a_pipe_is_read_as_a_stream(tmp_path):
+    import sys
+
+    code = ("import sys; sys.path.insert(0, %r); from nirnaya_b200 import mps; m = mps.read_mps('/dev/stdin'); "
+            "print(m.lp.nrow, m.lp.ncol, m.lp.nnz, repr(m.lp.cost.tolist()))" % ROOT)
+    out = subprocess.run([sys.executable, "-c", code], input=CASES["basic"], capture_output=True, text=True,
+                         timeout=120)
+    path = _write(tmp_path, "basic", CASES["basic"])
+    from nirnaya_b200 import mps
+
+    m = mps.read_mps(path)
+    assert out.stdout.strip() == f"{m.lp.nrow} {m.lp.ncol} {m.lp.nnz} {m.lp.cost.tolist()!r}", out.stderr
