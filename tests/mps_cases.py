@@ -413,3 +413,91 @@ def random_mps(lp, seed: int, integer_frac: float = 0.1, ranges: bool = True, se
             out.append(f" UP BND C{j} {_num(rng, b)}")
     out.append("ENDATA")
     return nl.join(out) + nl
+
+
+# number spellings std::stod accepts, and tokens it rejects or overflows on
+_GOOD = ["1", "-2.5", "3e2", "4D-1", "0.0", "-0", ".5", "5.", "+7", "1e20", "-1e20", "1e19", "00012", "2.25d+1",
+        "0.1", "1.0000000000000000000001", "123456789012345678901234", "7E-3", "-0.0"]
+_BAD = ["abc", "1e400", "1e-400", "x1", "inf", "nan", "0x10", "1.5x", "2d", "1e"]
+
+
+def _num(rng, pbad):
+    return str(rng.choice(_BAD)) if rng.random() < pbad else str(rng.choice(_GOOD))
+
+
+def fuzz_mps(rng):
+    """A random MPS text: a mostly valid skeleton (NAME, OBJSENSE / OBJNAME
+    forms, ROWS with odd types and duplicates, COLUMNS with markers, column-0
+    lines and headers inside, RHS with and without set names, RANGES,
+    BOUNDS of every type, a quadratic block) with comments, CRLF and, now
+    and then, tokens that are not numbers or not names."""
+    pbad = rng.choice([0.0, 0.0, 0.002, 0.02])
+    nr, nc = int(rng.integers(1, 30)), int(rng.integers(1, 40))
+    rows = [f"R{i}" for i in range(nr)]
+    cols = [f"C{j}" for j in range(nc)]
+    L = []
+
+    def noise():
+        if rng.random() < 0.05:
+            L.append(str(rng.choice(["", "* c", "   ", "\t*", "*"])))
+
+    L.append("NAME " + ("M%d" % rng.integers(99) if rng.random() < 0.8 else ""))
+    if rng.random() < 0.3:
+        L += ["OBJSENSE", "    " + str(rng.choice(["MAX", "MIN", "MAXIMIZE"]))] if rng.random() < 0.5 else \
+             ["OBJSENSE " + str(rng.choice(["MAX", "MIN"]))]
+    if rng.random() < 0.15:
+        L.append("OBJNAME " + str(rng.choice(["OBJ", "F2", "R0"])))
+    L.append(str(rng.choice(["ROWS", "rows", "Rows"])))
+    L.append(" N OBJ")
+    if rng.random() < 0.3:
+        L.append(" N F2")
+    for r in rows:
+        L.append(f" {rng.choice(list('LGEXle'))} {r}")
+        noise()
+    if rng.random() < 0.05:
+        L.append(f" L {rows[0]}")  # duplicate row
+    L.append("COLUMNS")
+    in_int = False
+    for c in cols:
+        if rng.random() < 0.15:
+            in_int = not in_int
+            L.append(f"    M{rng.integers(9)} 'MARKER' '{'INTORG' if in_int else 'INTEND'}'")
+        k = int(rng.integers(0, 5))
+        names = ["OBJ"] * (rng.random() < 0.7) + list(rng.choice(rows + ["F2", "zz"], size=k))
+        i = 0
+        while i < len(names):
+            two = rng.random() < 0.5 and i + 1 < len(names)
+            t = [c] + [f"{nm} {_num(rng, pbad)}" for nm in names[i:i + (2 if two else 1)]]
+            L.append((" " if rng.random() < 0.95 else "") + " ".join(t))
+            i += 2 if two else 1
+            noise()
+        if rng.random() < 0.03:
+            L.append("OBJSENSE MAX")
+    if in_int and rng.random() < 0.7:
+        L.append("    MX 'MARKER' 'INTEND'")
+    L.append("RHS")
+    for r in rng.choice(rows + ["OBJ"], size=int(rng.integers(0, nr + 1))):
+        L.append((" RHS " if rng.random() < 0.6 else " ") + f"{r} {_num(rng, pbad)}")
+    if rng.random() < 0.5:
+        L.append("RANGES")
+        for r in rng.choice(rows, size=int(rng.integers(0, nr + 1))):
+            L.append(f" RNG {r} {_num(rng, pbad)}")
+    if rng.random() < 0.8:
+        L.append("BOUNDS")
+        for _ in range(int(rng.integers(0, 2 * nc))):
+            bt = str(rng.choice(["UP", "LO", "FX", "FR", "MI", "PL", "BV", "LI", "UI", "SC", "up", "fx"]))
+            c = str(rng.choice(cols + (["nope"] if rng.random() < 0.02 else [])))
+            if bt.upper() in ("FR", "MI", "PL", "BV"):
+                L.append(f" {bt} BND {c}")
+            elif rng.random() < 0.8:
+                L.append(f" {bt} BND {c} {_num(rng, pbad)}")
+            else:
+                L.append(f" {bt} {c} {_num(rng, pbad)}")
+    if rng.random() < 0.2:
+        L.append(str(rng.choice(["QUADOBJ", "QMATRIX", "QSECTION"])))
+        for _ in range(int(rng.integers(0, 6))):
+            L.append(f" {rng.choice(cols)} {rng.choice(cols)} {_num(rng, pbad)}")
+    if rng.random() < 0.9:
+        L.append("ENDATA")
+    nl = str(rng.choice(["\n", "\r\n"]))
+    return nl.join(L) + (nl if rng.random() < 0.9 else "")

@@ -264,3 +264,21 @@ def test_a_pipe_is_read_as_a_stream(tmp_path):
 
     m = mps.read_mps(path)
     assert out.stdout.strip() == f"{m.lp.nrow} {m.lp.ncol} {m.lp.nnz} {m.lp.cost.tolist()!r}", out.stderr
+
+
+def test_random_files_match_the_reference_live(tmp_path):
+    """Differential fuzzing: 400 seeded random files (mps_cases.fuzz_mps),
+    each read at 1-4 threads, against the reference reader.  Valid models,
+    every error message and every status must agree."""
+    if not _ref_available():
+        pytest.skip("the reference build (oracle/_ref) is absent")
+    from mps_cases import fuzz_mps
+
+    outcomes = set()
+    for seed in range(400):
+        rng = np.random.default_rng([0xF22, seed])
+        path = _write(tmp_path, "fuzz", fuzz_mps(rng))
+        got = _ours(path, int(rng.integers(1, 5)))
+        outcomes.add(got["status"] if got["status"] else ("ok", got["lp"].nnz > 0))
+        _check_against_reference(got, path, f"fuzz seed {seed}")
+    assert {("ok", True), 1, 12} <= outcomes
