@@ -58,3 +58,27 @@ def test_reference_arm_prints_one_contract_line():
     cb = line["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["cores"] >= 1 and "PdhgSolver::solve" in cb["sample"]
     assert set(cb["iterations_per_s_by_threads"]) >= {"1"}
+
+
+def _bench_line(tmp_path, *args):
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), *args, "--mps-dir", str(tmp_path)],
+                         capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert out.returncode == 0, out.stderr
+    return json.loads(out.stdout.strip().splitlines()[-1])
+
+
+def test_mps_read_mode_line(tmp_path):
+    line = _bench_line(tmp_path, "--mps-read", "--workload", "c1", "--steps", "2", "--warmup", "1")
+    assert line["metric"] == "mps_read_throughput" and line["unit"] == "MB/s" and line["value"] > 0
+    assert line["config"]["workload"] == "random_eq_2000x5000_nnz40000.mps" and line["config"]["nnz"] == 40000
+    assert set(line["seconds_by_threads"]) >= {"1"}
+    if line["reference"] is not None:
+        assert line["reference"]["models_bit_identical"] is True
+
+
+def test_host_path_mode_line(tmp_path):
+    line = _bench_line(tmp_path, "--host-path", "--workload", "c1")
+    assert line["metric"] == "host_path_seconds" and line["higher_is_better"] is False
+    assert set(line["seconds"]) == {"read", "presolve", "scale"}
+    if line["reference"] is not None:
+        assert line["reference"]["scaled_model_bit_identical"] is True
