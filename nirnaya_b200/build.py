@@ -84,7 +84,7 @@ def build_lpgen(force: bool = False, verbose: bool = False) -> str:
 def build_mps(force: bool = False, verbose: bool = False) -> str:
     target = os.path.join(HERE, "libnir_mps.so")
     srcs = [os.path.join(CSRC, "mps.cpp"), os.path.join(CSRC, "mps_write.cpp"), os.path.join(CSRC, "decimal.hpp"),
-            os.path.join(INC, "nir_mps.h"), os.path.join(INC, "nir_lp.h")]
+            os.path.join(CSRC, "text.hpp"), os.path.join(INC, "nir_mps.h"), os.path.join(INC, "nir_lp.h")]
     if force or _stale(target, srcs):
         cxx = os.environ.get("CXX", "g++")
         cmd = [cxx, "-std=c++17", "-O3", "-fPIC", "-shared", "-pthread", "-I" + INC, srcs[0], srcs[1], "-o", target]

@@ -421,7 +421,7 @@ _GOOD = ["1", "-2.5", "3e2", "4D-1", "0.0", "-0", ".5", "5.", "+7", "1e20", "-1e
 _BAD = ["abc", "1e400", "1e-400", "x1", "inf", "nan", "0x10", "1.5x", "2d", "1e"]
 
 
-def _num(rng, pbad):
+def _fuzz_num(rng, pbad):
     return str(rng.choice(_BAD)) if rng.random() < pbad else str(rng.choice(_GOOD))
 
 
@@ -467,7 +467,7 @@ def fuzz_mps(rng):
         i = 0
         while i < len(names):
             two = rng.random() < 0.5 and i + 1 < len(names)
-            t = [c] + [f"{nm} {_num(rng, pbad)}" for nm in names[i:i + (2 if two else 1)]]
+            t = [c] + [f"{nm} {_fuzz_num(rng, pbad)}" for nm in names[i:i + (2 if two else 1)]]
             L.append((" " if rng.random() < 0.95 else "") + " ".join(t))
             i += 2 if two else 1
             noise()
@@ -477,11 +477,11 @@ def fuzz_mps(rng):
         L.append("    MX 'MARKER' 'INTEND'")
     L.append("RHS")
     for r in rng.choice(rows + ["OBJ"], size=int(rng.integers(0, nr + 1))):
-        L.append((" RHS " if rng.random() < 0.6 else " ") + f"{r} {_num(rng, pbad)}")
+        L.append((" RHS " if rng.random() < 0.6 else " ") + f"{r} {_fuzz_num(rng, pbad)}")
     if rng.random() < 0.5:
         L.append("RANGES")
         for r in rng.choice(rows, size=int(rng.integers(0, nr + 1))):
-            L.append(f" RNG {r} {_num(rng, pbad)}")
+            L.append(f" RNG {r} {_fuzz_num(rng, pbad)}")
     if rng.random() < 0.8:
         L.append("BOUNDS")
         for _ in range(int(rng.integers(0, 2 * nc))):
@@ -490,13 +490,13 @@ def fuzz_mps(rng):
             if bt.upper() in ("FR", "MI", "PL", "BV"):
                 L.append(f" {bt} BND {c}")
             elif rng.random() < 0.8:
-                L.append(f" {bt} BND {c} {_num(rng, pbad)}")
+                L.append(f" {bt} BND {c} {_fuzz_num(rng, pbad)}")
             else:
-                L.append(f" {bt} {c} {_num(rng, pbad)}")
+                L.append(f" {bt} {c} {_fuzz_num(rng, pbad)}")
     if rng.random() < 0.2:
         L.append(str(rng.choice(["QUADOBJ", "QMATRIX", "QSECTION"])))
         for _ in range(int(rng.integers(0, 6))):
-            L.append(f" {rng.choice(cols)} {rng.choice(cols)} {_num(rng, pbad)}")
+            L.append(f" {rng.choice(cols)} {rng.choice(cols)} {_fuzz_num(rng, pbad)}")
     if rng.random() < 0.9:
         L.append("ENDATA")
     nl = str(rng.choice(["\n", "\r\n"]))
