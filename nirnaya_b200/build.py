@@ -3,7 +3,7 @@
   nirnaya_b200/libnir_pdhg.so   CUDA engine + C ABI (nvcc, sm_100a only)
   nirnaya_b200/libnir_lpgen.so  seeded instance generator (g++)
   nirnaya_b200/libnir_mlp.so    warm-start network (nvcc, sm_100a)
-  nirnaya_b200/libnir_mps.so    multi-threaded MPS reader (g++, host only)
+  nirnaya_b200/libnir_mps.so    multi-threaded MPS and SOL file I/O, solution check (g++, host only)
   nirnaya_b200/libnir_facade.so presolve and scaling before the path (g++, host only)
 
 Run `python -m nirnaya_b200.build` or call build_all().
@@ -83,11 +83,14 @@ def build_lpgen(force: bool = False, verbose: bool = False) -> str:
 
 def build_mps(force: bool = False, verbose: bool = False) -> str:
     target = os.path.join(HERE, "libnir_mps.so")
-    srcs = [os.path.join(CSRC, "mps.cpp"), os.path.join(CSRC, "mps_write.cpp"), os.path.join(CSRC, "decimal.hpp"),
-            os.path.join(CSRC, "text.hpp"), os.path.join(INC, "nir_mps.h"), os.path.join(INC, "nir_lp.h")]
+    srcs = [os.path.join(CSRC, "mps.cpp"), os.path.join(CSRC, "mps_write.cpp"), os.path.join(CSRC, "sol.cpp"),
+            os.path.join(CSRC, "decimal.hpp"), os.path.join(CSRC, "text.hpp"), os.path.join(INC, "nir_mps.h"),
+            os.path.join(INC, "nir_sol.h"), os.path.join(INC, "nir_lp.h")]
     if force or _stale(target, srcs):
         cxx = os.environ.get("CXX", "g++")
-        cmd = [cxx, "-std=c++17", "-O3", "-fPIC", "-shared", "-pthread", "-I" + INC, srcs[0], srcs[1], "-o", target]
+        # no FMA contraction: the double-double steps of sol.cpp need each rounding
+        cmd = [cxx, "-std=c++17", "-O3", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared", "-pthread",
+               "-I" + INC, *srcs[:3], "-o", target]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.run(cmd, check=True)

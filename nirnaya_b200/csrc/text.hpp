@@ -115,6 +115,29 @@ struct NameMap {
     int32_t find(const char* p, size_t n) const { return find_h(hash_name(p, n), p, n); }
     // returns the existing value, or inserts v and returns -1
     int32_t insert(const char* p, size_t n, int32_t v) { return insert_h(hash_name(p, n), p, p, n, v); }
+    // inserts, or sets the value of a name already there
+    void assign(const char* p, size_t n, int32_t v) {
+        if (2 * (count + 1) > slots.size()) grow();
+        const uint64_t h = hash_name(p, n);
+        const size_t mask = slots.size() - 1;
+        const uint32_t tag = uint32_t(h >> 32);
+        for (size_t i = h & mask;; i = (i + 1) & mask) {
+            Slot& s = slots[i];
+            if (s.v < 0) {
+                s.tag = tag;
+                s.n = uint32_t(n);
+                s.v = v;
+                s.p = p;
+                std::memcpy(s.key, p, std::min<size_t>(n, 16));
+                ++count;
+                return;
+            }
+            if (same(s, tag, p, n)) {
+                s.v = v;
+                return;
+            }
+        }
+    }
     // with the hash given; `cmp` holds the name's bytes (a copy of the first
     // 16 when n <= 16 is enough), `p` is what the slot keeps
     int32_t insert_h(uint64_t h, const char* cmp, const char* p, size_t n, int32_t v) {

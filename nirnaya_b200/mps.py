@@ -1,4 +1,5 @@
-"""Python binding of the multi-threaded MPS reader (libnir_mps.so, include/nir_mps.h).
+"""Python binding of the multi-threaded MPS reader (libnir_mps.so, include/nir_mps.h)
+and of the SOL file I/O and solution check in the same library (include/nir_sol.h).
 
 `read_mps(path)` is sov::MpsReader::read (src/io/mps_reader.hpp:15-304)
 followed by Model::validate (src/model/model.hpp:117-178): it returns the
@@ -22,6 +23,12 @@ _LIB = None
 
 EXPORTED = ["nir_mps_read", "nir_mps_view", "nir_mps_vartypes", "nir_mps_model_name", "nir_mps_names",
             "nir_mps_quadratic", "nir_mps_timings", "nir_mps_free", "nir_mps_write", "nir_mps_last_error"]
+EXPORTED_SOL = ["nir_sol_write", "nir_sol_read", "nir_sol_objective_token", "nir_eval_objective",
+                "nir_verify_solution"]
+
+# worst_kind of nir_verify_report -> the reference's worst_item prefix (src/io/sol_io.hpp:33-92)
+WORST_ITEM = {0: "", 1: "Solution size mismatch", 2: "NaN/Inf in variable ", 3: "Lower bound on ",
+              4: "Upper bound on ", 5: "Integrality on ", 6: "Row lower bound on ", 7: "Row upper bound on "}
 
 CONTINUOUS, INTEGER, BINARY = 0, 1, 2
 TIMING_PHASES = ("file_read", "line_scan", "columns_parse", "columns_replay", "csc_build", "other")
@@ -66,6 +73,22 @@ def lib() -> C.CDLL:
         L.nir_mps_free.argtypes = [C.c_void_p]
         L.nir_mps_last_error.restype = C.c_char_p
         L.nir_mps_last_error.argtypes = []
+        _D = C.POINTER(C.c_double)
+        L.nir_sol_write.restype = C.c_int
+        L.nir_sol_write.argtypes = [C.c_char_p, C.c_char_p, C.c_double, C.c_double, C.c_int32, _D, C.c_int64,
+                                    C.POINTER(C.c_char_p), C.c_int64, C.c_int32]
+        L.nir_sol_read.restype = C.c_int
+        L.nir_sol_read.argtypes = [C.c_char_p, C.c_int32, C.POINTER(C.c_char_p), C.c_int32, _D, _D,
+                                   C.POINTER(C.c_int32)]
+        L.nir_sol_objective_token.restype = C.c_char_p
+        L.nir_sol_objective_token.argtypes = [C.c_int32]
+        L.nir_eval_objective.restype = C.c_double
+        L.nir_eval_objective.argtypes = [C.POINTER(NirLpView), C.c_int64, C.POINTER(C.c_int64),
+                                         C.POINTER(C.c_int32), _D, _D]
+        L.nir_verify_solution.restype = C.c_int
+        L.nir_verify_solution.argtypes = [C.POINTER(NirLpView), C.POINTER(C.c_int8), C.c_int64,
+                                          C.POINTER(C.c_int64), C.POINTER(C.c_int32), _D, _D, C.c_int64,
+                                          C.c_double, C.c_double, C.c_int32, C.POINTER(VerifyReport)]
         _LIB = L
     return _LIB
 
@@ -92,6 +115,12 @@ class MpsModel:
         out = LP(lp.nrow, lp.ncol, lp.col_start, lp.row_index, lp.value, -lp.cost, lp.collo, lp.colup, lp.rowlo,
                  lp.rowup, -lp.obj_offset)
         return out, -self.q_value
+
+
+class VerifyReport(C.Structure):
+    _fields_ = [("passed", C.c_int32), ("worst_kind", C.c_int32), ("worst_index", C.c_int64),
+                ("max_bound_viol", C.c_double), ("max_row_viol", C.c_double), ("max_int_viol", C.c_double),
+                ("computed_obj", C.c_double), ("obj_rel_err", C.c_double)]
 
 
 class _Handle:
@@ -189,3 +218,79 @@ def write_mps(path: str, lp: LP, vartype=None, sense: int = 1, name: str = "", c
                          int(sense), name.encode(), cn, rn, *qargs, int(threads), os.fsencode(path))
     if st != 0:
         raise MpsError(st, L.nir_mps_last_error().decode(errors="replace"))
+
+
+def _name_array(names):
+    if names is None:
+        return None, 0
+    arr = (C.c_char_p * len(names))()
+    arr[:] = [n.encode() for n in names]
+    return arr, len(names)
+
+
+def write_sol(path: str, x, status: str = "optimal", objective: float = 0.0, gap: float = 0.0, col_names=None,
+              ncol: int | None = None, threads: int = 0) -> None:
+    """SolIo::write_sol's bytes (src/io/sol_io.hpp:110-132); status is the
+    reference's status_to_string text."""
+    L = lib()
+    xv = np.ascontiguousarray(x, np.float64)
+    names, nn = _name_array(col_names)
+    st = L.nir_sol_write(os.fsencode(path), status.encode(), float(objective), float(gap),
+                         int(len(xv) if ncol is None else ncol), xv.ctypes.data_as(C.POINTER(C.c_double)),
+                         len(xv), names, nn, int(threads))
+    if st != 0:
+        raise MpsError(st, f"cannot write {path}")
+
+
+def read_sol(path: str, col_names, threads: int = 0):
+    """SolIo::read_sol (src/io/sol_io.hpp:134-170): (x, objective, the
+    objective lines' tokens)."""
+    L = lib()
+    names, n = _name_array(col_names)
+    x = np.zeros(n)
+    obj = C.c_double()
+    nobj = C.c_int32()
+    st = L.nir_sol_read(os.fsencode(path), n, names, int(threads), x.ctypes.data_as(C.POINTER(C.c_double)),
+                        C.byref(obj), C.byref(nobj))
+    if st == 14:
+        raise MpsError(st, f"cannot open {path}")
+    tokens = [L.nir_sol_objective_token(k).decode() for k in range(nobj.value)]
+    if st != 0:
+        raise MpsError(st, f"objective token is not a number: {tokens}")
+    return x, obj.value, tokens
+
+
+def _q_args(q):
+    if q is None:
+        return (0, None, None, None), None
+    qs, qi, qv = (np.ascontiguousarray(q[0], np.int64), np.ascontiguousarray(q[1], np.int32),
+                  np.ascontiguousarray(q[2], np.float64))
+    return (int(qs[-1]), qs.ctypes.data_as(C.POINTER(C.c_int64)), qi.ctypes.data_as(C.POINTER(C.c_int32)),
+            qv.ctypes.data_as(C.POINTER(C.c_double))), (qs, qi, qv)
+
+
+def eval_objective(lp: LP, x, q=None) -> float:
+    """Model::eval_objective (src/model/model.hpp:73-98) in double-double."""
+    qa, keep = _q_args(q)
+    xv = np.ascontiguousarray(x, np.float64)
+    return lib().nir_eval_objective(C.byref(lp.view()), *qa, xv.ctypes.data_as(C.POINTER(C.c_double)))
+
+
+def verify_solution(lp: LP, x, claimed_obj: float, tol: float = 1e-6, vartype=None, col_names=None,
+                    row_names=None, q=None, threads: int = 0) -> dict:
+    """verify_solution (src/io/sol_io.hpp:25-106): the report's fields, with
+    worst_item spelled as the reference spells it when names are given."""
+    qa, keep = _q_args(q)
+    xv = np.ascontiguousarray(x, np.float64)
+    vt = None if vartype is None else np.ascontiguousarray(vartype, np.int8)
+    rep = VerifyReport()
+    lib().nir_verify_solution(C.byref(lp.view()), None if vt is None else vt.ctypes.data_as(C.POINTER(C.c_int8)),
+                              *qa, xv.ctypes.data_as(C.POINTER(C.c_double)), len(xv), float(claimed_obj),
+                              float(tol), int(threads), C.byref(rep))
+    item = WORST_ITEM[rep.worst_kind]
+    if rep.worst_kind >= 2:
+        names = row_names if rep.worst_kind >= 6 else col_names
+        item += names[rep.worst_index] if names is not None else str(rep.worst_index)
+    return dict(passed=bool(rep.passed), max_bound_viol=rep.max_bound_viol, max_row_viol=rep.max_row_viol,
+                max_int_viol=rep.max_int_viol, computed_obj=rep.computed_obj, obj_rel_err=rep.obj_rel_err,
+                worst_item=item)

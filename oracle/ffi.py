@@ -118,6 +118,10 @@ def ref_lib():
         lib.ref_presolved_map_sizes.restype = C.c_int64
         lib.ref_presolved_map_sizes.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
         lib.ref_presolved_free.argtypes = [C.c_void_p]
+        lib.ref_write_sol.argtypes = [_VP, C.POINTER(C.c_char_p), C.c_int, C.c_double, C.c_double, _D, C.c_int64,
+                                      C.c_char_p]
+        lib.ref_verify_full.argtypes = [_VP, C.POINTER(C.c_int8), C.POINTER(C.c_char_p), _D, C.c_int64, C.c_double,
+                                        C.c_double, C.POINTER(C.c_int), _D, C.c_char_p, C.c_int]
         lib.ref_scale.argtypes = [_VP, C.POINTER(C.c_int8), C.c_int, C.c_int64, C.POINTER(C.c_int64),
                                   C.POINTER(C.c_int32), _D, _D, _D, C.POINTER(C.c_int)] + [_D] * 7
         _ref = lib
@@ -364,3 +368,52 @@ def ref_scale(lp: LP, vartype=None, enable: bool = True, q=None) -> dict:
                   _dptr(out["colup"]), _dptr(out["value"]), _dptr(out["rowlo"]), _dptr(out["rowup"]),
                   None if qo is None else _dptr(qo))
     return dict(active=bool(act.value), R=R, C=Cs, q_value=qo, **out)
+
+
+def _names(names):
+    arr = (C.c_char_p * len(names))()
+    arr[:] = [n.encode() for n in names]
+    return arr
+
+
+def ref_write_sol(lp: LP, names, status: int, obj: float, gap: float, x, path: str) -> int:
+    """SolIo::write_sol for a model with these column names."""
+    xv = np.ascontiguousarray(x, np.float64)
+    return ref_lib().ref_write_sol(C.byref(lp.view()), _names(names), status, obj, gap, _dptr(xv), len(xv),
+                                   path.encode())
+
+
+REF_SOL_TOOL = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_ref", "ref_sol_tool")
+
+
+def ref_read_sol(model_mps: str, sol_path: str, ncol: int):
+    """SolIo::read_sol of sol_path for the model in model_mps, run as its own
+    process (oracle/_ref/ref_sol_tool): ("ok", x, objective), ("exception",
+    what) or ("cannot-open",)."""
+    import subprocess
+
+    out = subprocess.run([REF_SOL_TOOL, model_mps, sol_path], capture_output=True, text=True, timeout=600)
+    lines = out.stdout.splitlines()
+    head = lines[0].split(" ", 1)
+    if head[0] in ("exception", "cannot-open", "model-error"):
+        return tuple(head)
+    obj = float.fromhex(lines[1].split()[1])
+    x = np.zeros(ncol)
+    for ln in lines[2:]:
+        j, v = ln.split()
+        x[int(j)] = float.fromhex(v)
+    return "ok", x, obj
+
+
+def ref_verify_full(lp: LP, x, claimed: float, tol: float = 1e-6, vartype=None, names=None) -> dict:
+    """verify_solution with every report field (names: C<j>/R<i> unless given)."""
+    xv = np.ascontiguousarray(x, np.float64)
+    vt = None if vartype is None else np.ascontiguousarray(vartype, np.int8)
+    passed = C.c_int()
+    out = np.zeros(5)
+    worst = C.create_string_buffer(512)
+    ref_lib().ref_verify_full(C.byref(lp.view()), None if vt is None else vt.ctypes.data_as(C.POINTER(C.c_int8)),
+                              None if names is None else _names(names), _dptr(xv), len(xv), claimed, tol,
+                              C.byref(passed), _dptr(out), worst, 512)
+    return dict(passed=bool(passed.value), max_bound_viol=out[0], max_row_viol=out[1], max_int_viol=out[2],
+                computed_obj=out[3], obj_rel_err=out[4], worst_item=worst.value.decode())

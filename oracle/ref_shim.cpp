@@ -15,11 +15,14 @@
 //   ref_write_mps       sov::MpsReader::write         src/io/mps_reader.hpp:306-412
 //   ref_mps_roundtrip   MpsReader::read then ::write  (names and all kept)
 //   ref_presolve        sov::Presolver::presolve      src/presolve/presolve.hpp:32-345
+//   ref_write_sol       sov::SolIo::write_sol         src/io/sol_io.hpp:110-132
+//   ref_verify_full     sov::verify_solution          src/io/sol_io.hpp:25-106 (every field)
 //   ref_scale           sov::scale_model              src/model/scaling.hpp:56-154
 //   ref_dd_probe        sov::dd_real / NeumaierSum    src/core/dd_real.hpp:27-104
 
 #include "include/sov/solver.hpp"
 
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -322,6 +325,39 @@ int64_t ref_presolved_map_sizes(const ref_presolved* h, int64_t* ncols) {
 }
 
 void ref_presolved_free(ref_presolved* h) { delete h; }
+
+namespace {
+sov::Model named_model(const nir_lp_view* v, const int8_t* vartype, const char* const* names) {
+    sov::Model m = to_model(v);
+    if (vartype)
+        for (sov::Idx j = 0; j < v->ncol; ++j) m.vartype[size_t(j)] = static_cast<sov::VarType>(vartype[j]);
+    if (names)
+        for (sov::Idx j = 0; j < v->ncol; ++j) m.col_names[size_t(j)] = names[j];
+    return m;
+}
+}  // namespace
+
+int ref_write_sol(const nir_lp_view* v, const char* const* names, int status, double obj, double gap,
+                  const double* x, int64_t nx, const char* path) {
+    sov::Model m = named_model(v, nullptr, names);
+    std::vector<double> xv(x, x + nx);
+    return sov::SolIo::write_sol(path, m, static_cast<sov::Status>(status), obj, gap, xv) ? 0 : 14;
+}
+
+int ref_verify_full(const nir_lp_view* v, const int8_t* vartype, const char* const* names, const double* x,
+                    int64_t nx, double claimed, double tol, int* passed, double* out5, char* worst, int worst_cap) {
+    sov::Model m = named_model(v, vartype, names);
+    std::vector<double> xv(x, x + nx);
+    sov::VerificationReport r = sov::verify_solution(m, xv, claimed, tol);
+    *passed = r.passed ? 1 : 0;
+    out5[0] = r.max_bound_viol;
+    out5[1] = r.max_row_viol;
+    out5[2] = r.max_int_viol;
+    out5[3] = r.computed_obj;
+    out5[4] = r.obj_rel_err;
+    std::snprintf(worst, size_t(worst_cap), "%s", r.worst_item.c_str());
+    return 0;
+}
 
 // scale_model: scales and the scaled arrays (Q scaled when qnnz > 0)
 int ref_scale(const nir_lp_view* v, const int8_t* vartype, int enable, int64_t qnnz, const int64_t* q_start,
