@@ -606,12 +606,15 @@ def mps_read_bench(args):
 
 
 def host_path_bench(args):
-    """The host steps Solver::solve takes before PdhgSolver::solve on the CLI
-    path (include/sov/solver.hpp:135-181): read the MPS file, presolve, scale.
-    This build's libraries (all host threads) against the reference's own
-    code (oracle/_ref, one thread, as it runs), each step once after one
-    warm-up, with a bit-for-bit comparison of the scaled model handed to
-    PDHG.  One JSON line; wall-clock timing (host-only work)."""
+    """The host steps of the CLI path around PdhgSolver::solve
+    (include/sov/solver.hpp:135-313): read the MPS file, presolve, scale;
+    then, on a solution (the reduced model's bound-clipped midpoint, put
+    back by postsolve), verify it in double-double and write the SOL file.
+    This build's libraries (all host threads; each step's best of three
+    runs after one warm-up) against the reference's own code (oracle/_ref,
+    one thread, as it runs; each step once), with a bit-for-bit comparison of the scaled model handed to
+    PDHG and of the verification report.  One JSON line; wall-clock timing
+    (host-only work)."""
     import numpy as np
 
     from nirnaya_b200 import facade
@@ -625,6 +628,11 @@ def host_path_bench(args):
     lp = L.generate(wl["kind"], wl["seed"], **wl["kw"])
     mps.write_mps(path, lp, name=wl["label"])
 
+    def solution(lpm, pre):
+        lo = np.where(np.isfinite(pre.reduced.collo), pre.reduced.collo, -1.0)
+        up = np.where(np.isfinite(pre.reduced.colup), pre.reduced.colup, 1.0)
+        return pre.postsolve(0.5 * (lo + up))
+
     def ours():
         t = {}
         t0 = time.perf_counter()
@@ -637,10 +645,20 @@ def host_path_bench(args):
         t0 = time.perf_counter()
         sc = facade.scale(pre.reduced, pre.vartype)
         t["scale"] = time.perf_counter() - t0
-        return t, sc
+        x = solution(lpm, pre)
+        t0 = time.perf_counter()
+        obj = mps.eval_objective(lpm, x)
+        rep = mps.verify_solution(lpm, x, obj, 1e-6, m.vartype)
+        t["verify"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        mps.write_sol(path + ".ours.sol", x, "optimal", obj, 0.0)  # the file's names are C<j>
+        t["write_sol"] = time.perf_counter() - t0
+        return t, sc, x, obj, rep
 
     ours()
-    t_ours, sc = ours()
+    runs = [ours() for _ in range(3)]
+    t_ours = {k: min(r[0][k] for r in runs) for k in runs[0][0]}  # each step's best of three
+    _, sc, x, obj, rep = runs[-1]
     ref = None
     if ffi.ref_available():
         t = {}
@@ -653,12 +671,27 @@ def host_path_bench(args):
         t0 = time.perf_counter()
         rs = ffi.ref_scale(rp["reduced"], rp["vartype"])
         t["scale"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        rrep = ffi.ref_verify_full(rl, x, obj, 1e-6, vartype=rvt)
+        t["verify"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        ffi.ref_write_sol(rl, None, 0, obj, 0.0, x, path + ".ref.sol")
+        t["write_sol"] = time.perf_counter() - t0
         same = (sc.active == rs["active"] and np.array_equal(sc.R, rs["R"]) and np.array_equal(sc.C, rs["C"]) and
                 all(np.array_equal(getattr(sc.lp, k).view(np.uint8), rs[k].view(np.uint8))
                     for k in ("cost", "collo", "colup", "value", "rowlo", "rowup")))
+        same_rep = all(np.float64(rep[k]).tobytes() == np.float64(rrep[k]).tobytes()
+                       for k in ("max_bound_viol", "max_row_viol", "max_int_viol", "computed_obj", "obj_rel_err"))
+        with open(path + ".ours.sol", "rb") as a, open(path + ".ref.sol", "rb") as b:
+            same_sol = a.read() == b.read()
         ref = {"seconds": t, "total": sum(t.values()), "cores": 1, "kind": "reference",
-               "sample": "MpsReader::read, Presolver::presolve (level 2), scale_model, once each",
-               "scaled_model_bit_identical": bool(same)}
+               "sample": "MpsReader::read, Presolver::presolve (level 2), scale_model, verify_solution, "
+                         "SolIo::write_sol, once each",
+               "scaled_model_bit_identical": bool(same), "verification_bit_identical": bool(same_rep),
+               "sol_bytes_identical": bool(same_sol)}
+    for suffix in (".ours.sol", ".ref.sol"):
+        if os.path.exists(path + suffix):
+            os.remove(path + suffix)
     total = sum(t_ours.values())
     print(json.dumps({"metric": "host_path_seconds", "value": total, "unit": "s", "higher_is_better": False,
                       "data": "synthetic (seeded generator, include/nir_lpgen.h), written as MPS",
@@ -724,7 +757,8 @@ def main():
     ap.add_argument("--mps-dir", default=os.path.join(ROOT, "_bench_tmp"),
                     help="where --mps-read writes its input file")
     ap.add_argument("--host-path", action="store_true",
-                    help="MPS read + presolve + scale (the CLI's host steps before PDHG) against the reference's")
+                    help="the CLI's host steps around PDHG (read, presolve, scale, verify, write_sol) "
+                         "against the reference's")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     if args.host_path:

@@ -377,10 +377,10 @@ def _names(names):
 
 
 def ref_write_sol(lp: LP, names, status: int, obj: float, gap: float, x, path: str) -> int:
-    """SolIo::write_sol for a model with these column names."""
+    """SolIo::write_sol for a model with these column names (None: C<j>)."""
     xv = np.ascontiguousarray(x, np.float64)
-    return ref_lib().ref_write_sol(C.byref(lp.view()), _names(names), status, obj, gap, _dptr(xv), len(xv),
-                                   path.encode())
+    return ref_lib().ref_write_sol(C.byref(lp.view()), None if names is None else _names(names), status, obj, gap,
+                                   _dptr(xv), len(xv), path.encode())
 
 
 REF_SOL_TOOL = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_ref", "ref_sol_tool")

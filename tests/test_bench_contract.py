@@ -79,6 +79,7 @@ def test_mps_read_mode_line(tmp_path):
 def test_host_path_mode_line(tmp_path):
     line = _bench_line(tmp_path, "--host-path", "--workload", "c1")
     assert line["metric"] == "host_path_seconds" and line["higher_is_better"] is False
-    assert set(line["seconds"]) == {"read", "presolve", "scale"}
+    assert set(line["seconds"]) == {"read", "presolve", "scale", "verify", "write_sol"}
     if line["reference"] is not None:
-        assert line["reference"]["scaled_model_bit_identical"] is True
+        ref = line["reference"]
+        assert ref["scaled_model_bit_identical"] and ref["verification_bit_identical"] and ref["sol_bytes_identical"]
