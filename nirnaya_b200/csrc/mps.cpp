@@ -523,7 +523,7 @@ struct Reader {
                 tokenize(buf + this_line, buf + le, tk);
                 if (tk.empty()) continue;
                 int marker = -1;
-                if (memmem(buf + this_line, le - this_line, "INT", 3)) {
+                if (std::memchr(buf + this_line, 'I', le - this_line)) {  // both markers hold an I
                     for (const Tok& t : tk) {
                         if (contains(t, "INTORG", 6)) marker = 1;
                         else if (contains(t, "INTEND", 6)) marker = 0;
