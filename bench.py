@@ -602,6 +602,7 @@ def mps_read_bench(args):
             "seconds_by_threads": by_threads,
             "writer_seconds": t_write, "reference": ref,
             "speedup_vs_reference": (ref["seconds"] / t) if ref else None}
+    os.remove(path)  # a few hundred MB: not left in the tree
     print(json.dumps(line))
 
 
@@ -689,13 +690,14 @@ def host_path_bench(args):
                          "SolIo::write_sol, once each",
                "scaled_model_bit_identical": bool(same), "verification_bit_identical": bool(same_rep),
                "sol_bytes_identical": bool(same_sol)}
-    for suffix in (".ours.sol", ".ref.sol"):
+    size = os.path.getsize(path)
+    for suffix in (".ours.sol", ".ref.sol", ""):  # a few hundred MB: not left in the tree
         if os.path.exists(path + suffix):
             os.remove(path + suffix)
     total = sum(t_ours.values())
     print(json.dumps({"metric": "host_path_seconds", "value": total, "unit": "s", "higher_is_better": False,
                       "data": "synthetic (seeded generator, include/nir_lpgen.h), written as MPS",
-                      "config": {"workload": wl["label"] + ".mps", "bytes": os.path.getsize(path),
+                      "config": {"workload": wl["label"] + ".mps", "bytes": size,
                                  "threads": os.cpu_count(), "reduced": [sc.lp.nrow, sc.lp.ncol, sc.lp.nnz]},
                       "seconds": t_ours, "reference": ref,
                       "speedup_vs_reference": (ref["total"] / total) if ref else None}))
