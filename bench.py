@@ -30,7 +30,7 @@ reference's own PdhgSolver::solve (compiled from source into oracle/_ref) on
 a bounded sample of the same workload.
 
 With --gpus N > 1 (torchrun), every rank solves its own replica (the path
-does not shard a single LP; see DESIGN.md) and the time is the max over
+does not shard a single LP) and the time is the max over
 ranks.  --impl reference runs the reference's CPU PDHG on rank 0 only.
 """
 from __future__ import annotations
@@ -185,7 +185,8 @@ def dual_bytes(lp, w):
 
 
 def spmv_bytes(lp, transpose, word):
-    """Algorithmic bytes of a plain CSR SpMV (SURVEY's formula)."""
+    """Algorithmic bytes of a plain CSR SpMV: index and value per nonzero, row
+    pointers, the input vector read once, the output vector written once."""
     R, Cc = (lp.ncol, lp.nrow) if transpose else (lp.nrow, lp.ncol)
     iw = 4
     return (iw + word) * lp.nnz + 4 * (R + 1) + word * Cc + word * R

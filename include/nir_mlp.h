@@ -6,7 +6,7 @@
  * iterate, dual iterate and primal weight for the PDLP engine
  * (nir_pdhg_params.x_init / y_init / omega_init in nir_pdhg.h).  The
  * reference has no learned component: this is new, and the PDLP engine
- * stays both the fallback and the judge (a warm start counts only when the
+ * stays both the fallback and the arbiter (a warm start counts only when the
  * solve it seeds reaches the same relative-KKT tolerance).
  *
  * Layers: d_in -> width (ReLU) -> ... (depth hidden layers) -> d_out.

@@ -14,7 +14,7 @@ generates for training instances.  Its prediction seeds the engine
 (x_init, y_init, omega_init); `evaluate` solves each held-out instance cold
 and warm to the same relative-KKT tolerance: a warm result is accepted only
 when its solve reaches that tolerance, otherwise the cold result stands
-(the cold-start PDLP is both the fallback and the judge).
+(the cold-start PDLP is both the fallback and the arbiter).
 """
 from __future__ import annotations
 
