@@ -22,9 +22,14 @@
 //   * the solve stops at 1e-6 relative KKT and, so that Solver's dd_real
 //     verification passes, at a per-row relative violation of at most
 //     0.1 * tol.checker_tol.
+//   * the scales of scale_model (which Solver applies just before) are
+//     undone exactly before the engine runs and the solution is mapped
+//     back: the engine preconditions by itself, and power-of-two
+//     equilibration ahead of it slows the restarted PDHG's duality gap;
 // Environment knobs (no Options field is added, so options.hpp stays as
 // it is): NIR_PDHG_ALGO = pdlp | pdhg | reference, NIR_PDHG_PRECISION =
-// mixed | fp64 | fp32, NIR_PDHG_TOL, NIR_PDHG_MAX_ITERS, NIR_PDHG_DEVICE.
+// mixed | fp64 | fp32, NIR_PDHG_TOL, NIR_PDHG_MAX_ITERS, NIR_PDHG_DEVICE,
+// NIR_PDHG_KEEP_SCALING=1 (solve the scaled model as given).
 // There is no CPU fallback: an engine error is thrown as
 // std::runtime_error, which the C API turns into its -1 + last_error.
 #pragma once
@@ -42,6 +47,7 @@
 #include "../core/types.hpp"
 #include "../model/model.hpp"
 #include "nir_pdhg.h"
+#include "nir_sov_glue.hpp"
 
 namespace sov {
 
@@ -72,6 +78,43 @@ public:
         lp.rowup = model.rowup.data();
         lp.obj_offset = model.obj_offset;
 
+        // Undo the scales of the scale_model call that produced this model
+        // (Solver scales, then calls here), exactly: they are powers of two.
+        // The engine preconditions by itself, and the relative KKT, the row
+        // margin and Solver's check then all refer to the same space.
+        // NIR_PDHG_KEEP_SCALING=1 solves the model as given.
+        const nir::sov_glue::LastScaling& sc = nir::sov_glue::last_scaling();
+        const bool undo = sc.active && sc.R.size() == size_t(model.nrow) && sc.C.size() == size_t(model.ncol) &&
+                          env_int("NIR_PDHG_KEEP_SCALING", 0) == 0;
+        std::vector<double> uc, ulo, uup, uval, url, uru;
+        if (undo) {
+            uc.resize(size_t(model.ncol));
+            ulo.resize(size_t(model.ncol));
+            uup.resize(size_t(model.ncol));
+            uval.resize(size_t(lp.nnz));
+            for (Idx j = 0; j < model.ncol; ++j) {
+                const double cj = sc.C[size_t(j)];
+                uc[size_t(j)] = model.cost[size_t(j)] / cj;
+                ulo[size_t(j)] = is_finite_bound(model.collo[size_t(j)]) ? model.collo[size_t(j)] * cj : model.collo[size_t(j)];
+                uup[size_t(j)] = is_finite_bound(model.colup[size_t(j)]) ? model.colup[size_t(j)] * cj : model.colup[size_t(j)];
+                for (Off k = model.A.start[size_t(j)]; k < model.A.start[size_t(j) + 1]; ++k)
+                    uval[size_t(k)] = model.A.value[size_t(k)] / sc.R[size_t(model.A.index[size_t(k)])] / cj;
+            }
+            url.resize(size_t(model.nrow));
+            uru.resize(size_t(model.nrow));
+            for (Idx i = 0; i < model.nrow; ++i) {
+                const double ri = sc.R[size_t(i)];
+                url[size_t(i)] = is_finite_bound(model.rowlo[size_t(i)]) ? model.rowlo[size_t(i)] / ri : model.rowlo[size_t(i)];
+                uru[size_t(i)] = is_finite_bound(model.rowup[size_t(i)]) ? model.rowup[size_t(i)] / ri : model.rowup[size_t(i)];
+            }
+            lp.cost = uc.data();
+            lp.collo = ulo.data();
+            lp.colup = uup.data();
+            lp.value = uval.data();
+            lp.rowlo = url.data();
+            lp.rowup = uru.data();
+        }
+
         nir_pdhg_params p;
         nir_pdhg_default_params(&p);
         const long long ref_cap = std::max<long long>(5000, static_cast<long long>(opt.simplex_iter_limit) / 10);
@@ -97,6 +140,10 @@ public:
         if (st == NIR_STATUS_ITERATION_LIMIT && p.feas_tol > 0.0 && info.rel_kkt <= p.tol)
             res.status = Status::Optimal;
         res.iterations = static_cast<Idx>(std::min<int64_t>(info.iterations, 2147483647));
+        if (undo) {  // back to the variables of the model given: x / C, y / R
+            for (Idx j = 0; j < model.ncol; ++j) res.x[size_t(j)] /= sc.C[size_t(j)];
+            for (Idx i = 0; i < model.nrow; ++i) res.y[size_t(i)] /= sc.R[size_t(i)];
+        }
         res.objective = model.eval_objective(res.x);
         return res;
     }

@@ -7,7 +7,8 @@
 // before PDHG (include/sov/solver.hpp:180-181).  The equilibration runs in
 // libnir_facade.so (nir_scale, include/nir_facade.h) on all host threads
 // or NIR_FACADE_THREADS.  Its scales and scaled arrays are the reference's,
-// bit for bit.
+// bit for bit.  The scales are also recorded (include/nir_sov_glue.hpp) for
+// the drop-in PdhgSolver, which undoes them before the GPU engine runs.
 #pragma once
 #include <algorithm>
 #include <cmath>
@@ -18,6 +19,7 @@
 
 #include "model.hpp"
 #include "nir_facade.h"
+#include "nir_sov_glue.hpp"
 
 namespace sov {
 
@@ -65,6 +67,8 @@ inline Model scale_model(const Model& orig, bool enable_scaling, ScalingInfo& in
     info.R.assign(size_t(orig.nrow), 1.0);
     info.C.assign(size_t(orig.ncol), 1.0);
     info.active = false;
+    nir::sov_glue::LastScaling& last = nir::sov_glue::last_scaling();  // read by the drop-in PdhgSolver
+    last.active = false;
     if (!enable_scaling || orig.A.nnz() == 0) return orig;
     nir_lp_view v;
     v.nrow = orig.nrow;
@@ -92,6 +96,9 @@ inline Model scale_model(const Model& orig, bool enable_scaling, ScalingInfo& in
                              scaled.rowup.data(), qnnz > 0 ? scaled.Q.value.data() : nullptr);
     if (st != 0) throw std::runtime_error(std::string("scale_model: ") + nir_facade_last_error());
     info.active = active != 0;
+    last.active = info.active;
+    last.R = info.R;
+    last.C = info.C;
     return scaled;
 }
 

@@ -284,3 +284,32 @@ def test_dropin_cli_presolve_heavy_models_match(tmp_path, seed):
     ref, ours = _cli_pair(tmp_path, path, ["--method", "dual"])
     assert ours == ref
     assert "Presolve:" in ours[1] or "infeasible" in ours[1] or "unbounded" in ours[1]
+
+
+def test_dropin_pdhg_undoes_scale_model_exactly(tmp_path):
+    """The drop-in PdhgSolver hands the engine the model before scale_model
+    (bit for bit) and maps the returned point back exactly; checked with a
+    stand-in for the engine entry point (tests/native/
+    pdhg_dropin_scaling_harness.cpp), so no GPU is needed."""
+    if not os.path.isdir(os.path.join(REF_DIR, "include", "sov")):
+        pytest.skip("the reference sources are absent")
+    tree = tmp_path / "tree"
+    for sub in ("include", "src"):
+        for dirpath, _, files in os.walk(os.path.join(REF_DIR, sub)):
+            rel = os.path.relpath(dirpath, REF_DIR)
+            os.makedirs(tree / rel, exist_ok=True)
+            for f in files:
+                if f.endswith((".hpp", ".h")):
+                    os.symlink(os.path.join(dirpath, f), tree / rel / f)
+    sov = os.path.join(ROOT, "nirnaya_b200", "sov")
+    for name, where in (("pdhg_solver.hpp", "src/gpu"), ("scaling.hpp", "src/model"), ("presolve.hpp", "src/presolve"),
+                        ("mps_reader.hpp", "src/io"), ("sol_io.hpp", "src/io")):
+        os.remove(tree / where / name)
+        os.symlink(os.path.join(sov, name), tree / where / name)
+    exe = tmp_path / "harness"
+    subprocess.run(["g++", "-std=c++17", "-O2", "-fno-fast-math", f"-I{tree}", f"-I{os.path.join(ROOT, 'include')}",
+                    os.path.join(ROOT, "tests", "native", "pdhg_dropin_scaling_harness.cpp"), "-o", str(exe),
+                    f"-L{os.path.join(ROOT, 'nirnaya_b200')}", "-lnir_mps", "-lnir_facade",
+                    f"-Wl,-rpath,{os.path.join(ROOT, 'nirnaya_b200')}", "-lpthread"], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr
