@@ -313,3 +313,36 @@ def test_dropin_pdhg_undoes_scale_model_exactly(tmp_path):
                     f"-Wl,-rpath,{os.path.join(ROOT, 'nirnaya_b200')}", "-lpthread"], check=True)
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not has_gpu(), reason="needs a CUDA device")
+@pytest.mark.parametrize("presolve,scale", [("0", "0"), ("2", "1")])
+def test_c_api_pdhg_scaling_and_presolve_equivalence(presolve, scale):
+    """tests/unit_tests.cpp:177-203's badly scaled LP (coefficients over three
+    decades, a fixed column, a singleton row) with method=pdhg, with and
+    without presolve and scaling: the same optimum, 29.5 (x = (6500, 4, 3)),
+    and a passing double-double check.  With scaling on, the drop-in undoes
+    scale_model's scales before the engine and maps the point back."""
+    lib = _sov(_need("libsov.so"))
+    lib.sov_get_status.restype = C.c_int
+    env = lib.sov_env_create()
+    m = lib.sov_model_create(env, b"Badly_Scaled_LP")
+    for k, v in (("log_level", "0"), ("method", "pdhg"), ("presolve", presolve), ("scale", scale)):
+        lib.sov_set_option_string(m, k.encode(), v.encode())
+    for cost, lo, up in ((1e-3, 0.0, 1e4), (2.0, 0.0, 100.0), (5.0, 3.0, 3.0)):
+        lib.sov_add_col(m, cost, lo, up, 0, None)
+    for lo, cols, vals in ((10.0, [0, 1], [1e-3, 1.0]), (20.0, [0, 1, 2], [2e-3, 1.0, 1.0]), (4.0, [1], [1.0])):
+        idx = (C.c_int * len(cols))(*cols)
+        val = (C.c_double * len(vals))(*vals)
+        lib.sov_add_row(m, lo, 1e20, len(cols), idx, val, None)
+    try:
+        assert lib.sov_optimize(m) == 0, lib.sov_error_message(m)
+        assert lib.sov_get_status(m) == 0
+        assert abs(lib.sov_get_obj(m) - 29.5) <= 1e-5 * 29.5
+        x = (C.c_double * 3)()
+        lib.sov_get_x(m, x)
+        assert abs(x[0] - 6500.0) <= 1e-2 and abs(x[1] - 4.0) <= 1e-5 and x[2] == 3.0
+    finally:
+        lib.sov_model_free(m)
+        lib.sov_env_free(env)
