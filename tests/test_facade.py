@@ -59,12 +59,18 @@ def rich_instance(seed, m=400, n=900, int_frac=0.3, density=4):
             vals.append(v)
     vt = (rng.random(n) < int_frac).astype(np.int8)
     collo = np.where(rng.random(n) < 0.85, np.round(rng.uniform(-2, 1, n)), -INF)
-    colup = np.where(rng.random(n) < 0.85, collo + np.round(rng.uniform(0, 4, n)), INF)
+    width = np.round(rng.uniform(0, 4, n))
+    colup = np.where(rng.random(n) < 0.85, np.where(np.isfinite(collo), collo + width, width - 1.0), INF)
     fixed = rng.random(n) < 0.08
     colup[fixed & np.isfinite(collo)] = collo[fixed & np.isfinite(collo)]
     colup = np.where(np.isfinite(collo), np.maximum(colup, collo), colup)
     cost = np.round(rng.normal(size=n), 2)
     cost[rng.random(n) < 0.1] = 0.0
+    # mostly bounded below: no cost pushes a column toward an infinite bound
+    # (a few keep it, so the unbounded stop of R2 is still reached)
+    keep = rng.random(n) < 0.03
+    cost = np.where(~keep & ~np.isfinite(collo) & (cost > 0), -cost, cost)
+    cost = np.where(~keep & ~np.isfinite(colup) & (cost < 0), 0.0, cost)
     # row bounds around the activity of a point inside the column bounds
     x0 = np.clip(rng.uniform(-1, 2, n), np.where(np.isfinite(collo), collo, -5),
                  np.where(np.isfinite(colup), colup, 5))
