@@ -86,22 +86,26 @@ def rich_instance(seed, m=400, n=900, int_frac=0.3, density=4):
 
 def forcing_instance(seed):
     """Rows whose activity bound equals a row bound (R14 at min and max),
-    redundant rows, and integer rows that tighten bounds (R7)."""
+    redundant rows, and integer rows that tighten bounds (R7).  Each row
+    has columns of its own, so the model stays feasible and presolve runs
+    to the reduced model; the columns no row uses are empty (R2)."""
     rng = np.random.default_rng([0xF0C, seed])
-    n, m = 60, 30
+    n, m = 130, 30
     rows, cols, vals = [], [], []
     rowlo, rowup = np.full(m, -INF), np.full(m, INF)
     collo, colup = np.zeros(n), np.full(n, 4.0)
     vt = (rng.random(n) < 0.5).astype(np.int8)
+    fresh = list(rng.permutation(n))  # each row gets columns of its own
     for i in range(m):
-        js = rng.choice(n, size=int(rng.integers(2, 6)), replace=False)
+        r = i % 5
+        k = int(rng.integers(2, 5))
+        js = np.array([fresh.pop() for _ in range(k)])
         a = rng.choice([1.0, 2.0, -1.0, 0.5], size=js.size)
         rows += [i] * js.size
         cols += js.tolist()
         vals += a.tolist()
         mn = float(np.sum(np.where(a > 0, a * collo[js], a * colup[js])))
         mx = float(np.sum(np.where(a > 0, a * colup[js], a * collo[js])))
-        r = i % 5
         if r == 0:
             rowup[i] = mn            # forcing at the minimum
         elif r == 1:
