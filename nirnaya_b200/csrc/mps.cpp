@@ -118,8 +118,8 @@ std::string number_error(const Tok& t) {
 }
 
 struct Triplets {
-    std::vector<int32_t> row, col;
-    std::vector<double> val;
+    uvector<int32_t> row, col;
+    uvector<double> val;
     size_t size() const { return val.size(); }
     void push(int32_t r, int32_t c, double v) {
         row.push_back(r);
@@ -142,11 +142,11 @@ struct nir_mps {
     std::vector<double> cost, collo, colup, rowlo, rowup;
     std::vector<int8_t> vartype;
     std::vector<int64_t> start{0};
-    std::vector<int32_t> index;
-    std::vector<double> value;
+    nir::text::uvector<int32_t> index;
+    nir::text::uvector<double> value;
     std::vector<int64_t> qstart{0};
-    std::vector<int32_t> qindex;
-    std::vector<double> qvalue;
+    nir::text::uvector<int32_t> qindex;
+    nir::text::uvector<double> qvalue;
     std::string name = "mps_model";
     std::vector<char> col_chars, row_chars;  // names, packed
     std::vector<int64_t> col_off{0}, row_off{0};
@@ -159,7 +159,7 @@ namespace {
 // column sorted by row and duplicates summed; sums that come to zero are
 // dropped.  The sort is stable here.
 void from_triplets(int32_t nrow, int32_t ncol, const Triplets& t, std::vector<int64_t>& start,
-                   std::vector<int32_t>& index, std::vector<double>& value, int threads) {
+                   uvector<int32_t>& index, uvector<double>& value, int threads) {
     const size_t T = t.size();
     auto keep = [&](size_t k) {
         return t.row[k] >= 0 && t.row[k] < nrow && t.col[k] >= 0 && t.col[k] < ncol && t.val[k] != 0.0;
@@ -193,8 +193,8 @@ void from_triplets(int32_t nrow, int32_t ncol, const Triplets& t, std::vector<in
             }
         });
     }
-    std::vector<int32_t> ri(size_t(cnt[ncol]));
-    std::vector<double> rv(size_t(cnt[ncol]));
+    uvector<int32_t> ri(size_t(cnt[ncol]));
+    uvector<double> rv(size_t(cnt[ncol]));
     run_threads(ns, [&](int k) {
         std::vector<int64_t>& w = pos[size_t(k)];
         for (size_t q = T * size_t(k) / size_t(ns); q < T * size_t(k + 1) / size_t(ns); ++q)
@@ -602,7 +602,7 @@ struct Reader {
                     in_int = ev == -2;
                     continue;
                 }
-                if (size_t(ev) + 8 < G) __builtin_prefetch(cols.slot_for(r.groups[size_t(ev) + 8].hash));
+                if (size_t(ev) + 32 < G) __builtin_prefetch(cols.slot_for(r.groups[size_t(ev) + 32].hash));
                 ColGroup& g = r.groups[size_t(ev)];
                 if (last && last->n == g.n &&
                     (g.n <= 16 ? std::memcmp(last->key, g.key, g.n) : std::memcmp(last->p, g.p, g.n)) == 0) {

@@ -9,11 +9,37 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
+#include <memory>
 #include <thread>
+#include <utility>
 #include <vector>
 
 namespace nir {
 namespace text {
+
+// An allocator whose resize leaves new elements uninitialised (default-
+// initialised), for large buffers that are about to be written anyway: the
+// pages are then first touched by the threads that fill them.
+template <class T>
+struct NoInit : std::allocator<T> {
+    template <class U>
+    struct rebind {
+        using other = NoInit<U>;
+    };
+    NoInit() = default;
+    template <class U>
+    NoInit(const NoInit<U>&) noexcept {}
+    template <class U>
+    void construct(U* p) noexcept {
+        ::new (static_cast<void*>(p)) U;
+    }
+    template <class U, class... A>
+    void construct(U* p, A&&... a) {
+        ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
+    }
+};
+template <class T>
+using uvector = std::vector<T, NoInit<T>>;
 
 // isspace in the C locale, which is what istream's >> splits on
 inline bool is_space(char c) { return c == ' ' || c == '\t' || c == '\n' || c == '\v' || c == '\f' || c == '\r'; }
