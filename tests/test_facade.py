@@ -279,3 +279,21 @@ def test_facade_rejects_inconsistent_input():
         facade.presolve(bad)
     with pytest.raises(RuntimeError, match="status 12"):
         facade.scale(bad)
+
+
+@pytest.mark.parametrize("case", ["empty", "cols_only", "rows_only", "rows_only_infeasible"])
+def test_degenerate_models_match(case):
+    """Models with no rows, no columns or neither, through presolve and
+    scaling, as the reference treats them (solved in presolve, or the
+    infeasible empty row)."""
+    z64, z32, z = np.zeros(1, np.int64), np.zeros(0, np.int32), np.zeros(0)
+    lp = {
+        "empty": L.LP(0, 0, z64, z32, z, z, z, z, z, z),
+        "cols_only": L.LP(0, 3, np.zeros(4, np.int64), z32, z, np.array([1.0, -1.0, 0.0]),
+                          np.array([0.0, -INF, -1.0]), np.array([2.0, 5.0, 3.0]), z, z),
+        "rows_only": L.LP(2, 0, z64, z32, z, z, z, z, np.array([-1.0, 0.0]), np.array([1.0, 0.0])),
+        "rows_only_infeasible": L.LP(1, 0, z64, z32, z, z, z, z, np.array([1.0]), np.array([2.0])),
+    }[case]
+    a = _check_presolve(lp, None)
+    assert a.solved_in_presolve
+    _check_scale(lp)
