@@ -612,7 +612,7 @@ def host_path_bench(args):
     (include/sov/solver.hpp:135-313): read the MPS file, presolve, scale;
     then, on a solution (the reduced model's bound-clipped midpoint, put
     back by postsolve), verify it in double-double and write the SOL file.
-    This build's libraries (all host threads; each step's best of three
+    This package's libraries (all host threads; each step's best of three
     runs after one warm-up) against the reference's own code (oracle/_ref,
     one thread, as it runs; each step once), with a bit-for-bit comparison of the scaled model handed to
     PDHG and of the verification report.  One JSON line; wall-clock timing
