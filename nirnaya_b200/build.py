@@ -99,7 +99,8 @@ def build_mps(force: bool = False, verbose: bool = False) -> str:
 
 def build_facade(force: bool = False, verbose: bool = False) -> str:
     target = os.path.join(HERE, "libnir_facade.so")
-    srcs = [os.path.join(CSRC, "facade.cpp"), os.path.join(INC, "nir_facade.h"), os.path.join(INC, "nir_lp.h")]
+    srcs = [os.path.join(CSRC, "facade.cpp"), os.path.join(CSRC, "text.hpp"), os.path.join(INC, "nir_facade.h"),
+            os.path.join(INC, "nir_lp.h")]
     if force or _stale(target, srcs):
         cxx = os.environ.get("CXX", "g++")
         # no FMA contraction: the reference's x86-64 build has none

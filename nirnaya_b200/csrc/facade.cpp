@@ -31,8 +31,11 @@
 #include <vector>
 
 #include "nir_facade.h"
+#include "text.hpp"
 
 namespace {
+
+using nir::text::uvector;  // buffers that are written in full right after they are sized
 
 thread_local std::string g_err;
 
@@ -69,8 +72,8 @@ int hw_threads(int t) { return t > 0 ? t : int(std::max(1u, std::thread::hardwar
 // parallel over column ranges; each range writes after the ranges before it.
 struct Csr {
     std::vector<int64_t> start;
-    std::vector<int32_t> index;
-    std::vector<double> value;
+    uvector<int32_t> index;
+    uvector<double> value;
 };
 
 Csr csr_of(int32_t m, int32_t n, const int64_t* cs, const int32_t* ci, const double* cv, int threads) {
@@ -134,8 +137,9 @@ struct nir_presolved {
     int32_t nrow = 0, ncol = 0;
     double obj_offset = 0.0;
     std::vector<int64_t> start{0};
-    std::vector<int32_t> index;
-    std::vector<double> value, cost, collo, colup, rowlo, rowup;
+    nir::text::uvector<int32_t> index;
+    nir::text::uvector<double> value;
+    std::vector<double> cost, collo, colup, rowlo, rowup;
     std::vector<int8_t> vartype;
     std::vector<int32_t> col_map, row_map;
     std::vector<double> fixed_x;
@@ -543,8 +547,8 @@ struct Presolve {
             }
         });
         for (int32_t c = 0; c < N; ++c) cnt[size_t(c) + 1] += cnt[size_t(c)];
-        std::vector<int32_t> ri(size_t(cnt[size_t(N)]));
-        std::vector<double> rv(size_t(cnt[size_t(N)]));
+        uvector<int32_t> ri(size_t(cnt[size_t(N)]));
+        uvector<double> rv(size_t(cnt[size_t(N)]));
         std::vector<int64_t> kept(size_t(N), 0);
         parallel_ranges(N, threads, 1 << 12, [&](int64_t a, int64_t b) {
             std::vector<std::pair<int32_t, double>> buf;
