@@ -346,3 +346,29 @@ def test_c_api_pdhg_scaling_and_presolve_equivalence(presolve, scale):
     finally:
         lib.sov_model_free(m)
         lib.sov_env_free(env)
+
+
+@pytest.mark.parametrize("objective_line", ["# objective 42.5", "# objective abc", "# objective 1e400"])
+def test_dropin_checker_on_odd_sol_files_matches_the_reference(tmp_path, objective_line):
+    """tools/checker.cpp on the drop-in SOL reader against the reference's:
+    the same report on a file of odd value tokens, and the same failure
+    when std::stod rejects the objective (the exception leaves main)."""
+    if not os.path.exists(REF_CHECKER):
+        pytest.skip("the reference checker (oracle/_ref/checker) is absent")
+    from test_sol import SOL_LINES
+
+    from nirnaya_b200 import lp as L
+    from nirnaya_b200 import mps
+
+    lp = L.generate(1, 0, m=5, n=30)
+    lp.cost[lp.cost == 0.0] = 1.0
+    model, sol = str(tmp_path / "m.mps"), str(tmp_path / "x.sol")
+    mps.write_mps(model, lp, name="solmodel", col_names=[f"C{j}" for j in range(30)])
+    lines = [ln for ln in SOL_LINES if "objective" not in ln] + [objective_line]
+    with open(sol, "w", newline="") as f:
+        f.write("\n".join(lines) + "\n")
+    ours = subprocess.run([_need("checker"), model, sol], capture_output=True, text=True, timeout=120)
+    ref = subprocess.run([REF_CHECKER, model, sol], capture_output=True, text=True, timeout=120)
+    assert (ours.returncode, ours.stdout) == (ref.returncode, ref.stdout)
+    if "abc" in objective_line or "1e400" in objective_line:
+        assert ref.returncode != 0 and ("stod" in ref.stderr) == ("stod" in ours.stderr)
