@@ -32,6 +32,7 @@
 
 #include <stdint.h>
 #include "nir_lp.h"
+#include "nir_sol.h" /* nir_verify_report */
 
 #ifdef __cplusplus
 extern "C" {
@@ -232,6 +233,38 @@ int nir_pdhg_batch_solve(nir_pdhg_batch* b, const nir_pdhg_params* params, int (
                          double* x_out, double* y_out, nir_pdhg_info* infos, nir_pdhg_info* total);
 
 void nir_pdhg_batch_free(nir_pdhg_batch* b);
+
+/* --- the solution check on the device ---
+ *
+ * verify_solution (src/io/sol_io.hpp:25-106) run on the GPU against the LP
+ * the handle holds.  *out receives what nir_verify_solution
+ * (include/nir_sol.h) reports on the host for the same LP, point, integer
+ * marks, claimed objective and tolerance, bit for bit, with no quadratic part
+ * (the PDHG path takes LPs only):
+ *   - row activities are double-double sums in the reference's order,
+ *     one row per thread;
+ *   - the objective is the double-double sum of Model::eval_objective
+ *     (src/model/model.hpp:73-98).
+ * The host check in libnir_mps.so remains the reference for this one.
+ *
+ * x: ncol host doubles.  vartype: ncol bytes (1 integer, 2 binary) or NULL
+ * (all continuous).  claimed_obj: NaN when there is none (obj_rel_err is then
+ * 0).  Returns 0, or NIR_STATUS_INPUT_ERROR / NIR_STATUS_INTERNAL_ERROR with
+ * nir_pdhg_last_error(). */
+int nir_pdhg_verify(nir_pdhg* h, const double* x, const int8_t* vartype, double claimed_obj, double tol,
+                    nir_verify_report* out);
+
+/* The same check for every instance of a batch, in one pass over the
+ * batch's device matrix, replacing `count` host verify_solution calls.
+ *   - x: the instances' points concatenated in instance order (sum of ncol
+ *     doubles), or NULL for the points the last nir_pdhg_batch_solve
+ *     returned, which are still on the device.  x == NULL before any batch
+ *     solve is an input error.
+ *   - vartype: concatenated likewise, or NULL.
+ *   - claimed_obj: count doubles, or NULL (none).
+ *   - out: count reports, in instance order. */
+int nir_pdhg_batch_verify(nir_pdhg_batch* b, const double* x, const int8_t* vartype, const double* claimed_obj,
+                          double tol, nir_verify_report* out);
 
 /* --- no-allocation entry point --- */
 

@@ -23,6 +23,7 @@ import numpy as np
 
 from . import pdhg as P
 from .lp import LP, NirLpView
+from .mps import VerifyReport, report_dict
 
 _bound = False
 
@@ -36,6 +37,8 @@ def _lib():
         L.nir_pdhg_batch_solve.argtypes = [C.c_void_p, C.POINTER(P.Params), P.POLL_FN, C.c_void_p, D, D,
                                            C.POINTER(P.Info), C.POINTER(P.Info)]
         L.nir_pdhg_batch_free.argtypes = [C.c_void_p]
+        L.nir_pdhg_batch_verify.argtypes = [C.c_void_p, D, C.POINTER(C.c_int8), D, C.c_double,
+                                            C.POINTER(VerifyReport)]
         _bound = True
     return L
 
@@ -93,6 +96,38 @@ class BatchEngine:
             c0 += lp.ncol
             r0 += lp.nrow
         return out, total
+
+    def verify(self, xs=None, claimed=None, tol: float = 1e-6, vartypes=None) -> list[dict]:
+        """verify_solution (src/io/sol_io.hpp:25-106) for every instance on
+        the GPU (nir_pdhg_batch_verify): per instance, the report
+        mps.verify_solution gives on the host, bit for bit.  xs: one point
+        per instance, or None for the points the last solve returned (still
+        on the device).  claimed: one objective per instance or None.
+        vartypes: one int8 array per instance or None."""
+        x = None
+        if xs is not None:
+            if len(xs) != len(self.lps):
+                raise ValueError(f"{len(xs)} points for {len(self.lps)} instances")
+            for xi, lp in zip(xs, self.lps):
+                if np.shape(xi) != (lp.ncol,):
+                    raise ValueError("a point's length differs from its instance's column count")
+            x = np.ascontiguousarray(np.concatenate([np.asarray(xi, np.float64) for xi in xs]) if self.n else
+                                     np.zeros(0))
+        vt = None
+        if vartypes is not None:
+            vt = np.ascontiguousarray(np.concatenate([np.asarray(v, np.int8) for v in vartypes]), np.int8)
+            if vt.size != self.n:
+                raise ValueError("vartypes do not match the instances' column counts")
+        cl = None if claimed is None else np.ascontiguousarray(claimed, np.float64)
+        if cl is not None and cl.size != len(self.lps):
+            raise ValueError(f"{cl.size} claimed objectives for {len(self.lps)} instances")
+        reps = (VerifyReport * len(self.lps))()
+        rc = _lib().nir_pdhg_batch_verify(self._h, None if x is None else P._dptr(x),
+                                          None if vt is None else vt.ctypes.data_as(C.POINTER(C.c_int8)),
+                                          None if cl is None else P._dptr(cl), float(tol), reps)
+        if rc != 0:
+            raise RuntimeError(f"nir_pdhg_batch_verify failed ({P.STATUS_NAMES.get(rc, rc)}): {P.last_error()}")
+        return [report_dict(r) for r in reps]
 
 
 def shard_instances(work, world: int) -> list[list[int]]:

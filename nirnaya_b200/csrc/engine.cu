@@ -30,6 +30,7 @@
 #include "k_persistent.cuh"
 #include "k_reference.cuh"
 #include "k_setup.cuh"
+#include "k_verify.cuh"
 #include "k_batch.cuh"
 #include "nir_pdhg.h"
 
@@ -180,6 +181,16 @@ struct nir_pdhg {
     unsigned* gs_gen = nullptr;
     int* gs_err = nullptr;
     int launches = 0;
+    // the device solution check's buffers, allocated by its first call
+    struct Verify {
+        bool ready = false;
+        double *x = nullptr, *rv = nullptr, *obj = nullptr, *claimed = nullptr, *offset = nullptr;
+        int8_t *vt = nullptr, *rs = nullptr;
+        long long* fb = nullptr;
+        void *b = nullptr, *g = nullptr;  // nir::vfy::Rec[count] each
+        nir_verify_report* rep = nullptr;
+        int *row_off = nullptr, *col_off = nullptr;  // one instance: {0, m}, {0, n}
+    } vfy;
 
     // zero-filled allocation with `pad` spare elements past the end (the
     // row-block copies read 16-byte windows that may reach past the end)
@@ -1782,3 +1793,4 @@ extern "C" int nir_pdhg_reference_solve_noalloc(const nir_csr_dev* A, const nir_
 }
 
 #include "engine_batch.cuh"
+#include "engine_verify.cuh"

@@ -32,6 +32,7 @@ struct nir_pdhg_batch {
     nir::DevState* insts = nullptr;
     double *d_bnorm = nullptr, *d_cnorm = nullptr, *d_offset = nullptr, *d_norm = nullptr;
     ChunkGraph graphs[2];
+    bool solved = false;  // h->out_x holds the points the last batch solve returned
     ~nir_pdhg_batch() {
         if (h && h->device >= 0) cudaSetDevice(h->device);
         for (auto& g : graphs) {
@@ -221,6 +222,7 @@ int batch_solve_impl(nir_pdhg_batch* B, const nir_pdhg_params& p, int (*poll)(vo
     cudaStream_t s = h->stream;
     const double t0 = now_sec();
     const int n = h->n, m = h->m, I = B->count;
+    B->solved = false;  // out_x serves as scratch until the final unscale
     if (p.algorithm != NIR_ALGO_PDLP) throw std::invalid_argument("the batch runs NIR_ALGO_PDLP only");
     if (p.spmv_block_nnz > nir::kWarpCapMax) throw std::invalid_argument("spmv_block_nnz must be in [1, 256]");
     if (p.check_every < 1 || p.reflection < 0.0 || p.reflection > 1.0 || !(p.tol >= 0.0))
@@ -376,6 +378,7 @@ int batch_solve_impl(nir_pdhg_batch* B, const nir_pdhg_params& p, int (*poll)(vo
     std::vector<double> x(n), y(m);
     d2h(h, x.data(), h->out_x, n * sizeof(double));
     d2h(h, y.data(), h->out_y, m * sizeof(double));
+    B->solved = true;
     if (x_out) std::memcpy(x_out, x.data(), n * sizeof(double));
     if (y_out) std::memcpy(y_out, y.data(), m * sizeof(double));
     const double t_end = now_sec();

@@ -287,6 +287,13 @@ def verify_solution(lp: LP, x, claimed_obj: float, tol: float = 1e-6, vartype=No
     lib().nir_verify_solution(C.byref(lp.view()), None if vt is None else vt.ctypes.data_as(C.POINTER(C.c_int8)),
                               *qa, xv.ctypes.data_as(C.POINTER(C.c_double)), len(xv), float(claimed_obj),
                               float(tol), int(threads), C.byref(rep))
+    return report_dict(rep, col_names, row_names)
+
+
+def report_dict(rep: VerifyReport, col_names=None, row_names=None) -> dict:
+    """A nir_verify_report as the reference's VerificationReport fields
+    (src/io/sol_io.hpp:14-22), worst_item spelled as the reference spells it
+    (column or row index in place of a name when names are not given)."""
     item = WORST_ITEM[rep.worst_kind]
     if rep.worst_kind >= 2:
         names = row_names if rep.worst_kind >= 6 else col_names

@@ -26,6 +26,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from .lp import LP, NirLpView
+from .mps import VerifyReport, report_dict
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libnir_pdhg.so")
@@ -87,6 +88,7 @@ EXPORTED = [
     "nir_pdhg_solve_lp", "nir_pdhg_free", "nir_pdhg_last_error", "nir_pdhg_spmv", "nir_pdhg_time_spmv",
     "nir_pdhg_set_profiling", "nir_pdhg_kernel_times", "nir_pdhg_get_layout", "nir_pdhg_history",
     "nir_pdhg_reference_solve_noalloc", "nir_pdhg_batch_create", "nir_pdhg_batch_solve", "nir_pdhg_batch_free",
+    "nir_pdhg_verify", "nir_pdhg_batch_verify",
 ]
 
 _lib = None
@@ -114,6 +116,8 @@ def lib():
         L.nir_pdhg_kernel_times.argtypes = [C.c_void_p, C.POINTER(KernelTime)]
         L.nir_pdhg_get_layout.argtypes = [C.c_void_p, C.POINTER(Layout)]
         L.nir_pdhg_history.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.c_int]
+        L.nir_pdhg_verify.argtypes = [C.c_void_p, D, C.POINTER(C.c_int8), C.c_double, C.c_double,
+                                      C.POINTER(VerifyReport)]
         _lib = L
     return _lib
 
@@ -225,6 +229,22 @@ class Engine:
         if cnt < 0:
             raise RuntimeError(last_error())
         return buf[:cnt].copy()
+
+    def verify(self, x, claimed_obj: float = float("nan"), tol: float = 1e-6, vartype=None, col_names=None,
+               row_names=None) -> dict:
+        """verify_solution (src/io/sol_io.hpp:25-106) on the GPU against
+        this handle's LP (nir_pdhg_verify): the report mps.verify_solution
+        gives on the host, bit for bit."""
+        xv = np.ascontiguousarray(x, np.float64)
+        if xv.shape != (self.lp.ncol,):
+            raise ValueError(f"x has {xv.size} values for {self.lp.ncol} columns")
+        vt = None if vartype is None else np.ascontiguousarray(vartype, np.int8)
+        rep = VerifyReport()
+        rc = lib().nir_pdhg_verify(self._h, _dptr(xv), None if vt is None else vt.ctypes.data_as(C.POINTER(C.c_int8)),
+                                   float(claimed_obj), float(tol), C.byref(rep))
+        if rc != 0:
+            raise RuntimeError(f"nir_pdhg_verify failed ({STATUS_NAMES.get(rc, rc)}): {last_error()}")
+        return report_dict(rep, col_names, row_names)
 
     def layout(self) -> Layout:
         lo = Layout()
