@@ -704,6 +704,93 @@ def host_path_bench(args):
                       "speedup_vs_reference": (ref["total"] / total) if ref else None}))
 
 
+def verify_batch_bench(args):
+    """C3's 256 solution checks (verify_solution, src/io/sol_io.hpp:25-106)
+    on the device (nir_pdhg_batch_verify), against this package's host check
+    and the reference's.  Two device figures:
+      - in place: the points a short batch solve left on the device, so the
+        call is the three kernels plus 2 KB of claimed objectives in and the
+        reports out;
+      - from the host: seeded points near each instance's construction point,
+        copied in by the call (the end-to-end figure).
+    Every device report is compared with the host check's, bit for bit."""
+    import numpy as np
+
+    from nirnaya_b200 import batch as B
+    from nirnaya_b200 import mps, pdhg
+
+    wl = WORKLOADS["c3"]
+    lps = batch_instances(wl)
+    rng = np.random.default_rng(7)
+    xs = [lp.x0 + 1e-7 * rng.normal(size=lp.ncol) for lp in lps]
+    claimed = np.array([float(np.dot(lp.cost, x)) + lp.obj_offset for lp, x in zip(lps, xs)])
+    tol = 1e-6
+    t0 = time.perf_counter()
+    host = [mps.verify_solution(lp, x, float(c), tol) for lp, x, c in zip(lps, xs, claimed)]
+    t_host = time.perf_counter() - t0
+    t_ref = None
+    try:
+        from oracle import ffi
+
+        t0 = time.perf_counter()
+        for lp, x, c in zip(lps, xs, claimed):
+            ffi.ref_verify_full(lp, x, float(c), tol)
+        t_ref = time.perf_counter() - t0
+    except Exception as e:  # the reference library is built only where its sources are
+        print(f"reference check not timed: {e}", file=sys.stderr)
+
+    def same(a, b):
+        return all(np.float64(a[k]).view(np.uint64) == np.float64(b[k]).view(np.uint64)
+                   if isinstance(a[k], float) else a[k] == b[k] for k in a)
+
+    with B.BatchEngine(lps, 0) as eng:
+        for _ in range(args.warmup):
+            dev = eng.verify(xs, claimed, tol)
+        e2e = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            dev = eng.verify(xs, claimed, tol)
+            e2e.append(time.perf_counter() - t0)
+        from_host_ok = all(same(d, h) for d, h in zip(dev, host))
+        res, _ = eng.solve(pdhg.default_params(max_iters=64, tol=0.0))
+        solved_claimed = np.array([r[2].objective for r in res])
+        for _ in range(args.warmup):
+            eng.verify(None, solved_claimed, tol)
+        with ClockSampler(0) as clk:
+            resident = []
+            for _ in range(args.steps):
+                t0 = time.perf_counter()
+                inplace = eng.verify(None, solved_claimed, tol)
+                resident.append(time.perf_counter() - t0)
+        in_place_ok = all(same(d, mps.verify_solution(lp, r[0], float(c), tol))
+                          for d, lp, r, c in zip(inplace, lps, res, solved_claimed))
+    nnz = sum(lp.nnz for lp in lps)
+    m = sum(lp.nrow for lp in lps)
+    n = sum(lp.ncol for lp in lps)
+    alg = 12.0 * nnz + 38.0 * m + 40.0 * n
+    t_dev = statistics.median(resident)
+    peak, peak_kind = peaks()
+    achieved = alg / t_dev / 1e9
+    print(json.dumps({
+        "metric": "C3 solution check: verify_solution for 256 instances",
+        "value": t_dev, "unit": "s", "higher_is_better": False, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "dtype": "f64 (double-double sums)", "data": "synthetic (seeded generator)",
+        "config": {"workload": wl["label"], "instances": len(lps), "nnz": nnz, "rows": m, "cols": n, "tol": tol,
+                   "points": "in place: a 64-iteration batch solve's; from the host: x0 + 1e-7 N(0,1)",
+                   "timing": "host clock around the synchronous call (median)"},
+        "e2e": {"value": statistics.median(e2e), "unit": "s", "h2d_bytes_per_step": 8 * n + 8 * len(lps),
+                "d2h_bytes_per_step": 48 * len(lps)},
+        "host_check_s": t_host, "reference_check_s": t_ref,
+        "reports_bit_identical": {"from_host": from_host_ok, "in_place": in_place_ok},
+        "gpu_launches": 3 * args.steps,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "kernel": "k_vfy_cols + k_vfy_rows + k_vfy_report, 12 B/nnz + 38 B/row "
+                                                "+ 40 B/column over the call time",
+                     "peak_kind": peak_kind},
+        "clocks": clk.summary(),
+    }), flush=True)
+
+
 def reference_iterations(args):
     """Counts the reference PDHG's iterations to 1e-6 relative KKT on the
     workload: the bit-identical GPU restatement of its loop
@@ -759,6 +846,8 @@ def main():
                     help="MPS reader throughput on the workload written as an MPS file, then exit")
     ap.add_argument("--mps-dir", default=os.path.join(ROOT, "_bench_tmp"),
                     help="where --mps-read writes its input file")
+    ap.add_argument("--verify-batch", action="store_true",
+                    help="C3's 256 solution checks on the device against the host check and the reference's")
     ap.add_argument("--host-path", action="store_true",
                     help="the CLI's host steps around PDHG (read, presolve, scale, verify, write_sol) "
                          "against the reference's")
@@ -766,6 +855,9 @@ def main():
     wl = WORKLOADS[args.workload]
     if args.host_path:
         host_path_bench(args)
+        return
+    if args.verify_batch:
+        verify_batch_bench(args)
         return
     if args.mps_read:
         mps_read_bench(args)

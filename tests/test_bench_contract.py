@@ -83,3 +83,14 @@ def test_host_path_mode_line(tmp_path):
     if line["reference"] is not None:
         ref = line["reference"]
         assert ref["scaled_model_bit_identical"] and ref["verification_bit_identical"] and ref["sol_bytes_identical"]
+
+
+def test_verify_batch_mode_is_wired_and_needs_a_gpu():
+    """--verify-batch measures the device check; without a GPU it fails
+    loudly at the engine (no CPU fallback) after the host legs ran."""
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--help"], capture_output=True, text=True,
+                         timeout=120)
+    assert out.returncode == 0 and "--verify-batch" in out.stdout
+    import bench
+
+    assert callable(bench.verify_batch_bench)
