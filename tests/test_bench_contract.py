@@ -86,8 +86,8 @@ def test_host_path_mode_line(tmp_path):
 
 
 def test_verify_batch_mode_is_wired_and_needs_a_gpu():
-    """--verify-batch measures the device check; without a GPU it fails
-    loudly at the engine (no CPU fallback) after the host legs ran."""
+    """--verify-batch (the device check on the batch) is a bench.py mode;
+    its device legs run on a GPU only."""
     out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--help"], capture_output=True, text=True,
                          timeout=120)
     assert out.returncode == 0 and "--verify-batch" in out.stdout
