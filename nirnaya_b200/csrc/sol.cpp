@@ -454,59 +454,40 @@ int nir_verify_solution(const nir_lp_view* lp, const int8_t* vartype, int64_t qn
         *out = rep;
         return 0;
     }
-    // rows in double-double: a CSR of the columns with x != 0 (entries of a
-    // row in ascending column order), built in parallel over column ranges
-    // that each write after the ranges before them; then rows in parallel
+    // rows in double-double: thread k owns a range of rows and scans the
+    // columns with x != 0 in order, adding the entries that fall in its
+    // range.  Every row's terms thus arrive in ascending column order, the
+    // order of the reference's column loop, and each thread's accumulators
+    // stay in its own cache.  One more thread evaluates the objective
+    // meanwhile.
     {
         const int64_t nnz = lp->nnz;
-        const int ns = int(std::max<int64_t>(1, std::min<int64_t>(T, nnz / 65536 + 1)));
-        std::vector<int32_t> jb(static_cast<size_t>(ns) + 1, n);
-        jb[0] = 0;
-        for (int k = 1; k < ns; ++k) {
-            jb[size_t(k)] = int32_t(std::lower_bound(lp->col_start, lp->col_start + n + 1, nnz * k / ns) - lp->col_start);
-            jb[size_t(k)] = std::max(jb[size_t(k) - 1], std::min(jb[size_t(k)], n));
-        }
-        std::vector<std::vector<int64_t>> pos(static_cast<size_t>(ns));
-        run_threads(ns, [&](int k) {
-            auto& c = pos[size_t(k)];
-            c.assign(size_t(m), 0);
-            for (int32_t j = jb[size_t(k)]; j < jb[size_t(k) + 1]; ++j)
-                if (x[j] != 0.0)
-                    for (int64_t q = lp->col_start[j]; q < lp->col_start[j + 1]; ++q) ++c[size_t(lp->row_index[q])];
-        });
-        std::vector<int64_t> rs(size_t(m) + 1, 0);
-        for (int32_t i = 0; i < m; ++i) {
-            int64_t o = rs[size_t(i)];
-            for (int k = 0; k < ns; ++k) {
-                const int64_t c = pos[size_t(k)][size_t(i)];
-                pos[size_t(k)][size_t(i)] = o;
-                o += c;
+        const int nr = int(std::max<int64_t>(1, std::min<int64_t>(T, 1 + nnz / 131072)));
+        std::vector<Rec> rows(static_cast<size_t>(nr));
+        double obj = 0.0;
+        run_threads(nr + 1, [&](int k) {
+            if (k == nr) {
+                obj = nir_eval_objective(lp, qnnz, q_start, q_index, q_value, x);
+                return;
             }
-            rs[size_t(i) + 1] = o;
-        }
-        std::vector<int32_t> rc(size_t(rs[size_t(m)]));
-        std::vector<double> rv(size_t(rs[size_t(m)]));
-        run_threads(ns, [&](int k) {
-            auto& w = pos[size_t(k)];
-            for (int32_t j = jb[size_t(k)]; j < jb[size_t(k) + 1]; ++j) {
-                if (x[j] == 0.0) continue;
+            const int32_t lo = int32_t(int64_t(m) * k / nr), hi = int32_t(int64_t(m) * (k + 1) / nr);
+            const uint32_t span = uint32_t(hi - lo);
+            if (span == 0) return;
+            std::vector<DD> acc(span);
+            for (int32_t j = 0; j < n; ++j) {
+                const double xj = x[j];
+                if (xj == 0.0) continue;
                 for (int64_t q = lp->col_start[j]; q < lp->col_start[j + 1]; ++q) {
-                    const int64_t p = w[size_t(lp->row_index[q])]++;
-                    rc[size_t(p)] = j;
-                    rv[size_t(p)] = lp->value[q];
+                    const uint32_t i = uint32_t(lp->row_index[q] - lo);  // rows below lo wrap past span
+                    if (i < span) add_prod(acc[i], lp->value[q], xj);
                 }
             }
-        });
-        const int nr = int(std::max<int64_t>(1, std::min<int64_t>(T, m / 8192 + 1)));
-        std::vector<Rec> rows(static_cast<size_t>(nr));
-        run_threads(nr, [&](int k) {
             Rec r;
-            for (int64_t i = int64_t(m) * k / nr; i < int64_t(m) * (k + 1) / nr; ++i) {
-                DD act;
-                for (int64_t q = rs[size_t(i)]; q < rs[size_t(i) + 1]; ++q) add_prod(act, rv[size_t(q)], x[rc[size_t(q)]]);
-                const double a = act.hi + act.lo;
-                if (fin(lp->rowlo[i])) r.see(std::max(0.0, lp->rowlo[i] - a) / (1.0 + std::abs(lp->rowlo[i])), 2 * i, 6);
-                if (fin(lp->rowup[i])) r.see(std::max(0.0, a - lp->rowup[i]) / (1.0 + std::abs(lp->rowup[i])), 2 * i + 1, 7);
+            for (uint32_t i = 0; i < span; ++i) {
+                const int64_t g = int64_t(lo) + i;
+                const double a = acc[i].hi + acc[i].lo;
+                if (fin(lp->rowlo[g])) r.see(std::max(0.0, lp->rowlo[g] - a) / (1.0 + std::abs(lp->rowlo[g])), 2 * g, 6);
+                if (fin(lp->rowup[g])) r.see(std::max(0.0, a - lp->rowup[g]) / (1.0 + std::abs(lp->rowup[g])), 2 * g + 1, 7);
             }
             rows[size_t(k)] = r;
         });
@@ -517,8 +498,8 @@ int nir_verify_solution(const nir_lp_view* lp, const int8_t* vartype, int64_t qn
             rep.worst_kind = R.kind;
             rep.worst_index = R.pos / 2;
         }
+        rep.computed_obj = obj;
     }
-    rep.computed_obj = nir_eval_objective(lp, qnnz, q_start, q_index, q_value, x);
     if (std::isfinite(claimed_obj))
         rep.obj_rel_err = std::abs(rep.computed_obj - claimed_obj) / (1.0 + std::abs(rep.computed_obj));
     if (rep.max_bound_viol > tol || rep.max_row_viol > tol || rep.max_int_viol > tol || rep.obj_rel_err > 1e-5)

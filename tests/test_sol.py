@@ -185,3 +185,37 @@ def test_eval_objective_matches():
         x = np.random.default_rng(seed).normal(size=lp.ncol)
         ref = ffi.ref_lib().ref_eval_objective(ffi.C.byref(lp.view()), ffi._dptr(x))
         assert _bits(mps.eval_objective(lp, x)) == _bits(ref)
+
+
+def test_verify_splits_rows_into_ranges_on_larger_models():
+    """Above 131,072 nonzeros the row activities are summed in row ranges,
+    one per thread, each scanning the columns in order: the same report as
+    the reference at every thread count, ties across ranges included."""
+    ffi = _ffi()
+    rng = np.random.default_rng(11)
+    lp = L.generate(2, 4, m=20000, n=50000, target_nnz=600000)
+    assert lp.nnz > 4 * 131072
+    vt = (rng.random(lp.ncol) < 0.1).astype(np.int8)
+    for trial in range(3):
+        x = np.clip(rng.normal(size=lp.ncol) * 3, lp.collo, lp.colup) if trial else rng.normal(size=lp.ncol)
+        x[rng.random(lp.ncol) < 0.3] = 0.0
+        for tol in (1e-9, 10.0):
+            b = ffi.ref_verify_full(lp, x, 1.0, tol, vartype=vt)
+            for threads in (1, 3, 8):
+                a = mps.verify_solution(lp, x, 1.0, tol, vartype=vt, col_names=[f"C{j}" for j in range(lp.ncol)],
+                                        row_names=[f"R{i}" for i in range(lp.nrow)], threads=threads)
+                for k in ("max_bound_viol", "max_row_viol", "max_int_viol", "computed_obj", "obj_rel_err"):
+                    assert _bits(a[k]) == _bits(b[k]), (trial, tol, threads, k)
+                assert a["passed"] == b["passed"] and a["worst_item"] == b["worst_item"], (trial, threads)
+    # every row the same violation: the first row is named, whichever range reports it
+    m, per = 60000, 5
+    rows = rng.permutation(np.repeat(np.arange(m), per)).astype(np.int32)
+    n = m * per
+    tie = L.LP(m, n, np.arange(n + 1, dtype=np.int64), rows, np.ones(n), np.zeros(n), np.zeros(n), np.ones(n),
+               np.full(m, 1e6), np.full(m, np.inf), 0.0)
+    x = np.full(n, 0.5)
+    b = ffi.ref_verify_full(tie, x, 0.0, 1e-6)
+    for threads in (1, 2, 8):
+        a = mps.verify_solution(tie, x, 0.0, 1e-6, row_names=[f"R{i}" for i in range(m)], threads=threads)
+        assert a["worst_item"] == b["worst_item"] == "Row lower bound on R0"
+        assert _bits(a["max_row_viol"]) == _bits(b["max_row_viol"])
