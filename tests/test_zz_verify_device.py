@@ -20,7 +20,6 @@ from nirnaya_b200 import mps
 
 INC = os.path.join(ROOT, "include")
 CSRC = os.path.join(ROOT, "nirnaya_b200", "csrc")
-gpu = [pytest.mark.gpu, pytest.mark.skipif(not has_gpu(), reason="needs a CUDA device")]
 
 
 def _same(a: dict, b: dict) -> bool:
