@@ -26,10 +26,17 @@
 //     undone exactly before the engine runs and the solution is mapped
 //     back: the engine preconditions by itself, and power-of-two
 //     equilibration ahead of it slows the restarted PDHG's duality gap;
+//   * optionally, a crossover turns the engine's point into a vertex: a
+//     basis is read off the point and the program's own simplex
+//     (sov::LpSolver) is warm-started from it (nir::dropin::crossover
+//     below).
 // Environment knobs (no Options field is added, so options.hpp stays as
 // it is): NIR_PDHG_ALGO = pdlp | pdhg | reference, NIR_PDHG_PRECISION =
 // mixed | fp64 | fp32, NIR_PDHG_TOL, NIR_PDHG_MAX_ITERS, NIR_PDHG_DEVICE,
-// NIR_PDHG_KEEP_SCALING=1 (solve the scaled model as given).
+// NIR_PDHG_KEEP_SCALING=1 (solve the scaled model as given),
+// NIR_PDHG_CROSSOVER = 1 (after every solve) | auto (when the engine stops
+// short of Optimal), NIR_PDHG_CROSSOVER_TOL (relative distance at which a
+// value sits at its bound, default 1e-6).
 // There is no CPU fallback: an engine error is thrown as
 // std::runtime_error, which the C API turns into its -1 + last_error.
 #pragma once
@@ -45,9 +52,114 @@
 #include "../core/status.hpp"
 #include "../core/timer.hpp"
 #include "../core/types.hpp"
+#include "../lp/lp_solver.hpp"
 #include "../model/model.hpp"
 #include "nir_pdhg.h"
 #include "nir_sov_glue.hpp"
+
+namespace nir {
+namespace dropin {
+
+// The result of a crossover from an approximate LP optimum to a vertex.
+struct CrossoverResult {
+    sov::Status status = sov::Status::NumericalTrouble;
+    std::vector<double> x;           // the vertex (model columns)
+    std::vector<double> y;           // row duals, as LpSolver gives them to Solver
+    sov::Idx simplex_iterations = 0;
+    sov::Idx crash_structurals = 0;  // structural columns in the crash basis
+};
+
+// Where a value v in [lo, up] goes in a crash basis: at the bound it lies
+// within tol of (relative to 1 + |bound|), or basic.  *interior receives
+// the relative distance to the nearer bound of a basic value (kInf when
+// both bounds are infinite) and -1 otherwise.
+inline sov::VarStatus crash_status(double v, double lo, double up, double tol, double* interior) {
+    const bool fl = sov::is_finite_bound(lo), fu = sov::is_finite_bound(up);
+    *interior = -1.0;
+    if (fl && fu && lo == up) return sov::VarStatus::Fixed;
+    const double dl = fl ? (v - lo) / (1.0 + std::abs(lo)) : sov::kInf;
+    const double du = fu ? (up - v) / (1.0 + std::abs(up)) : sov::kInf;
+    if (dl <= tol || du <= tol) return dl <= du ? sov::VarStatus::AtLower : sov::VarStatus::AtUpper;
+    *interior = std::min(dl, du);
+    return sov::VarStatus::Basic;
+}
+
+// Crossover: from (x, y), an approximate optimum of `model`, to an optimal
+// vertex.
+//   1. The crash basis.  Every column and every row logical (whose value is
+//      the row activity) strictly inside its bounds is a basic candidate;
+//      the others sit at the bound they touch.
+//   2. Exactly nrow basics are needed.
+//      - When there are more candidates, those nearest a bound are moved
+//        to it.
+//      - When there are fewer, the logicals of the rows at a bound with the
+//        smallest |y| (the weakest binding rows) fill the basis.
+//   3. The program's own simplex (sov::LpSolver, src/lp/lp_solver.hpp) is
+//      warm-started from that basis (set_basis, :896-907) and solves to
+//      optimality.  Its factorisation swaps logicals in for dependent
+//      columns (:183-212).
+// Near an optimum most of the basis is already right, so few pivots are
+// left to make.
+inline CrossoverResult crossover(const sov::Model& model, const std::vector<double>& x, const std::vector<double>& y,
+                                 const sov::Options& opt, const sov::Deadline& deadline, double tol) {
+    using sov::Idx;
+    using sov::VarStatus;
+    const Idx n = model.ncol, m = model.nrow;
+    std::vector<double> act(size_t(m), 0.0);
+    for (Idx j = 0; j < n; ++j)
+        for (sov::Off k = model.A.start[size_t(j)]; k < model.A.start[size_t(j) + 1]; ++k)
+            act[size_t(model.A.index[size_t(k)])] += model.A.value[size_t(k)] * x[size_t(j)];
+    std::vector<VarStatus> st(size_t(n + m));
+    std::vector<std::pair<double, Idx>> cand;  // (relative distance to the nearer bound, variable)
+    for (Idx v = 0; v < n + m; ++v) {
+        const bool col = v < n;
+        const size_t i = size_t(col ? v : v - n);
+        double d;
+        st[size_t(v)] = col ? crash_status(x[i], model.collo[i], model.colup[i], tol, &d)
+                            : crash_status(act[i], model.rowlo[i], model.rowup[i], tol, &d);
+        if (st[size_t(v)] == VarStatus::Basic) cand.push_back({d, v});
+    }
+    std::stable_sort(cand.begin(), cand.end(),
+                     [](const std::pair<double, Idx>& a, const std::pair<double, Idx>& b) { return a.first > b.first; });
+    for (size_t k = size_t(m); k < cand.size(); ++k) {  // too many: the least interior go to a bound
+        const Idx v = cand[k].second;
+        const bool col = v < n;
+        const size_t i = size_t(col ? v : v - n);
+        const double val = col ? x[i] : act[i];
+        const double lo = col ? model.collo[i] : model.rowlo[i], up = col ? model.colup[i] : model.rowup[i];
+        const bool fl = sov::is_finite_bound(lo), fu = sov::is_finite_bound(up);
+        if (!fl && !fu) st[size_t(v)] = VarStatus::FreeZero;
+        else if (fl && (!fu || val - lo <= up - val)) st[size_t(v)] = VarStatus::AtLower;
+        else st[size_t(v)] = VarStatus::AtUpper;
+    }
+    if (cand.size() < size_t(m)) {  // too few: logicals of the weakest binding rows
+        std::vector<std::pair<double, Idx>> fill;
+        for (Idx i = 0; i < m; ++i)
+            if (st[size_t(n + i)] != VarStatus::Basic) fill.push_back({std::abs(y[size_t(i)]), n + i});
+        std::stable_sort(fill.begin(), fill.end(),
+                         [](const std::pair<double, Idx>& a, const std::pair<double, Idx>& b) { return a.first < b.first; });
+        for (size_t k = 0; k < size_t(m) - cand.size(); ++k) st[size_t(fill[k].second)] = VarStatus::Basic;
+    }
+    sov::BasisSnapshot snap;
+    snap.status = st;
+    CrossoverResult r;
+    for (Idx v = 0; v < n + m; ++v)
+        if (st[size_t(v)] == VarStatus::Basic) {
+            snap.basic_index.push_back(v);
+            if (v < n) ++r.crash_structurals;
+        }
+    sov::LpSolver lp(opt);
+    lp.load(model);
+    lp.set_basis(snap);
+    r.status = lp.solve(deadline);
+    r.simplex_iterations = lp.stats.iterations;
+    r.x.assign(lp.value.begin(), lp.value.begin() + n);
+    r.y = lp.row_duals;
+    return r;
+}
+
+}  // namespace dropin
+}  // namespace nir
 
 namespace sov {
 
@@ -143,6 +255,26 @@ public:
         if (undo) {  // back to the variables of the model given: x / C, y / R
             for (Idx j = 0; j < model.ncol; ++j) res.x[size_t(j)] /= sc.C[size_t(j)];
             for (Idx i = 0; i < model.nrow; ++i) res.y[size_t(i)] /= sc.R[size_t(i)];
+        }
+        // Crossover to a vertex of the model given, when asked for.  Its
+        // result replaces the engine's only when the simplex proves it
+        // optimal; its pivots count as iterations.
+        const char* xo = std::getenv("NIR_PDHG_CROSSOVER");
+        const std::string mode = xo ? xo : "";
+        bool finite = true;
+        for (double v : res.x) finite = finite && std::isfinite(v);
+        for (double v : res.y) finite = finite && std::isfinite(v);
+        if ((mode == "1" || (mode == "auto" && res.status != Status::Optimal)) && model.nrow > 0 && finite &&
+            res.status != Status::TimeLimit && !deadline.expired()) {
+            const char* t = std::getenv("NIR_PDHG_CROSSOVER_TOL");
+            const nir::dropin::CrossoverResult c =
+                nir::dropin::crossover(model, res.x, res.y, opt, deadline, t && *t ? std::atof(t) : 1e-6);
+            if (c.status == Status::Optimal) {
+                res.x = c.x;
+                res.y = c.y;
+                res.status = Status::Optimal;
+            }
+            res.iterations += c.simplex_iterations;
         }
         res.objective = model.eval_objective(res.x);
         return res;

@@ -148,6 +148,30 @@ def test_cli_method_pdhg_on_crude_blending(tmp_path, args):
     assert "PASS=YES" in r.stdout
 
 
+@pytest.mark.gpu
+@pytest.mark.skipif(not has_gpu(), reason="needs a CUDA device")
+def test_cli_crossover_returns_the_vertex_on_crude_blending(tmp_path):
+    """NIR_PDHG_CROSSOVER=1: after PDLP, the crash basis and the program's
+    own simplex give the published optimum (.sol:2) to 1e-9 relative, where
+    PDHG alone is within 1e-6."""
+    g = GOLD["crude_blending"]
+    lib = _sov(_need("libsov.so"))
+    env = lib.sov_env_create()
+    m = lib.sov_model_create(env, b"MRPL_Crude_Blending_LP")
+    _build_model(lib, m, G.lp_from(g["lp_internal_min"]), g["sense"])
+    path = str(tmp_path / "crude.mps")
+    assert lib.sov_write_mps(m, path.encode()) == 0
+    lib.sov_model_free(m)
+    lib.sov_env_free(env)
+    sol = str(tmp_path / "crude.sol")
+    r = subprocess.run([_need("sovsolve"), path, "--method", "pdhg", "--sol", sol], capture_output=True, text=True,
+                       timeout=600, env=dict(os.environ, NIR_PDHG_CROSSOVER="1"))
+    assert r.returncode == 0 and "PASS=YES" in r.stdout, r.stdout + r.stderr
+    with open(sol) as f:
+        obj = float(next(ln for ln in f if ln.startswith("# objective")).split()[2])
+    assert abs(obj - g["sol_objective"]) <= 1e-9 * abs(g["sol_objective"]), (obj, g["sol_objective"])
+
+
 # ---- the MPS reader drop-in (nirnaya_b200/sov/mps_reader.hpp): CPU only
 
 REF_DIR = os.environ.get("NIRNAYA_REF", "/root/reference")
@@ -286,11 +310,10 @@ def test_dropin_cli_presolve_heavy_models_match(tmp_path, seed):
     assert "Presolve:" in ours[1] or "infeasible" in ours[1] or "unbounded" in ours[1]
 
 
-def test_dropin_pdhg_undoes_scale_model_exactly(tmp_path):
-    """The drop-in PdhgSolver hands the engine the model before scale_model
-    (bit for bit) and maps the returned point back exactly; checked with a
-    stand-in for the engine entry point (tests/native/
-    pdhg_dropin_scaling_harness.cpp), so no GPU is needed."""
+def _harness(tmp_path, source):
+    """Builds tests/native/<source> against a tree of the reference's headers
+    with the five drop-in headers linked in; the engine entry point is the
+    harness's own stand-in, so no GPU is needed."""
     if not os.path.isdir(os.path.join(REF_DIR, "include", "sov")):
         pytest.skip("the reference sources are absent")
     tree = tmp_path / "tree"
@@ -308,11 +331,37 @@ def test_dropin_pdhg_undoes_scale_model_exactly(tmp_path):
         os.symlink(os.path.join(sov, name), tree / where / name)
     exe = tmp_path / "harness"
     subprocess.run(["g++", "-std=c++17", "-O2", "-fno-fast-math", f"-I{tree}", f"-I{os.path.join(ROOT, 'include')}",
-                    os.path.join(ROOT, "tests", "native", "pdhg_dropin_scaling_harness.cpp"), "-o", str(exe),
+                    os.path.join(ROOT, "tests", "native", source), "-o", str(exe),
                     f"-L{os.path.join(ROOT, 'nirnaya_b200')}", "-lnir_mps", "-lnir_facade",
                     f"-Wl,-rpath,{os.path.join(ROOT, 'nirnaya_b200')}", "-lpthread"], check=True)
-    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    return subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
+
+
+def test_dropin_pdhg_undoes_scale_model_exactly(tmp_path):
+    """The drop-in PdhgSolver hands the engine the model before scale_model
+    (bit for bit) and maps the returned point back exactly; checked with a
+    stand-in for the engine entry point (tests/native/
+    pdhg_dropin_scaling_harness.cpp), so no GPU is needed."""
+    r = _harness(tmp_path, "pdhg_dropin_scaling_harness.cpp")
     assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr
+
+
+def test_dropin_crossover_reaches_the_simplex_optimum(tmp_path):
+    """NIR_PDHG_CROSSOVER: from an approximate optimum (the simplex's,
+    perturbed by 1e-8 and by 1e-6 relative), the drop-in's crossover reaches
+    the simplex's optimal objective with a passing dd check.  Checked on the
+    reference's worked example (x = (3, 1), duals (1.5, 0.5)), its PDHG and
+    transport LPs and seeded random LPs.  It runs through Solver with
+    presolve and scaling on and off, and `auto` runs only after an engine
+    result short of Optimal (tests/native/pdhg_dropin_crossover_harness.cpp)."""
+    r = _harness(tmp_path, "pdhg_dropin_crossover_harness.cpp")
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout + r.stderr
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("random_")]
+    assert len(lines) == 4
+    for ln in lines:  # near an optimum the crash basis leaves (almost) nothing to pivot
+        scratch = int(ln.split("simplex from slacks ")[1].split()[0])
+        pivots = int(ln.split("crossover ")[1].split()[0])
+        assert pivots <= scratch // 10, ln
 
 
 @pytest.mark.gpu
