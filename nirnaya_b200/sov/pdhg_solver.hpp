@@ -69,32 +69,18 @@ struct CrossoverResult {
     sov::Idx crash_structurals = 0;  // structural columns in the crash basis
 };
 
-// Where a value v in [lo, up] goes in a crash basis: at the bound it lies
-// within tol of (relative to 1 + |bound|), or basic.  *interior receives
-// the relative distance to the nearer bound of a basic value (kInf when
-// both bounds are infinite) and -1 otherwise.
-inline sov::VarStatus crash_status(double v, double lo, double up, double tol, double* interior) {
-    const bool fl = sov::is_finite_bound(lo), fu = sov::is_finite_bound(up);
-    *interior = -1.0;
-    if (fl && fu && lo == up) return sov::VarStatus::Fixed;
-    const double dl = fl ? (v - lo) / (1.0 + std::abs(lo)) : sov::kInf;
-    const double du = fu ? (up - v) / (1.0 + std::abs(up)) : sov::kInf;
-    if (dl <= tol || du <= tol) return dl <= du ? sov::VarStatus::AtLower : sov::VarStatus::AtUpper;
-    *interior = std::min(dl, du);
-    return sov::VarStatus::Basic;
-}
-
 // Crossover: from (x, y), an approximate optimum of `model`, to an optimal
 // vertex.
-//   1. The crash basis.  Every column and every row logical (whose value is
-//      the row activity) strictly inside its bounds is a basic candidate;
-//      the others sit at the bound they touch.
-//   2. Exactly nrow basics are needed.
-//      - When there are more candidates, those nearest a bound are moved
-//        to it.
-//      - When there are fewer, the logicals of the rows at a bound with the
-//        smallest |y| (the weakest binding rows) fill the basis.
-//   3. The program's own simplex (sov::LpSolver, src/lp/lp_solver.hpp) is
+//   1. The crash basis, by complementarity.  For every column and every row
+//      logical (whose value is the row activity), two measures:
+//      - p, its relative distance to the nearer bound (0 within tol, inf
+//        when free);
+//      - q, its reduced cost over a common dual scale: c_j - (A'y)_j for a
+//        column, y_i for a row.
+//      A basic variable has p large and q near zero; a nonbasic one the
+//      reverse.  Ranked by p / (p + q), ties by q ascending, the first nrow
+//      are basic.  The others sit at their nearer bound.
+//   2. The program's own simplex (sov::LpSolver, src/lp/lp_solver.hpp) is
 //      warm-started from that basis (set_basis, :896-907) and solves to
 //      optimality.  Its factorisation swaps logicals in for dependent
 //      columns (:183-212).
@@ -105,49 +91,56 @@ inline CrossoverResult crossover(const sov::Model& model, const std::vector<doub
     using sov::Idx;
     using sov::VarStatus;
     const Idx n = model.ncol, m = model.nrow;
-    std::vector<double> act(size_t(m), 0.0);
+    std::vector<double> act(size_t(m), 0.0), d(model.cost.begin(), model.cost.end());
     for (Idx j = 0; j < n; ++j)
-        for (sov::Off k = model.A.start[size_t(j)]; k < model.A.start[size_t(j) + 1]; ++k)
-            act[size_t(model.A.index[size_t(k)])] += model.A.value[size_t(k)] * x[size_t(j)];
+        for (sov::Off k = model.A.start[size_t(j)]; k < model.A.start[size_t(j) + 1]; ++k) {
+            const size_t i = size_t(model.A.index[size_t(k)]);
+            act[i] += model.A.value[size_t(k)] * x[size_t(j)];
+            d[size_t(j)] -= model.A.value[size_t(k)] * y[i];
+        }
+    double dscale = 0.0;
+    for (double c : model.cost) dscale = std::max(dscale, std::abs(c));
+    for (double v : y) dscale = std::max(dscale, std::abs(v));
+    dscale += 1.0;
+    struct Key {
+        double r, q;
+        Idx v;
+    };
+    std::vector<Key> keys;
+    keys.reserve(size_t(n + m));
     std::vector<VarStatus> st(size_t(n + m));
-    std::vector<std::pair<double, Idx>> cand;  // (relative distance to the nearer bound, variable)
     for (Idx v = 0; v < n + m; ++v) {
-        const bool col = v < n;
-        const size_t i = size_t(col ? v : v - n);
-        double d;
-        st[size_t(v)] = col ? crash_status(x[i], model.collo[i], model.colup[i], tol, &d)
-                            : crash_status(act[i], model.rowlo[i], model.rowup[i], tol, &d);
-        if (st[size_t(v)] == VarStatus::Basic) cand.push_back({d, v});
-    }
-    std::stable_sort(cand.begin(), cand.end(),
-                     [](const std::pair<double, Idx>& a, const std::pair<double, Idx>& b) { return a.first > b.first; });
-    for (size_t k = size_t(m); k < cand.size(); ++k) {  // too many: the least interior go to a bound
-        const Idx v = cand[k].second;
         const bool col = v < n;
         const size_t i = size_t(col ? v : v - n);
         const double val = col ? x[i] : act[i];
         const double lo = col ? model.collo[i] : model.rowlo[i], up = col ? model.colup[i] : model.rowup[i];
         const bool fl = sov::is_finite_bound(lo), fu = sov::is_finite_bound(up);
-        if (!fl && !fu) st[size_t(v)] = VarStatus::FreeZero;
-        else if (fl && (!fu || val - lo <= up - val)) st[size_t(v)] = VarStatus::AtLower;
-        else st[size_t(v)] = VarStatus::AtUpper;
+        const double dl = fl ? (val - lo) / (1.0 + std::abs(lo)) : sov::kInf;
+        const double du = fu ? (up - val) / (1.0 + std::abs(up)) : sov::kInf;
+        // the place of a nonbasic variable: the nearer finite bound
+        if (fl && fu && lo == up) st[size_t(v)] = VarStatus::Fixed;
+        else if (!fl && !fu) st[size_t(v)] = VarStatus::FreeZero;
+        else st[size_t(v)] = (fl && dl <= du) ? VarStatus::AtLower : VarStatus::AtUpper;
+        double p = std::min(dl, du);
+        if (p <= tol) p = 0.0;
+        const double q = std::abs(col ? d[i] : y[i]) / dscale;
+        double r;
+        if (st[size_t(v)] == VarStatus::Fixed) r = -1.0;
+        else if (!std::isfinite(p)) r = 1.0;
+        else r = p > 0.0 ? p / (p + q) : 0.0;
+        keys.push_back({r, q, v});
     }
-    if (cand.size() < size_t(m)) {  // too few: logicals of the weakest binding rows
-        std::vector<std::pair<double, Idx>> fill;
-        for (Idx i = 0; i < m; ++i)
-            if (st[size_t(n + i)] != VarStatus::Basic) fill.push_back({std::abs(y[size_t(i)]), n + i});
-        std::stable_sort(fill.begin(), fill.end(),
-                         [](const std::pair<double, Idx>& a, const std::pair<double, Idx>& b) { return a.first < b.first; });
-        for (size_t k = 0; k < size_t(m) - cand.size(); ++k) st[size_t(fill[k].second)] = VarStatus::Basic;
-    }
+    std::stable_sort(keys.begin(), keys.end(), [](const Key& a, const Key& b) {
+        return a.r > b.r || (a.r == b.r && a.q < b.q);
+    });
     sov::BasisSnapshot snap;
-    snap.status = st;
     CrossoverResult r;
-    for (Idx v = 0; v < n + m; ++v)
-        if (st[size_t(v)] == VarStatus::Basic) {
-            snap.basic_index.push_back(v);
-            if (v < n) ++r.crash_structurals;
-        }
+    for (size_t k = 0; k < size_t(m); ++k) {
+        st[size_t(keys[k].v)] = VarStatus::Basic;
+        snap.basic_index.push_back(keys[k].v);
+        if (keys[k].v < n) ++r.crash_structurals;
+    }
+    snap.status = st;
     sov::LpSolver lp(opt);
     lp.load(model);
     lp.set_basis(snap);

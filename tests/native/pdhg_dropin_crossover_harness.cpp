@@ -143,7 +143,10 @@ struct Lcg {  // a small deterministic generator for the test models
     }
 };
 
-static sov::Model random_lp(unsigned seed, int m, int n) {
+// zero_cost: every feasible point is optimal; *x0_out receives the strictly
+// feasible point the rows are built around.
+static sov::Model random_lp(unsigned seed, int m, int n, bool zero_cost = false,
+                            std::vector<double>* x0_out = nullptr) {
     Lcg rng{0x9E3779B97F4A7C15ULL ^ seed};
     sov::ModelBuilder mb("random");
     std::vector<double> x0(static_cast<size_t>(n));
@@ -165,7 +168,7 @@ static sov::Model random_lp(unsigned seed, int m, int n) {
         double c = rng.uniform();
         for (auto& e : cols[size_t(j)]) c += e.second * y0[size_t(e.first)];
         const double up = (j % 4 == 0) ? sov::kInf : 10.0 + 5.0 * rng.uniform();
-        id[size_t(j)] = mb.add_col(c, 0.0, up);
+        id[size_t(j)] = mb.add_col(zero_cost ? 0.0 : c, 0.0, up);
     }
     std::vector<std::vector<sov::Idx>> ri(static_cast<size_t>(m));
     std::vector<std::vector<double>> rv(static_cast<size_t>(m));
@@ -182,6 +185,7 @@ static sov::Model random_lp(unsigned seed, int m, int n) {
             default: mb.add_row(-sov::kInf, a + 0.5, ri[size_t(i)], rv[size_t(i)]); break;
         }
     }
+    if (x0_out) *x0_out = x0;
     return mb.finalize();
 }
 
@@ -261,6 +265,41 @@ int main() {
         if (res.status != sov::Status::Optimal || !res.verification.passed || res.iterations < 7)
             return fail(c.name, "auto did not finish an engine result stopped at its cap");
         unsetenv("NIR_PDHG_CROSSOVER");
+    }
+    // an interior point of the optimal face: with zero costs every feasible
+    // point is optimal, and x0 lies strictly inside its column bounds, so
+    // there are more basic candidates than rows
+    {
+        std::vector<double> x0;
+        const sov::Model z = random_lp(99, 60, 150, true, &x0);
+        const nir::dropin::CrossoverResult r =
+            nir::dropin::crossover(z, x0, std::vector<double>(size_t(z.nrow), 0.0), opt, dl, 1e-6);
+        if (r.status != sov::Status::Optimal || !sov::verify_solution(z, r.x, 0.0, 1e-9).passed)
+            return fail("zero_cost", "crossover from an interior feasible point");
+        int inside = 0;
+        for (sov::Idx j = 0; j < z.ncol; ++j)
+            if (r.x[size_t(j)] > z.collo[size_t(j)] + 1e-9 &&
+                (!sov::is_finite_bound(z.colup[size_t(j)]) || r.x[size_t(j)] < z.colup[size_t(j)] - 1e-9))
+                ++inside;
+        if (inside > z.nrow) return fail("zero_cost", "more columns inside their bounds than rows: not a vertex");
+        std::printf("zero_cost: m=%d n=%d crash basic columns %lld, %lld pivots, %d columns inside their bounds\n",
+                    int(z.nrow), int(z.ncol), (long long)r.crash_structurals, (long long)r.simplex_iterations, inside);
+    }
+    // a point 1e-3 off, as an early stop of the engine leaves it
+    {
+        const sov::Model f = random_lp(21, 80, 200);
+        std::vector<double> xa, ya;
+        approximate_optimum(f, xa, ya, 1e-3);
+        sov::LpSolver ref(opt);
+        ref.load(f);
+        ref.solve(dl);
+        const double obj_ref = f.eval_objective(std::vector<double>(ref.value.begin(), ref.value.begin() + f.ncol));
+        const nir::dropin::CrossoverResult r = nir::dropin::crossover(f, xa, ya, opt, dl, 1e-6);
+        if (r.status != sov::Status::Optimal ||
+            std::abs(f.eval_objective(r.x) - obj_ref) > 1e-9 * (1.0 + std::abs(obj_ref)))
+            return fail("far", "crossover from a point 1e-3 off");
+        std::printf("far: m=%d n=%d from 1e-3 off: %lld pivots (simplex from slacks %lld)\n", int(f.nrow),
+                    int(f.ncol), (long long)r.simplex_iterations, (long long)ref.stats.iterations);
     }
     std::printf("ok\n");
     return 0;

@@ -348,20 +348,24 @@ def test_dropin_pdhg_undoes_scale_model_exactly(tmp_path):
 
 def test_dropin_crossover_reaches_the_simplex_optimum(tmp_path):
     """NIR_PDHG_CROSSOVER: from an approximate optimum (the simplex's,
-    perturbed by 1e-8 and by 1e-6 relative), the drop-in's crossover reaches
-    the simplex's optimal objective with a passing dd check.  Checked on the
+    perturbed by 1e-8, 1e-6 and 1e-3 relative) or an interior point of an
+    optimal face, the drop-in's crossover reaches the simplex's optimal
+    objective with a passing dd check, in a small fraction of the simplex's
+    own pivots.  Checked on the
     reference's worked example (x = (3, 1), duals (1.5, 0.5)), its PDHG and
     transport LPs and seeded random LPs.  It runs through Solver with
     presolve and scaling on and off, and `auto` runs only after an engine
     result short of Optimal (tests/native/pdhg_dropin_crossover_harness.cpp)."""
     r = _harness(tmp_path, "pdhg_dropin_crossover_harness.cpp")
     assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout + r.stderr
-    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("random_")]
-    assert len(lines) == 4
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith(("random_", "transport"))]
+    assert len(lines) == 5
     for ln in lines:  # near an optimum the crash basis leaves (almost) nothing to pivot
         scratch = int(ln.split("simplex from slacks ")[1].split()[0])
-        pivots = int(ln.split("crossover ")[1].split()[0])
-        assert pivots <= scratch // 10, ln
+        pivots = [int(ln.split("crossover ")[1].split()[0]), int(ln.split("), ")[1].split()[0])]
+        assert max(pivots) <= scratch // 8, ln
+    far = next(ln for ln in r.stdout.splitlines() if ln.startswith("far:"))
+    assert int(far.split("off: ")[1].split()[0]) <= int(far.split("from slacks ")[1].rstrip(")")) // 8, far
 
 
 @pytest.mark.gpu
