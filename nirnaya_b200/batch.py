@@ -111,8 +111,7 @@ class BatchEngine:
             for xi, lp in zip(xs, self.lps):
                 if np.shape(xi) != (lp.ncol,):
                     raise ValueError("a point's length differs from its instance's column count")
-            x = np.ascontiguousarray(np.concatenate([np.asarray(xi, np.float64) for xi in xs]) if self.n else
-                                     np.zeros(0))
+            x = np.ascontiguousarray(np.concatenate([np.asarray(xi, np.float64) for xi in xs]))
         vt = None
         if vartypes is not None:
             vt = np.ascontiguousarray(np.concatenate([np.asarray(v, np.int8) for v in vartypes]), np.int8)
