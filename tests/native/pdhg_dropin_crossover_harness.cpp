@@ -18,7 +18,9 @@
 //      check.  On the worked example it gives x = (3, 1) and the simplex's
 //      duals (1.5, 0.5);
 //   4. NIR_PDHG_CROSSOVER=auto runs only when the engine stopped short of
-//      Optimal, and then turns its IterationLimit into Optimal.
+//      Optimal, and then turns its IterationLimit into Optimal;
+//   5. from real PDHG iterates (the reference loop run to 1e-6 relative KKT
+//      by the oracle), crossover reaches the simplex's optimum.
 // Prints one line per model, then "ok" and exits 0.  Otherwise it names the
 // first failed check and exits 1.
 #include <cmath>
@@ -28,6 +30,7 @@
 #include <vector>
 
 #include "include/sov/solver.hpp"
+#include "nir_oracle.h"  // the reference PDHG loop restated in C, for a real PDHG iterate
 
 namespace {
 
@@ -300,6 +303,38 @@ int main() {
             return fail("far", "crossover from a point 1e-3 off");
         std::printf("far: m=%d n=%d from 1e-3 off: %lld pivots (simplex from slacks %lld)\n", int(f.nrow),
                     int(f.ncol), (long long)r.simplex_iterations, (long long)ref.stats.iterations);
+    }
+    // real PDHG iterates: the reference loop (oracle) to 1e-6 relative KKT
+    for (unsigned seed = 0; seed < 3; ++seed) {
+        const sov::Model f = random_lp(31 + seed, 30 + 10 * int(seed), 80 + 20 * int(seed));
+        nir_lp_view v;
+        std::memset(&v, 0, sizeof(v));
+        v.nrow = f.nrow;
+        v.ncol = f.ncol;
+        v.nnz = f.A.nnz();
+        v.col_start = f.A.start.data();
+        v.row_index = f.A.index.data();
+        v.value = f.A.value.data();
+        v.cost = f.cost.data();
+        v.collo = f.collo.data();
+        v.colup = f.colup.data();
+        v.rowlo = f.rowlo.data();
+        v.rowup = f.rowup.data();
+        std::vector<double> xp(size_t(f.ncol)), yp(size_t(f.nrow));
+        or_pdhg_out po;
+        or_ref_pdhg(&v, 3000000, 64, 1e-6, 1, xp.data(), yp.data(), &po);
+        sov::LpSolver ref(opt);
+        ref.load(f);
+        ref.solve(dl);
+        const double obj_ref = f.eval_objective(std::vector<double>(ref.value.begin(), ref.value.begin() + f.ncol));
+        const nir::dropin::CrossoverResult r = nir::dropin::crossover(f, xp, yp, opt, dl, 1e-6);
+        if (r.status != sov::Status::Optimal ||
+            std::abs(f.eval_objective(r.x) - obj_ref) > 1e-9 * (1.0 + std::abs(obj_ref)))
+            return fail("pdhg_iterate", "crossover from a PDHG iterate");
+        std::printf("pdhg_iterate_%u: m=%d n=%d PDHG %lld iterations (rel KKT %.1e), crossover %lld pivots "
+                    "(simplex from slacks %lld)\n",
+                    seed, int(f.nrow), int(f.ncol), (long long)po.iterations, po.last_kkt,
+                    (long long)r.simplex_iterations, (long long)ref.stats.iterations);
     }
     std::printf("ok\n");
     return 0;

@@ -310,7 +310,7 @@ def test_dropin_cli_presolve_heavy_models_match(tmp_path, seed):
     assert "Presolve:" in ours[1] or "infeasible" in ours[1] or "unbounded" in ours[1]
 
 
-def _harness(tmp_path, source):
+def _harness(tmp_path, source, oracle=False):
     """Builds tests/native/<source> against a tree of the reference's headers
     with the five drop-in headers linked in; the engine entry point is the
     harness's own stand-in, so no GPU is needed."""
@@ -330,10 +330,12 @@ def _harness(tmp_path, source):
         os.remove(tree / where / name)
         os.symlink(os.path.join(sov, name), tree / where / name)
     exe = tmp_path / "harness"
+    orc = os.path.join(ROOT, "oracle")
+    extra = [f"-I{orc}", f"-L{orc}", "-loracle", f"-Wl,-rpath,{orc}"] if oracle else []
     subprocess.run(["g++", "-std=c++17", "-O2", "-fno-fast-math", f"-I{tree}", f"-I{os.path.join(ROOT, 'include')}",
                     os.path.join(ROOT, "tests", "native", source), "-o", str(exe),
                     f"-L{os.path.join(ROOT, 'nirnaya_b200')}", "-lnir_mps", "-lnir_facade",
-                    f"-Wl,-rpath,{os.path.join(ROOT, 'nirnaya_b200')}", "-lpthread"], check=True)
+                    f"-Wl,-rpath,{os.path.join(ROOT, 'nirnaya_b200')}", *extra, "-lpthread"], check=True)
     return subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
 
 
@@ -348,15 +350,16 @@ def test_dropin_pdhg_undoes_scale_model_exactly(tmp_path):
 
 def test_dropin_crossover_reaches_the_simplex_optimum(tmp_path):
     """NIR_PDHG_CROSSOVER: from an approximate optimum (the simplex's,
-    perturbed by 1e-8, 1e-6 and 1e-3 relative) or an interior point of an
-    optimal face, the drop-in's crossover reaches the simplex's optimal
+    perturbed by 1e-8, 1e-6 and 1e-3 relative), a real PDHG iterate (the
+    reference loop in the oracle) or an interior point of an optimal face,
+    the drop-in's crossover reaches the simplex's optimal
     objective with a passing dd check, in a small fraction of the simplex's
     own pivots.  Checked on the
     reference's worked example (x = (3, 1), duals (1.5, 0.5)), its PDHG and
     transport LPs and seeded random LPs.  It runs through Solver with
     presolve and scaling on and off, and `auto` runs only after an engine
     result short of Optimal (tests/native/pdhg_dropin_crossover_harness.cpp)."""
-    r = _harness(tmp_path, "pdhg_dropin_crossover_harness.cpp")
+    r = _harness(tmp_path, "pdhg_dropin_crossover_harness.cpp", oracle=True)
     assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout + r.stderr
     lines = [ln for ln in r.stdout.splitlines() if ln.startswith(("random_", "transport"))]
     assert len(lines) == 5
@@ -366,6 +369,12 @@ def test_dropin_crossover_reaches_the_simplex_optimum(tmp_path):
         assert max(pivots) <= scratch // 8, ln
     far = next(ln for ln in r.stdout.splitlines() if ln.startswith("far:"))
     assert int(far.split("off: ")[1].split()[0]) <= int(far.split("from slacks ")[1].rstrip(")")) // 8, far
+    # from real PDHG iterates (the reference loop, restated in the oracle)
+    its = [ln for ln in r.stdout.splitlines() if ln.startswith("pdhg_iterate_")]
+    assert len(its) == 3
+    for ln in its:
+        pivots = int(ln.split("crossover ")[1].split()[0])
+        assert pivots <= int(ln.split("from slacks ")[1].rstrip(")")) // 8, ln
 
 
 @pytest.mark.gpu
