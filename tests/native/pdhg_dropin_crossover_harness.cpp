@@ -23,6 +23,11 @@
 //      by the oracle), crossover reaches the simplex's optimum.
 // Prints one line per model, then "ok" and exits 0.  Otherwise it names the
 // first failed check and exits 1.
+//
+// With the argument "c1" it measures instead, on the C1 model
+// (random_eq_2000x5000, seed 1): the reference loop (oracle) to its own stop,
+// then crossover, against the simplex from its slack basis (300 s limit).
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -30,6 +35,7 @@
 #include <vector>
 
 #include "include/sov/solver.hpp"
+#include "nir_lpgen.h"   // the seeded generator of the benchmark models
 #include "nir_oracle.h"  // the reference PDHG loop restated in C, for a real PDHG iterate
 
 namespace {
@@ -192,7 +198,62 @@ static sov::Model random_lp(unsigned seed, int m, int n, bool zero_cost = false,
     return mb.finalize();
 }
 
-int main() {
+static double seconds_since(const std::chrono::steady_clock::time_point& t0) {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+static sov::Model model_of(const nir_lp_view& v) { return model_from(&v); }
+
+static int measure_c1() {
+    nir_lpgen* g = nullptr;
+    nir_lpgen_opts o;
+    std::memset(&o, 0, sizeof(o));
+    if (nir_lpgen_create(NIR_GEN_RANDOM_EQ, 1, &o, &g) != 0) return fail("c1", "generator");
+    nir_lp_view v;
+    nir_lpgen_view(g, &v);
+    const sov::Model f = model_of(v);
+    sov::Options opt;
+    opt.log_level = 0;
+    sov::Deadline dl;
+    // the reference loop to its own stop; the cap is the reference's
+    // max(5000, simplex_iter_limit / 10)
+    const long long cap = std::max<long long>(5000, static_cast<long long>(opt.simplex_iter_limit) / 10);
+    std::vector<double> xp(size_t(f.ncol)), yp(size_t(f.nrow));
+    or_pdhg_out po;
+    auto t0 = std::chrono::steady_clock::now();
+    or_ref_pdhg(&v, cap, 0, 0.0, 0, xp.data(), yp.data(), &po);
+    const double t_pdhg = seconds_since(t0);
+    or_kkt kk;
+    or_rel_kkt(&v, xp.data(), yp.data(), &kk);
+    t0 = std::chrono::steady_clock::now();
+    const nir::dropin::CrossoverResult r = nir::dropin::crossover(f, xp, yp, opt, dl, 1e-6);
+    const double t_x = seconds_since(t0);
+    const double obj = f.eval_objective(r.x);
+    const bool ok = r.status == sov::Status::Optimal && sov::verify_solution(f, r.x, obj, 1e-9).passed;
+    std::printf("c1: m=%d n=%d nnz=%lld\n", int(f.nrow), int(f.ncol), (long long)f.A.nnz());
+    std::printf("reference PDHG loop (oracle, 1 thread): %lld iterations, %.2f s, rel KKT %.2e, objective %.12g\n",
+                (long long)po.iterations, t_pdhg, kk.rel_kkt, f.eval_objective(xp));
+    std::printf("crossover: status %d, %lld pivots, %.2f s, objective %.12g, dd check at 1e-9 %s\n", int(r.status),
+                (long long)r.simplex_iterations, t_x, obj, ok ? "PASS" : "FAIL");
+    sov::Deadline limit;
+    limit.wall_limit_sec = 300.0;
+    sov::LpSolver lp(opt);
+    lp.load(f);
+    t0 = std::chrono::steady_clock::now();
+    const sov::Status st = lp.solve(limit);
+    std::printf("simplex from slacks: status %d, %lld iterations, %.2f s%s\n", int(st), (long long)lp.stats.iterations,
+                seconds_since(t0), st == sov::Status::Optimal ? "" : " (stopped)");
+    if (st == sov::Status::Optimal) {
+        const double o2 = f.eval_objective(std::vector<double>(lp.value.begin(), lp.value.begin() + f.ncol));
+        std::printf("simplex objective %.12g, crossover relative difference %.1e\n", o2,
+                    std::abs(obj - o2) / (1.0 + std::abs(o2)));
+    }
+    nir_lpgen_free(g);
+    return ok ? 0 : 1;
+}
+
+int main(int argc, char** argv) {
+    if (argc > 1 && std::strcmp(argv[1], "c1") == 0) return measure_c1();
     struct Case {
         const char* name;
         sov::Model m;

@@ -331,7 +331,7 @@ def _harness(tmp_path, source, oracle=False):
         os.symlink(os.path.join(sov, name), tree / where / name)
     exe = tmp_path / "harness"
     orc = os.path.join(ROOT, "oracle")
-    extra = [f"-I{orc}", f"-L{orc}", "-loracle", f"-Wl,-rpath,{orc}"] if oracle else []
+    extra = [f"-I{orc}", f"-L{orc}", "-loracle", "-lnir_lpgen", f"-Wl,-rpath,{orc}"] if oracle else []
     subprocess.run(["g++", "-std=c++17", "-O2", "-fno-fast-math", f"-I{tree}", f"-I{os.path.join(ROOT, 'include')}",
                     os.path.join(ROOT, "tests", "native", source), "-o", str(exe),
                     f"-L{os.path.join(ROOT, 'nirnaya_b200')}", "-lnir_mps", "-lnir_facade",
