@@ -36,7 +36,8 @@
 // NIR_PDHG_KEEP_SCALING=1 (solve the scaled model as given),
 // NIR_PDHG_CROSSOVER = 1 (after every solve) | auto (when the engine stops
 // short of Optimal), NIR_PDHG_CROSSOVER_TOL (relative distance at which a
-// value sits at its bound, default 1e-6).
+// value sits at its bound, default 1e-6), NIR_PDHG_CROSSOVER_METHOD =
+// primal (default) | dual (the simplex that finishes the crossover).
 // There is no CPU fallback: an engine error is thrown as
 // std::runtime_error, which the C API turns into its -1 + last_error.
 #pragma once
@@ -82,12 +83,13 @@ struct CrossoverResult {
 //      are basic.  The others sit at their nearer bound.
 //   2. The program's own simplex (sov::LpSolver, src/lp/lp_solver.hpp) is
 //      warm-started from that basis (set_basis, :896-907) and solves to
-//      optimality.  Its factorisation swaps logicals in for dependent
-//      columns (:183-212).
+//      optimality, by default with its primal simplex (:576).  Its
+//      factorisation swaps logicals in for dependent columns (:183-212).
 // Near an optimum most of the basis is already right, so few pivots are
 // left to make.
 inline CrossoverResult crossover(const sov::Model& model, const std::vector<double>& x, const std::vector<double>& y,
-                                 const sov::Options& opt, const sov::Deadline& deadline, double tol) {
+                                 const sov::Options& opt, const sov::Deadline& deadline, double tol,
+                                 const char* method = "primal") {
     using sov::Idx;
     using sov::VarStatus;
     const Idx n = model.ncol, m = model.nrow;
@@ -141,7 +143,13 @@ inline CrossoverResult crossover(const sov::Model& model, const std::vector<doub
         if (keys[k].v < n) ++r.crash_structurals;
     }
     snap.status = st;
-    sov::LpSolver lp(opt);
+    sov::Options lo = opt;
+    // "primal" (the default): LpSolver's primal simplex, which starts from
+    // the crash basis's nearly feasible point.  Otherwise its dual path,
+    // whose artificial-bounds phase 1 can wander off a basis with small
+    // dual infeasibilities.
+    if (method && *method) lo.method = method;
+    sov::LpSolver lp(lo);
     lp.load(model);
     lp.set_basis(snap);
     r.status = lp.solve(deadline);
@@ -260,8 +268,9 @@ public:
         if ((mode == "1" || (mode == "auto" && res.status != Status::Optimal)) && model.nrow > 0 && finite &&
             res.status != Status::TimeLimit && !deadline.expired()) {
             const char* t = std::getenv("NIR_PDHG_CROSSOVER_TOL");
-            const nir::dropin::CrossoverResult c =
-                nir::dropin::crossover(model, res.x, res.y, opt, deadline, t && *t ? std::atof(t) : 1e-6);
+            const char* how = std::getenv("NIR_PDHG_CROSSOVER_METHOD");
+            const nir::dropin::CrossoverResult c = nir::dropin::crossover(
+                model, res.x, res.y, opt, deadline, t && *t ? std::atof(t) : 1e-6, how && *how ? how : "primal");
             if (c.status == Status::Optimal) {
                 res.x = c.x;
                 res.y = c.y;

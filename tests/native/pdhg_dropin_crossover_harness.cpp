@@ -24,9 +24,11 @@
 // Prints one line per model, then "ok" and exits 0.  Otherwise it names the
 // first failed check and exits 1.
 //
-// With the argument "c1" it measures instead, on the C1 model
-// (random_eq_2000x5000, seed 1): the reference loop (oracle) to its own stop,
-// then crossover, against the simplex from its slack basis (300 s limit).
+// With the argument "c1" (or "measure <kind> <seed> [m]") it measures
+// instead, on the C1 model (random_eq_2000x5000, seed 1) or the generator
+// model named.  It runs the reference loop (oracle) for its own cap and for
+// six times that, crosses over from each point (240 s limit), and times the
+// simplex from its slack basis (300 s limit).
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -204,56 +206,68 @@ static double seconds_since(const std::chrono::steady_clock::time_point& t0) {
 
 static sov::Model model_of(const nir_lp_view& v) { return model_from(&v); }
 
-static int measure_c1() {
+// kind, seed, m: a generator model (include/nir_lpgen.h); m = 0 is the
+// kind's default.
+static int measure(int kind, unsigned long long seed, int m) {
+    std::setvbuf(stdout, nullptr, _IOLBF, 0);  // each line out as it is made
     nir_lpgen* g = nullptr;
     nir_lpgen_opts o;
     std::memset(&o, 0, sizeof(o));
-    if (nir_lpgen_create(NIR_GEN_RANDOM_EQ, 1, &o, &g) != 0) return fail("c1", "generator");
+    o.m = m;
+    if (nir_lpgen_create(kind, seed, &o, &g) != 0) return fail("measure", "generator");
     nir_lp_view v;
     nir_lpgen_view(g, &v);
     const sov::Model f = model_of(v);
     sov::Options opt;
     opt.log_level = 0;
-    sov::Deadline dl;
-    // the reference loop to its own stop; the cap is the reference's
-    // max(5000, simplex_iter_limit / 10)
+    std::printf("kind %d seed %llu: m=%d n=%d nnz=%lld\n", kind, seed, int(f.nrow), int(f.ncol),
+                (long long)f.A.nnz());
+    bool ok = true;
+    // the reference loop run for its own cap, max(5000, simplex_iter_limit / 10),
+    // and for six times as many iterations; then crossover from each point
     const long long cap = std::max<long long>(5000, static_cast<long long>(opt.simplex_iter_limit) / 10);
-    std::vector<double> xp(size_t(f.ncol)), yp(size_t(f.nrow));
-    or_pdhg_out po;
-    auto t0 = std::chrono::steady_clock::now();
-    or_ref_pdhg(&v, cap, 0, 0.0, 0, xp.data(), yp.data(), &po);
-    const double t_pdhg = seconds_since(t0);
-    or_kkt kk;
-    or_rel_kkt(&v, xp.data(), yp.data(), &kk);
-    t0 = std::chrono::steady_clock::now();
-    const nir::dropin::CrossoverResult r = nir::dropin::crossover(f, xp, yp, opt, dl, 1e-6);
-    const double t_x = seconds_since(t0);
-    const double obj = f.eval_objective(r.x);
-    const bool ok = r.status == sov::Status::Optimal && sov::verify_solution(f, r.x, obj, 1e-9).passed;
-    std::printf("c1: m=%d n=%d nnz=%lld\n", int(f.nrow), int(f.ncol), (long long)f.A.nnz());
-    std::printf("reference PDHG loop (oracle, 1 thread): %lld iterations, %.2f s, rel KKT %.2e, objective %.12g\n",
-                (long long)po.iterations, t_pdhg, kk.rel_kkt, f.eval_objective(xp));
-    std::printf("crossover: status %d, %lld pivots, %.2f s, objective %.12g, dd check at 1e-9 %s\n", int(r.status),
-                (long long)r.simplex_iterations, t_x, obj, ok ? "PASS" : "FAIL");
+    for (long long iters : {cap, 6 * cap}) {
+        std::vector<double> xp(size_t(f.ncol)), yp(size_t(f.nrow));
+        or_pdhg_out po;
+        auto t0 = std::chrono::steady_clock::now();
+        or_ref_pdhg(&v, iters, 0, 0.0, 0, xp.data(), yp.data(), &po);
+        const double t_pdhg = seconds_since(t0);
+        or_kkt kk;
+        or_rel_kkt(&v, xp.data(), yp.data(), &kk);
+        std::printf("reference PDHG loop (oracle, 1 thread): %lld iterations, %.2f s, rel KKT %.2e, max rel row "
+                    "violation %.2e\n",
+                    (long long)po.iterations, t_pdhg, kk.rel_kkt, kk.max_rel_row_viol);
+        for (const char* method : {"dual", "primal"}) {
+            sov::Deadline dl;
+            dl.wall_limit_sec = 240.0;
+            t0 = std::chrono::steady_clock::now();
+            const nir::dropin::CrossoverResult r = nir::dropin::crossover(f, xp, yp, opt, dl, 1e-6, method);
+            const double t_x = seconds_since(t0);
+            const double obj = f.eval_objective(r.x);
+            const bool pass = r.status == sov::Status::Optimal && sov::verify_solution(f, r.x, obj, 1e-9).passed;
+            std::printf("  crossover (%s): status %d, %lld pivots, %.2f s, crash basic columns %lld, objective "
+                        "%.12g, dd check at 1e-9 %s\n",
+                        method, int(r.status), (long long)r.simplex_iterations, t_x, (long long)r.crash_structurals,
+                        obj, pass ? "PASS" : "FAIL");
+            ok = ok && pass;
+        }
+    }
     sov::Deadline limit;
     limit.wall_limit_sec = 300.0;
     sov::LpSolver lp(opt);
     lp.load(f);
-    t0 = std::chrono::steady_clock::now();
+    auto t0 = std::chrono::steady_clock::now();
     const sov::Status st = lp.solve(limit);
     std::printf("simplex from slacks: status %d, %lld iterations, %.2f s%s\n", int(st), (long long)lp.stats.iterations,
                 seconds_since(t0), st == sov::Status::Optimal ? "" : " (stopped)");
-    if (st == sov::Status::Optimal) {
-        const double o2 = f.eval_objective(std::vector<double>(lp.value.begin(), lp.value.begin() + f.ncol));
-        std::printf("simplex objective %.12g, crossover relative difference %.1e\n", o2,
-                    std::abs(obj - o2) / (1.0 + std::abs(o2)));
-    }
     nir_lpgen_free(g);
     return ok ? 0 : 1;
 }
 
 int main(int argc, char** argv) {
-    if (argc > 1 && std::strcmp(argv[1], "c1") == 0) return measure_c1();
+    if (argc > 1 && std::strcmp(argv[1], "c1") == 0) return measure(NIR_GEN_RANDOM_EQ, 1, 0);
+    if (argc > 3 && std::strcmp(argv[1], "measure") == 0)
+        return measure(std::atoi(argv[2]), std::strtoull(argv[3], nullptr, 10), argc > 4 ? std::atoi(argv[4]) : 0);
     struct Case {
         const char* name;
         sov::Model m;
