@@ -310,7 +310,7 @@ def test_dropin_cli_presolve_heavy_models_match(tmp_path, seed):
     assert "Presolve:" in ours[1] or "infeasible" in ours[1] or "unbounded" in ours[1]
 
 
-def _harness(tmp_path, source, oracle=False):
+def _harness(tmp_path, source, oracle=False, args=(), timeout=300):
     """Builds tests/native/<source> against a tree of the reference's headers
     with the five drop-in headers linked in; the engine entry point is the
     harness's own stand-in, so no GPU is needed."""
@@ -336,7 +336,7 @@ def _harness(tmp_path, source, oracle=False):
                     os.path.join(ROOT, "tests", "native", source), "-o", str(exe),
                     f"-L{os.path.join(ROOT, 'nirnaya_b200')}", "-lnir_mps", "-lnir_facade",
                     f"-Wl,-rpath,{os.path.join(ROOT, 'nirnaya_b200')}", *extra, "-lpthread"], check=True)
-    return subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
+    return subprocess.run([str(exe), *args], capture_output=True, text=True, timeout=timeout)
 
 
 def test_dropin_pdhg_undoes_scale_model_exactly(tmp_path):
@@ -375,6 +375,20 @@ def test_dropin_crossover_reaches_the_simplex_optimum(tmp_path):
     for ln in its:
         pivots = int(ln.split("crossover ")[1].split()[0])
         assert pivots <= int(ln.split("from slacks ")[1].rstrip(")")) // 8, ln
+
+
+@pytest.mark.skipif(os.environ.get("NIR_MEASURE_CROSSOVER") != "1",
+                    reason="a measurement of several minutes: set NIR_MEASURE_CROSSOVER=1")
+@pytest.mark.parametrize("model", [("measure", "3", "12", "600"), ("c1",)])
+def test_crossover_measurement(tmp_path, model):
+    """Crossover timings on CPU (printed; run with -s): the reference loop
+    (oracle) for its own cap and six times that, then crossover from each
+    point with the primal and the dual finish, against the simplex from its
+    slack basis.  A multiperiod model (600 rows) and C1."""
+    r = _harness(tmp_path, "pdhg_dropin_crossover_harness.cpp", oracle=True, args=model, timeout=3600)
+    print(r.stdout)
+    if model[0] == "measure":
+        assert r.returncode == 0, r.stdout + r.stderr
 
 
 @pytest.mark.gpu
