@@ -143,13 +143,13 @@ inline CrossoverResult crossover(const sov::Model& model, const std::vector<doub
         if (keys[k].v < n) ++r.crash_structurals;
     }
     snap.status = st;
-    sov::Options lo = opt;
+    sov::Options lp_opt = opt;
     // "primal" (the default): LpSolver's primal simplex, which starts from
     // the crash basis's nearly feasible point.  Otherwise its dual path,
     // whose artificial-bounds phase 1 can wander off a basis with small
     // dual infeasibilities.
-    if (method && *method) lo.method = method;
-    sov::LpSolver lp(lo);
+    if (method && *method) lp_opt.method = method;
+    sov::LpSolver lp(lp_opt);
     lp.load(model);
     lp.set_basis(snap);
     r.status = lp.solve(deadline);
