@@ -728,6 +728,18 @@ def verify_batch_bench(args):
     t0 = time.perf_counter()
     host = [mps.verify_solution(lp, x, float(c), tol) for lp, x, c in zip(lps, xs, claimed)]
     t_host = time.perf_counter() - t0
+    # the same checks spread over all host threads, one instance per task
+    # (the library call releases the interpreter lock)
+    from concurrent.futures import ThreadPoolExecutor
+
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=cores) as pool:
+        pooled = list(pool.map(lambda a: mps.verify_solution(a[0], a[1], float(a[2]), tol, threads=1),
+                               zip(lps, xs, claimed)))
+    t_host_pool = time.perf_counter() - t0
+    if any(p != h for p, h in zip(pooled, host)):
+        raise RuntimeError("the host check differs between thread layouts")
     t_ref = None
     try:
         from oracle import ffi
@@ -780,7 +792,8 @@ def verify_batch_bench(args):
                    "timing": "host clock around the synchronous call (median)"},
         "e2e": {"value": statistics.median(e2e), "unit": "s", "h2d_bytes_per_step": 8 * n + 8 * len(lps),
                 "d2h_bytes_per_step": 48 * len(lps)},
-        "host_check_s": t_host, "reference_check_s": t_ref,
+        "host_check_s": t_host, "host_check_all_threads_s": t_host_pool, "host_threads": cores,
+        "reference_check_s": t_ref,
         "reports_bit_identical": {"from_host": from_host_ok, "in_place": in_place_ok},
         "gpu_launches": 3 * args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
