@@ -255,3 +255,35 @@ def test_single_handle_verify_matches_the_host_check():
                 got = eng.verify(x, claimed, tol, vartype=vt)
                 want = mps.verify_solution(lp, x, claimed, tol, vartype=vt)
                 assert _same(got, want), (mode, tol, got, want)
+
+
+def test_device_check_random_sweep(emu):
+    """30 random batches over all five generator kinds with bounds moved to
+    the edge values (+-inf, +-1e20, beyond 1e20, 0), random non-finite
+    entries, integer marks and tolerances: the emulated device check equals
+    the host check bit for bit."""
+    rng = np.random.default_rng(2024)
+    kinds = [(L.RANDOM_EQ, dict(m=60, n=150)), (L.ZIPF, dict(m=200, n=500, target_nnz=3000)),
+             (L.MULTIPERIOD, dict(m=500)), (L.BLEND_FAMILY, dict(m=100, n=250, target_nnz=1500)),
+             (L.BADLY_SCALED, dict(m=80, n=200, target_nnz=1200))]
+    edges = np.array([np.inf, -np.inf, 1e20, -1e20, 3e20, -5e25, 0.0])
+    for trial in range(30):
+        lps, xs, vts, claimed = [], [], [], []
+        for _ in range(int(rng.integers(1, 5))):
+            kind, kw = kinds[int(rng.integers(0, len(kinds)))]
+            lp = L.generate(kind, int(rng.integers(0, 1000)), **kw)
+            for arr in (lp.collo, lp.colup, lp.rowlo, lp.rowup):
+                hit = rng.random(arr.size) < 0.05
+                arr[hit] = edges[rng.integers(0, edges.size, int(hit.sum()))]
+            x = rng.normal(size=lp.ncol) * 10 ** rng.uniform(-2, 2)
+            x[rng.random(lp.ncol) < 0.3] = 0.0
+            if rng.random() < 0.2:
+                x[int(rng.integers(0, lp.ncol))] = [np.nan, np.inf][int(rng.integers(0, 2))]
+            lps.append(lp)
+            xs.append(x)
+            vts.append((rng.random(lp.ncol) < 0.2).astype(np.int8) * int(rng.integers(1, 3)))
+            claimed.append([np.nan, float(rng.normal() * 100)][int(rng.integers(0, 2))])
+        tol = float(10 ** rng.uniform(-10, 1))
+        got, want = emu(lps, xs, vts, np.array(claimed), tol), host_reports(lps, xs, vts, claimed, tol)
+        for k, (g, w) in enumerate(zip(got, want)):
+            assert _same(g, w), (trial, k, g, w)
