@@ -1,5 +1,5 @@
 // Host emulation of the device solution check (nirnaya_b200/csrc/k_verify.cuh),
-// for tests/test_verify_device.py.
+// for tests/test_zz_verify_device.py.
 //
 // Compiled with g++ (-ffp-contract=off) from the same header the kernels
 // use, so the per-element arithmetic is the kernels' own.  What the kernels
