@@ -163,11 +163,17 @@ def gather_results(local: dict, rank: int, world: int):
 
 
 def solve_sharded(lps: list[LP], rank: int, world: int, device: int = 0, params: P.Params | None = None,
-                  solve_fn=None):
+                  solve_fn=None, verify_tol: float | None = None):
     """Solves this rank's shard of `lps` as one batch and gathers
-    {index: (objective, status, iterations)} on rank 0. `solve_fn(lps)`
-    replaces the device solve (it must return one (objective, status,
-    iterations) per LP), which lets the sharding run on hosts without a GPU."""
+    {index: (objective, status, iterations)} on rank 0.
+
+    With verify_tol, each rank also checks its solved points where they lie,
+    on the device (BatchEngine.verify: verify_solution bit for bit).  Each
+    result then ends with the check's verdict: (objective, status,
+    iterations, passed).
+
+    `solve_fn(lps)` replaces the device solve, which lets the sharding run
+    on hosts without a GPU.  It returns one such tuple per LP."""
     mine = shard_instances([lp.nnz for lp in lps], world)[rank]
     local = {}
     if mine:
@@ -175,7 +181,10 @@ def solve_sharded(lps: list[LP], rank: int, world: int, device: int = 0, params:
         if solve_fn is None:
             with BatchEngine(sub, device) as eng:
                 res, _ = eng.solve(params)
-            vals = [(inf.objective, inf.status, inf.iterations) for _, _, inf in res]
+                vals = [(inf.objective, inf.status, inf.iterations) for _, _, inf in res]
+                if verify_tol is not None:
+                    reps = eng.verify(None, [v[0] for v in vals], verify_tol)
+                    vals = [v + (r["passed"],) for v, r in zip(vals, reps)]
         else:
             vals = solve_fn(sub)
         local = {i: v for i, v in zip(mine, vals)}

@@ -287,3 +287,19 @@ def test_device_check_random_sweep(emu):
         got, want = emu(lps, xs, vts, np.array(claimed), tol), host_reports(lps, xs, vts, claimed, tol)
         for k, (g, w) in enumerate(zip(got, want)):
             assert _same(g, w), (trial, k, g, w)
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not has_gpu(), reason="needs a CUDA device")
+def test_sharded_solve_checks_its_shard_on_the_device():
+    """solve_sharded(verify_tol=...): the rank's solved points are checked in
+    place and every result carries the verdict; solved instances pass."""
+    from nirnaya_b200 import batch as B
+    from nirnaya_b200 import pdhg
+
+    lps = [L.generate(L.RANDOM_EQ, 31, m=200, n=500), L.generate(L.MULTIPERIOD, 32, m=600),
+           L.generate(L.RANDOM_EQ, 33, m=80, n=200)]
+    got = B.solve_sharded(lps, 0, 1, params=pdhg.default_params(tol=1e-6, max_iters=200000), verify_tol=1e-4)
+    assert sorted(got) == [0, 1, 2]
+    for obj, status, iterations, passed in got.values():
+        assert status != pdhg.OPTIMAL or passed, (obj, status, iterations)
