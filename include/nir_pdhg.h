@@ -247,7 +247,9 @@ void nir_pdhg_batch_free(nir_pdhg_batch* b);
  *     (src/model/model.hpp:73-98).
  * The host check in libnir_mps.so remains the reference for this one.
  *
- * x: ncol host doubles.  vartype: ncol bytes (1 integer, 2 binary) or NULL
+ * x: ncol host doubles, or NULL for the point the last nir_pdhg_solve on this
+ * handle returned, which is still on the device (NULL before any solve is an
+ * input error).  vartype: ncol bytes (1 integer, 2 binary) or NULL
  * (all continuous).  claimed_obj: NaN when there is none (obj_rel_err is then
  * 0).  Returns 0, or NIR_STATUS_INPUT_ERROR / NIR_STATUS_INTERNAL_ERROR with
  * nir_pdhg_last_error(). */

@@ -181,6 +181,7 @@ struct nir_pdhg {
     unsigned* gs_gen = nullptr;
     int* gs_err = nullptr;
     int launches = 0;
+    const double* last_x = nullptr;  // the point the last solve returned, still on the device (null before one)
     // the device solution check's buffers, allocated by its first call
     struct Verify {
         bool ready = false;
@@ -952,6 +953,7 @@ int solve_reference(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), v
     d2h(h, y.data(), h->y64, m * sizeof(double));
     if (x_out) std::memcpy(x_out, x.data(), n * sizeof(double));
     if (y_out) std::memcpy(y_out, y.data(), m * sizeof(double));
+    h->last_x = h->x64;
     int status;
     if (st.ref_stopped) status = NIR_STATUS_OPTIMAL;
     else if (st.done) status = NIR_STATUS_ITERATION_LIMIT;
@@ -1348,6 +1350,7 @@ int solve_fast(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), void* 
     NIR_CUDA(cudaStreamSynchronize(s));
     if (x_out) std::memcpy(x_out, x.data(), n * sizeof(double));
     if (y_out) std::memcpy(y_out, y.data(), m * sizeof(double));
+    h->last_x = h->out_x;
     int status;
     if (st.done) status = st.status;
     else if (R.stopped_by_host) status = NIR_STATUS_TIME_LIMIT;
@@ -1478,6 +1481,7 @@ int nir_pdhg_solve(nir_pdhg* h, const nir_pdhg_params* p_in, int (*poll)(void*),
     try {
         NIR_CUDA(cudaSetDevice(h->device));
         const int before = h->launches;
+        h->last_x = nullptr;  // out_x and x64 serve as scratch until the solve's end
         int st;
         if (p.algorithm == NIR_ALGO_REFERENCE) st = solve_reference(h, p, poll, poll_ctx, x_out, y_out, info);
         else st = solve_fast(h, p, poll, poll_ctx, x_out, y_out, info);

@@ -76,16 +76,24 @@ extern "C" {
 
 int nir_pdhg_verify(nir_pdhg* h, const double* x, const int8_t* vartype, double claimed_obj, double tol,
                     nir_verify_report* out) {
-    if (!h || !out || (!x && h->n > 0)) {
-        g_err = !h ? "null handle" : (!out ? "null report" : "null point");
+    if (!h || !out) {
+        g_err = !h ? "null handle" : "null report";
+        return NIR_STATUS_INPUT_ERROR;
+    }
+    if (!x && !h->last_x) {
+        g_err = "no point given and no solve has returned one";
         return NIR_STATUS_INPUT_ERROR;
     }
     try {
         NIR_CUDA(cudaSetDevice(h->device));
         verify_buffers(h, 1);
-        if (h->n > 0) NIR_CUDA(cudaMemcpyAsync(h->vfy.x, x, size_t(h->n) * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-        verify_impl(h, 1, h->vfy.row_off, h->vfy.col_off, nullptr, &h->offset, h->vfy.x, vartype, &claimed_obj, tol,
-                    out);
+        const double* d_x = h->last_x;
+        if (x) {
+            if (h->n > 0)
+                NIR_CUDA(cudaMemcpyAsync(h->vfy.x, x, size_t(h->n) * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+            d_x = h->vfy.x;
+        }
+        verify_impl(h, 1, h->vfy.row_off, h->vfy.col_off, nullptr, &h->offset, d_x, vartype, &claimed_obj, tol, out);
         return 0;
     } catch (const std::invalid_argument& e) {
         g_err = e.what();

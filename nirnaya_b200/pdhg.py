@@ -234,13 +234,17 @@ class Engine:
                row_names=None) -> dict:
         """verify_solution (src/io/sol_io.hpp:25-106) on the GPU against
         this handle's LP (nir_pdhg_verify): the report mps.verify_solution
-        gives on the host, bit for bit."""
-        xv = np.ascontiguousarray(x, np.float64)
-        if xv.shape != (self.lp.ncol,):
-            raise ValueError(f"x has {xv.size} values for {self.lp.ncol} columns")
+        gives on the host, bit for bit.  x None checks the point the last
+        solve returned, where it still lies on the device."""
+        xv = None
+        if x is not None:
+            xv = np.ascontiguousarray(x, np.float64)
+            if xv.shape != (self.lp.ncol,):
+                raise ValueError(f"x has {xv.size} values for {self.lp.ncol} columns")
         vt = None if vartype is None else np.ascontiguousarray(vartype, np.int8)
         rep = VerifyReport()
-        rc = lib().nir_pdhg_verify(self._h, _dptr(xv), None if vt is None else vt.ctypes.data_as(C.POINTER(C.c_int8)),
+        rc = lib().nir_pdhg_verify(self._h, None if xv is None else _dptr(xv),
+                                   None if vt is None else vt.ctypes.data_as(C.POINTER(C.c_int8)),
                                    float(claimed_obj), float(tol), C.byref(rep))
         if rc != 0:
             raise RuntimeError(f"nir_pdhg_verify failed ({STATUS_NAMES.get(rc, rc)}): {last_error()}")

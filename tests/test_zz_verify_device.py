@@ -291,6 +291,24 @@ def test_device_check_random_sweep(emu):
 
 @pytest.mark.gpu
 @pytest.mark.skipif(not has_gpu(), reason="needs a CUDA device")
+@pytest.mark.parametrize("algorithm", ["pdlp", "reference"])
+def test_single_handle_checks_its_solved_point_in_place(algorithm):
+    """Engine.verify(None) after a solve (PDLP or the reference loop) checks
+    the returned point on the device: the host check's report for it."""
+    from nirnaya_b200 import pdhg
+
+    lp = L.generate(L.RANDOM_EQ, 5, m=300, n=750)
+    with pdhg.Engine(lp) as eng:
+        with pytest.raises(RuntimeError, match="no solve"):
+            eng.verify(None)
+        algo = pdhg.ALGO_PDLP if algorithm == "pdlp" else pdhg.ALGO_REFERENCE
+        x, _, info = eng.solve(pdhg.default_params(algorithm=algo, tol=1e-6, max_iters=20000))
+        got = eng.verify(None, info.objective, 1e-6)
+    assert _same(got, mps.verify_solution(lp, x, info.objective, 1e-6))
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not has_gpu(), reason="needs a CUDA device")
 def test_sharded_solve_checks_its_shard_on_the_device():
     """solve_sharded(verify_tol=...): the rank's solved points are checked in
     place and every result carries the verdict; solved instances pass."""
