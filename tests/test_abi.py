@@ -113,3 +113,24 @@ def test_python_solver_mirror_uses_the_dropin_iteration_cap():
     assert p.max_iters == 5000
     p = pdhg.PdhgSolver.params_from(pdhg.Options(pdhg_max_iters=123, extra={"check_every": 32}))
     assert p.max_iters == 123 and p.check_every == 32
+
+
+def test_verify_entry_points_reject_bad_arguments_before_any_device_call():
+    """nir_pdhg_verify / nir_pdhg_batch_verify check their arguments on the
+    host: a null handle or report is an input error with a message."""
+    import ctypes as C
+
+    from nirnaya_b200 import batch as B
+    from nirnaya_b200 import mps
+    from nirnaya_b200 import pdhg
+
+    if not os.path.exists(pdhg.LIB_PATH):
+        pytest.skip("libnir_pdhg.so not built")
+    lib = B._lib()
+    rep = mps.VerifyReport()
+    assert lib.nir_pdhg_verify(None, None, None, 0.0, 1e-6, C.byref(rep)) == pdhg.INPUT_ERROR
+    assert pdhg.last_error() == "null handle"
+    assert lib.nir_pdhg_batch_verify(None, None, None, None, 1e-6, C.byref(rep)) == pdhg.INPUT_ERROR
+    assert pdhg.last_error() == "null handle"
+    assert lib.nir_pdhg_batch_verify(None, None, None, None, 1e-6, None) == pdhg.INPUT_ERROR
+    assert pdhg.last_error() == "null report"
