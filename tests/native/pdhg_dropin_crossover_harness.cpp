@@ -264,7 +264,45 @@ static int measure(int kind, unsigned long long seed, int m) {
     return ok ? 0 : 1;
 }
 
+// "mps <file>...": each model's LP (integrality dropped; models with a
+// quadratic objective are skipped), crossover from its simplex optimum
+// perturbed by 1e-6, against the simplex from slacks.
+static int check_files(int argc, char** argv) {
+    sov::Options opt;
+    opt.log_level = 0;
+    for (int a = 2; a < argc; ++a) {
+        sov::Model f;
+        std::string err;
+        if (sov::MpsReader::read(argv[a], f, err) != sov::Status::Optimal) return fail(argv[a], err.c_str());
+        if (f.is_qp()) continue;
+        if (f.sense == sov::Sense::Maximize) {  // the LP as the solver minimises it
+            for (double& c : f.cost) c = -c;
+            f.obj_offset = -f.obj_offset;
+            f.sense = sov::Sense::Minimize;
+        }
+        f.vartype.assign(size_t(f.ncol), sov::VarType::Continuous);
+        std::vector<double> xa, ya;
+        const long long scratch = approximate_optimum(f, xa, ya, 1e-6);
+        if (scratch < 0) return fail(argv[a], "the simplex does not solve its LP");
+        sov::LpSolver ref(opt);
+        ref.load(f);
+        sov::Deadline dl;
+        ref.solve(dl);
+        const double obj_ref = f.eval_objective(std::vector<double>(ref.value.begin(), ref.value.begin() + f.ncol));
+        const nir::dropin::CrossoverResult r = nir::dropin::crossover(f, xa, ya, opt, dl, 1e-6);
+        const double obj = f.eval_objective(r.x);
+        if (r.status != sov::Status::Optimal || std::abs(obj - obj_ref) > 1e-9 * (1.0 + std::abs(obj_ref)) ||
+            !sov::verify_solution(f, r.x, obj, 1e-9).passed)
+            return fail(argv[a], "crossover on the model's LP");
+        std::printf("%s: m=%d n=%d objective %.12g, simplex from slacks %lld iterations, crossover %lld\n",
+                    f.name.c_str(), int(f.nrow), int(f.ncol), obj, scratch, (long long)r.simplex_iterations);
+    }
+    std::printf("ok\n");
+    return 0;
+}
+
 int main(int argc, char** argv) {
+    if (argc > 1 && std::strcmp(argv[1], "mps") == 0) return check_files(argc, argv);
     if (argc > 1 && std::strcmp(argv[1], "c1") == 0) return measure(NIR_GEN_RANDOM_EQ, 1, 0);
     if (argc > 3 && std::strcmp(argv[1], "measure") == 0)
         return measure(std::atoi(argv[2]), std::strtoull(argv[3], nullptr, 10), argc > 4 ? std::atoi(argv[4]) : 0);

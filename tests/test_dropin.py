@@ -377,6 +377,23 @@ def test_dropin_crossover_reaches_the_simplex_optimum(tmp_path):
         assert pivots <= int(ln.split("from slacks ")[1].rstrip(")")) // 8, ln
 
 
+def test_dropin_crossover_on_the_refinery_models(tmp_path):
+    """The reference's data/refinery models as LPs (integrality dropped, the
+    QPs skipped): crossover from each simplex optimum perturbed by 1e-6
+    reaches that optimum with a passing dd check, in no more pivots than
+    the simplex from slacks."""
+    if not os.path.isdir(REFINERY):
+        pytest.skip("the reference's refinery models are absent")
+    files = sorted(os.path.join(REFINERY, f) for f in os.listdir(REFINERY) if f.endswith(".mps"))
+    r = _harness(tmp_path, "pdhg_dropin_crossover_harness.cpp", oracle=True, args=["mps", *files])
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout + r.stderr
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("MRPL_")]
+    assert len(lines) >= 4
+    for ln in lines:
+        scratch = int(ln.split("simplex from slacks ")[1].split()[0])
+        assert int(ln.rsplit("crossover ", 1)[1]) <= scratch, ln
+
+
 @pytest.mark.skipif(os.environ.get("NIR_MEASURE_CROSSOVER") != "1",
                     reason="a measurement of several minutes: set NIR_MEASURE_CROSSOVER=1")
 @pytest.mark.parametrize("model", [("measure", "3", "12", "600"), ("c1",)])
