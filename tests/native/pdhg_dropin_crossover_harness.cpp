@@ -367,6 +367,19 @@ int main(int argc, char** argv) {
                 return fail(c.name, "vertex or duals of the worked example");
         }
 
+        // 3b: the dual finish, selected through the environment, reaches the same optimum
+        setenv("NIR_PDHG_CROSSOVER_METHOD", "dual", 1);
+        {
+            sov::Options so = opt;
+            so.method = "pdhg";
+            g_status = NIR_STATUS_OPTIMAL;
+            const sov::SolveResult res = sov::Solver(so).solve(c.m);
+            if (res.status != sov::Status::Optimal || !res.verification.passed ||
+                std::abs(res.objective - obj_ref) > 1e-9 * (1.0 + std::abs(obj_ref)))
+                return fail(c.name, "Solver with NIR_PDHG_CROSSOVER_METHOD=dual");
+        }
+        unsetenv("NIR_PDHG_CROSSOVER_METHOD");
+
         // 4: auto runs only when the engine stopped short
         setenv("NIR_PDHG_CROSSOVER", "auto", 1);
         sov::Options so = opt;
