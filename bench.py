@@ -740,7 +740,7 @@ def verify_batch_bench(args):
     t_host_pool = time.perf_counter() - t0
     if any(p != h for p, h in zip(pooled, host)):
         raise RuntimeError("the host check differs between thread layouts")
-    t_ref = None
+    t_ref = None  # the cpu_baseline leg: the reference's own check, built from its sources
     try:
         from oracle import ffi
 
@@ -793,7 +793,9 @@ def verify_batch_bench(args):
         "e2e": {"value": statistics.median(e2e), "unit": "s", "h2d_bytes_per_step": 8 * n + 8 * len(lps),
                 "d2h_bytes_per_step": 48 * len(lps)},
         "host_check_s": t_host, "host_check_all_threads_s": t_host_pool, "host_threads": cores,
-        "reference_check_s": t_ref,
+        "cpu_baseline": None if t_ref is None else {
+            "value": t_ref, "unit": "s", "cores": 1, "kind": "reference",
+            "sample": "the reference's verify_solution on all 256 instances, once, one after another"},
         "reports_bit_identical": {"from_host": from_host_ok, "in_place": in_place_ok},
         "gpu_launches": 3 * args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
