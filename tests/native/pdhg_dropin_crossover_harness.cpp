@@ -43,7 +43,6 @@
 namespace {
 
 int g_status = NIR_STATUS_OPTIMAL;  // what the stand-in engine reports
-int g_engine_calls = 0;
 
 sov::Model model_from(const nir_lp_view* lp) {
     sov::Model m;
@@ -95,7 +94,6 @@ extern "C" int nir_pdhg_default_params(nir_pdhg_params* p) {
 
 extern "C" int nir_pdhg_solve_lp(const nir_lp_view* lp, int, const nir_pdhg_params*, int (*)(void*), void*,
                                  double* x, double* y, nir_pdhg_info* info) {
-    ++g_engine_calls;
     std::vector<double> xa, ya;
     if (approximate_optimum(model_from(lp), xa, ya) < 0) return NIR_STATUS_NUMERICAL_TROUBLE;
     std::memcpy(x, xa.data(), xa.size() * sizeof(double));
