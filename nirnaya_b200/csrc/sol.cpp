@@ -458,14 +458,15 @@ int nir_verify_solution(const nir_lp_view* lp, const int8_t* vartype, int64_t qn
     // columns with x != 0 in order, adding the entries that fall in its
     // range.  Every row's terms thus arrive in ascending column order, the
     // order of the reference's column loop, and each thread's accumulators
-    // stay in its own cache.  One more thread evaluates the objective
-    // meanwhile.
+    // stay in its own cache.  With more than one thread allowed, one more
+    // thread evaluates the objective meanwhile.
     {
         const int64_t nnz = lp->nnz;
         const int nr = int(std::max<int64_t>(1, std::min<int64_t>(T, 1 + nnz / 131072)));
         std::vector<Rec> rows(static_cast<size_t>(nr));
         double obj = 0.0;
-        run_threads(nr + 1, [&](int k) {
+        const bool obj_thread = T > 1;  // with one thread the objective follows the rows
+        run_threads(nr + (obj_thread ? 1 : 0), [&](int k) {
             if (k == nr) {
                 obj = nir_eval_objective(lp, qnnz, q_start, q_index, q_value, x);
                 return;
@@ -498,7 +499,7 @@ int nir_verify_solution(const nir_lp_view* lp, const int8_t* vartype, int64_t qn
             rep.worst_kind = R.kind;
             rep.worst_index = R.pos / 2;
         }
-        rep.computed_obj = obj;
+        rep.computed_obj = obj_thread ? obj : nir_eval_objective(lp, qnnz, q_start, q_index, q_value, x);
     }
     if (std::isfinite(claimed_obj))
         rep.obj_rel_err = std::abs(rep.computed_obj - claimed_obj) / (1.0 + std::abs(rep.computed_obj));
