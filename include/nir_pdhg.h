@@ -295,9 +295,12 @@ typedef struct nir_csr_dev {
  * 32 + 2*ncol + nrow + ceil(nrow/256) <= 2^20, else NIR_STATUS_INPUT_ERROR.
  * The first call on a device resolves the array's device address
  * (cudaGetSymbolAddress) with that device current; make that first call
- * before any stream capture.  All calls share the array and each call
- * clears the state it needs: calls that overlap on the GPU (other streams,
- * other threads) race.  Returns *status. */
+ * before any stream capture.  The address is kept for the life of the
+ * process: after a cudaDeviceReset of that device it is stale, so do not
+ * call this entry point on a device that was reset.  Every call waits for
+ * its stream (it reads the stop test back every 32 iterations).  All calls
+ * share the array and each call clears the state it needs: calls that
+ * overlap on the GPU (other streams, other threads) race.  Returns *status. */
 int nir_pdhg_reference_solve_noalloc(const nir_csr_dev* A, const nir_csr_dev* At, const double* cost,
                                      const double* collo, const double* colup, const double* rowlo,
                                      const double* rowup, int64_t max_iters, void* stream, double* x_out,

@@ -173,7 +173,11 @@ def solve_sharded(lps: list[LP], rank: int, world: int, device: int = 0, params:
     iterations, passed).
 
     `solve_fn(lps)` replaces the device solve, which lets the sharding run
-    on hosts without a GPU.  It returns one such tuple per LP."""
+    on hosts without a GPU.  It returns one such tuple per LP.  The check
+    runs on the device solve only, so solve_fn and verify_tol together are
+    an error."""
+    if solve_fn is not None and verify_tol is not None:
+        raise ValueError("verify_tol checks the device solve's points; it cannot be combined with solve_fn")
     mine = shard_instances([lp.nnz for lp in lps], world)[rank]
     local = {}
     if mine:

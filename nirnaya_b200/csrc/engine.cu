@@ -185,6 +185,7 @@ struct nir_pdhg {
     // the device solution check's buffers, allocated by its first call
     struct Verify {
         bool ready = false;
+        int count = 0;  // instances the per-instance arrays hold
         double *x = nullptr, *rv = nullptr, *obj = nullptr, *claimed = nullptr, *offset = nullptr;
         int8_t *vt = nullptr, *rs = nullptr;
         long long* fb = nullptr;
@@ -1733,6 +1734,8 @@ extern "C" int nir_pdhg_reference_solve_noalloc(const nir_csr_dev* A, const nir_
     }
     // scratch: state (256 B) | xbar (n) | u (n) | v (m) | per-block maxima
     const long long state_d = 32;
+    static_assert(sizeof(nir::DevState) <= 32 * sizeof(double),
+                  "the solver state must fit the 32 doubles reserved for it ahead of xbar");
     const long long nblk = (m + nir::kBlock - 1) / nir::kBlock;
     const long long need = state_d + 2 * n + m + std::max(nblk, 1LL);
     if (need > kNoAllocScratchDoubles) {

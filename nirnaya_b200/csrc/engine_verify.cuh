@@ -13,7 +13,14 @@ namespace {
 
 void verify_buffers(nir_pdhg* h, int count) {
     auto& v = h->vfy;
-    if (v.ready) return;
+    if (v.ready) {
+        // the per-instance arrays were sized by the first call
+        if (count > v.count)
+            throw std::invalid_argument("a check of " + std::to_string(count) + " instances on a handle whose check buffers hold " +
+                                        std::to_string(v.count));
+        return;
+    }
+    v.count = count;
     v.x = h->alloc<double>(h->n);
     v.vt = h->alloc<int8_t>(h->n);
     v.rv = h->alloc<double>(h->m);

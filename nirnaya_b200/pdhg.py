@@ -242,6 +242,8 @@ class Engine:
             if xv.shape != (self.lp.ncol,):
                 raise ValueError(f"x has {xv.size} values for {self.lp.ncol} columns")
         vt = None if vartype is None else np.ascontiguousarray(vartype, np.int8)
+        if vt is not None and vt.shape != (self.lp.ncol,):
+            raise ValueError(f"vartype has {vt.size} marks for {self.lp.ncol} columns")
         rep = VerifyReport()
         rc = lib().nir_pdhg_verify(self._h, None if xv is None else _dptr(xv),
                                    None if vt is None else vt.ctypes.data_as(C.POINTER(C.c_int8)),

@@ -72,7 +72,7 @@ def verify_input(seed):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else (os.environ.get("NIRNAYA_REF") or os.path.join(ROOT, os.pardir, "reference"))
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), f"REF={ref}"], check=True)
     from nirnaya_b200 import build
     build.build_lpgen()

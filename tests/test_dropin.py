@@ -127,7 +127,8 @@ def test_c_api_and_ctypes_sdk_reach_the_engine():
 
 @pytest.mark.gpu
 @pytest.mark.skipif(not has_gpu(), reason="needs a CUDA device")
-@pytest.mark.parametrize("args", [["--method", "pdhg"], ["--set", "method=pdhg"], ["--set", "method=gpu"]])
+@pytest.mark.parametrize("args", [["--method", "pdhg"], ["--method=pdhg"], ["--method=gpu"], ["--set", "method=pdhg"],
+                                  ["--set", "method=gpu"]])
 def test_cli_method_pdhg_on_crude_blending(tmp_path, args):
     # data/refinery/MRPL_Crude_Blending_LP: optimum 22171.59777424483 (.sol:2)
     g = GOLD["crude_blending"]
@@ -150,7 +151,8 @@ def test_cli_method_pdhg_on_crude_blending(tmp_path, args):
 
 # ---- the MPS reader drop-in (nirnaya_b200/sov/mps_reader.hpp): CPU only
 
-REF_DIR = os.environ.get("NIRNAYA_REF", "/root/reference")
+# the reference checkout beside this repository, unless NIRNAYA_REF names another
+REF_DIR = os.environ.get("NIRNAYA_REF") or os.path.join(ROOT, os.pardir, "reference")
 REFINERY = os.path.join(REF_DIR, "data", "refinery")
 REF_CHECKER = os.path.join(ROOT, "oracle", "_ref", "checker")
 
@@ -266,6 +268,35 @@ def test_dropin_cli_cpu_methods_match_the_reference_cli(tmp_path, model, method)
     the .sol all equal the reference CLI's (only timings differ)."""
     ours, ref = _cli_pair(tmp_path, os.path.join(REFINERY, model + ".mps"), ["--method", method])[::-1]
     assert ours == ref
+
+
+@pytest.mark.parametrize("method", ["dual", "ipm"])
+def test_dropin_cli_accepts_the_method_equals_form(tmp_path, method):
+    """`--method=<m>` (README.md:27) selects the method as `--method <m>`
+    does; the reference's own loop drops that form (cli_main.cpp:77)."""
+    model = os.path.join(REFINERY, "MRPL_Crude_Blending_LP.mps")
+    if not os.path.exists(model):
+        pytest.skip("the reference's refinery models are absent")
+    ref = _cli_pair(tmp_path, model, ["--method", method])[0]
+    exe = _need("sovsolve")
+    sol = str(tmp_path / "eq.sol")
+    r = subprocess.run([exe, model, f"--method={method}", f"--sol={sol}"], capture_output=True, text=True, timeout=300)
+    text = "\n".join(ln for ln in r.stdout.splitlines() if "Time:" not in ln)
+    assert (r.returncode, text, open(sol).read()) == ref
+
+
+@pytest.mark.skipif(has_gpu(), reason="checks the no-GPU failure mode")
+@pytest.mark.parametrize("form", [["--method=pdhg"], ["--method", "pdhg"], ["--method=gpu"]])
+def test_dropin_cli_method_pdhg_form_reaches_the_engine(tmp_path, form):
+    """Every spelling of the PDHG method reaches the GPU engine, which
+    without a device fails loudly instead of falling back to the CPU."""
+    model = os.path.join(REFINERY, "MRPL_Crude_Blending_LP.mps")
+    if not os.path.exists(model):
+        pytest.skip("the reference's refinery models are absent")
+    r = subprocess.run([_need("sovsolve"), model, *form], capture_output=True, text=True, timeout=300)
+    out = r.stdout + r.stderr
+    assert "no CUDA device" in out, out
+    assert "Simplex" not in out, out
 
 
 @pytest.mark.parametrize("seed", [0, 1, 2])

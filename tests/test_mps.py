@@ -21,7 +21,8 @@ from conftest import ROOT
 from mps_cases import CASES, random_mps
 
 GOLDEN = os.path.join(ROOT, "tests", "golden", "mps_golden.json")
-REFINERY = os.path.join(os.environ.get("NIRNAYA_REF", "/root/reference"), "data", "refinery")
+# the reference checkout beside this repository, unless NIRNAYA_REF names another
+REFINERY = os.path.join(os.environ.get("NIRNAYA_REF") or os.path.join(ROOT, os.pardir, "reference"), "data", "refinery")
 KEYS = ("col_start", "row_index", "value", "cost", "collo", "colup", "rowlo", "rowup")
 
 
