@@ -168,20 +168,31 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def primal_bytes(lp, w):
+def primal_bytes(lp, w, vw=None):
     """Algorithmic bytes of one fused A'y + primal-update launch, counted
-    unfused: the CSR SpMV of A' (n rows; w-byte values, 4-byte indices and
+    unfused: the CSR SpMV of A' (n rows; vw-byte values, 4-byte indices and
     row pointers, y read once, A'y written once) plus the primal update
-    (x, c, l, u, A'y read, x and x-bar written), w = 4 (FP32) or 8 (FP64)."""
+    (x, c, l, u, A'y read, x and x-bar written), w = 4 (FP32) or 8 (FP64)
+    the vector width, vw the value width (w unless the values are FP32 with
+    FP64 vectors)."""
     n, m, nnz = lp.ncol, lp.nrow, lp.nnz
-    return (4 + w) * nnz + 4 * (n + 1) + w * m + w * n + 7 * w * n
+    vw = w if vw is None else vw
+    return (4 + vw) * nnz + 4 * (n + 1) + w * m + w * n + 7 * w * n
 
 
-def dual_bytes(lp, w):
+def dual_bytes(lp, w, vw=None):
     """Same for the fused A x-bar + dual-update launch: SpMV of A (m rows)
     plus the dual update (y, A x-bar, row bounds read, y written)."""
     n, m, nnz = lp.ncol, lp.nrow, lp.nnz
-    return (4 + w) * nnz + 4 * (m + 1) + w * n + w * m + 5 * w * m
+    vw = w if vw is None else vw
+    return (4 + vw) * nnz + 4 * (m + 1) + w * n + w * m + 5 * w * m
+
+
+def spmv_bytes_w(lp, transpose, vword, xword):
+    """spmv_bytes with separate value and vector widths (FP32 values with
+    FP64 vectors stream 8 bytes per nonzero but read and write FP64)."""
+    R, Cc = (lp.ncol, lp.nrow) if transpose else (lp.nrow, lp.ncol)
+    return (4 + vword) * lp.nnz + 4 * (R + 1) + xword * Cc + xword * R
 
 
 def spmv_bytes(lp, transpose, word):
@@ -276,21 +287,44 @@ def run_ours(args, rank, world, local):
                                      x.ctypes.data_as(C.POINTER(C.c_double)), y.ctypes.data_as(C.POINTER(C.c_double)),
                                      C.byref(info))
         e2e_s.append(time.perf_counter() - t0)
-        launches_e2e = info.kernel_launches
     e2e = allmax(statistics.median(e2e_s), world)
-    # dominant kernel, timed live with CUDA events on the engine's stream
-    eng.set_profiling(True)
+    # steady-state event timing of the fused kernels on the solved state,
+    # in the precision of each phase of the timed solves
+    kt = {}
     flush.fill_(1)
     eng.solve(params)
-    kt = eng.kernel_times()
-    eng.set_profiling(False)
-    lay = eng.layout()
-    # plain SpMV of A' in FP32 with a cold L2 (the SpMV GB/s of the metric)
-    spmv_t_us = eng.time_spmv(True, 2, reps=20, flush_l2=True)
-    spmv_a_us = eng.time_spmv(False, 2, reps=20, flush_l2=True)
+    lay_first = eng.layout()
+    kt[wl["precision"]] = eng.time_iteration(wl["precision"], reps=100)
+    # the same workload in FP64 throughout: one solve, for the mixed-precision gain
+    fp64 = None
+    if wl["precision"] != pdhg.PREC_FP64:
+        p64 = pdhg.default_params(precision=pdhg.PREC_FP64, tol=1e-6, max_iters=args.max_iters)
+        eng.solve(p64)  # the FP64 layout is tuned here (untimed)
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, _, i64 = eng.solve(p64)
+        torch.cuda.synchronize()
+        fp64 = dict(seconds=time.perf_counter() - t0, iterations=i64.iterations, status=i64.status,
+                    rel_kkt=i64.rel_kkt, objective=i64.objective)
+    kt[pdhg.PREC_FP64] = eng.time_iteration(pdhg.PREC_FP64, reps=100)
+    lay64 = eng.layout()
+    # plain SpMV with a cold L2 (the SpMV GB/s of the metric): the CTA-block
+    # kernel in each precision and the row-less gather ceilings
+    spmv = {}
+    for tr, side in ((False, "A"), (True, "At")):
+        for kname, kind, vw, xw, cap in (("cta_f32", pdhg.K_CTA32, 4, 4, lay_first.block_nnz),
+                                         ("cta_f32val_f64x", pdhg.K_CTA_MIXED, 4, 8, lay_first.block_nnz),
+                                         ("cta_f64", pdhg.K_CTA64, 8, 8, lay64.block_nnz),
+                                         ("ceiling_gather_f32", pdhg.K_CEIL_GATHER32, 4, 4, 0),
+                                         ("ceiling_gather_f64", pdhg.K_CEIL_GATHER64, 8, 8, 0),
+                                         ("ceiling_stream_f64", pdhg.K_CEIL_STREAM64, 8, 8, 0)):
+            us = eng.time_kernel(tr, kind, cap, reps=20, flush_l2=True)
+            by = spmv_bytes_w(lp, tr, vw, xw)
+            spmv[f"{side}_{kname}"] = {"us": us, "GBs": by / (us * 1e-6) / 1e9, "bytes": by, "block_nnz": cap}
     eng.close()
-    return dict(lp=lp, ms=ms, infos=infos, launches=launches, e2e=e2e, kt=kt, lay=lay, clocks=clk.summary(),
-                spmv_t_us=spmv_t_us, spmv_a_us=spmv_a_us, launches_e2e=launches_e2e)
+    return dict(lp=lp, ms=ms, infos=infos, launches=launches, e2e=e2e, kt=kt, lay=lay_first, lay64=lay64,
+                clocks=clk.summary(), spmv=spmv, fp64=fp64)
 
 
 def cpu_baseline(lp, label, seconds=15.0, threads=None):
@@ -433,8 +467,12 @@ def batch_line(args, r, world):
     }
 
 
-def run_learned(args, world):
-    """c4: the learned warm start pipeline on one GPU (replicas only)."""
+def learned_figures(n_train, n_test, n_pdhg, pdhg_iters, epochs):
+    """The learned warm start on the blending family (c4): PDLP solves
+    n_train training instances, the network trains on them, n_test held-out
+    instances are solved cold and warm (prediction included) to 1e-6, and
+    n_pdhg of them also by cold FP64 PDLP and by plain unrestarted FP64 PDHG.
+    Returns (figures, clocks)."""
     import numpy as np
 
     from nirnaya_b200 import learned as LW
@@ -444,25 +482,24 @@ def run_learned(args, world):
     p = pdhg.default_params(tol=1e-6, max_iters=1000000)
     eng = pdhg.Engine(fam.base, 0)
     t0 = time.perf_counter()
-    train = LW.solve_family(fam, range(100000, 100000 + args.c4_train), p, engine=eng)
+    train = LW.solve_family(fam, range(100000, 100000 + n_train), p, engine=eng)
     t_gen = time.perf_counter() - t0
     model = LW.WarmStart(fam, width=512, depth=3, seed=0, lr=1e-3)
     t0 = time.perf_counter()
-    fit = model.fit(train, epochs=args.c4_epochs, batch=8192, cols_per_instance=1024, rows_per_instance=512)
+    fit = model.fit(train, epochs=epochs, batch=8192, cols_per_instance=1024, rows_per_instance=512)
     t_fit = time.perf_counter() - t0
     losses = fit["col_loss"]
     us_step, flops_step = model.col_net.step_stats()
-    held = list(range(900000, 900000 + args.c4_test))
+    held = list(range(900000, 900000 + n_test))
     with ClockSampler(0) as clk:
         ev = LW.evaluate(fam, model, held, p, engine=eng)
     summ = ev.summary()
     # baselines on a subset: cold FP64 PDLP and plain (unrestarted) FP64 PDHG
-    sub = held[: args.c4_pdhg]
+    sub_ = held[:n_pdhg]
     p64 = pdhg.default_params(tol=1e-6, max_iters=1000000, precision=pdhg.PREC_FP64)
-    pp = pdhg.default_params(tol=1e-6, max_iters=args.c4_pdhg_iters, precision=pdhg.PREC_FP64,
-                             algorithm=pdhg.ALGO_PDHG)
+    pp = pdhg.default_params(tol=1e-6, max_iters=pdhg_iters, precision=pdhg.PREC_FP64, algorithm=pdhg.ALGO_PDHG)
     t64, tpl, itpl, stpl = [], [], [], []
-    for sd in sub:
+    for sd in sub_:
         rowlo, cost = fam.vectors(*fam.factors(sd))
         eng.update_vectors(cost=cost, rowlo=rowlo)
         t1 = time.perf_counter()
@@ -476,40 +513,162 @@ def run_learned(args, world):
     eng.close()
     model.close()
     warm_s = summ["warm_seconds_mean"]
+    pdhg_reached = all(s_ == pdhg.OPTIMAL for s_ in stpl)
+    fig = {
+        "workload": WORKLOADS["c4"]["label"], "m": fam.m, "n": fam.n, "nnz": int(fam.base.nnz),
+        "train_instances": n_train, "test_instances": n_test,
+        "network": "per-column and per-row 3 x 512 ReLU MLPs (shared weights)",
+        "learned_warm_mixed_s": warm_s,
+        "cold_mixed_pdlp_s": summ["cold_seconds_mean"],
+        "cold_fp64_pdlp_s": float(np.mean(t64)) if t64 else None,
+        "plain_fp64_pdhg_s": float(np.mean(tpl)) if tpl else None,
+        "plain_fp64_pdhg_iterations": float(np.mean(itpl)) if itpl else None,
+        "plain_fp64_pdhg_reached_tol": pdhg_reached, "baseline_subset": len(sub_),
+        "ratio_plain_fp64_pdhg_over_learned_warm": (float(np.mean(tpl)) / warm_s) if tpl else None,
+        "network_gain_cold_over_warm": summ["cold_seconds_mean"] / warm_s,
+        "learned": {**summ, "train_generation_s": t_gen, "train_fit_s": t_fit,
+                    "train_loss_first_last": [float(losses[0]), float(losses[-1])],
+                    "row_loss_first_last": [float(fit["row_loss"][0]), float(fit["row_loss"][-1])],
+                    "col_samples": fit["col_samples"], "row_samples": fit["row_samples"],
+                    "train_solutions_optimal": int((train.status == pdhg.OPTIMAL).sum())},
+        "note": None if pdhg_reached else "plain PDHG hit its iteration cap on some instances: its time is a lower bound",
+        "train_step_us": us_step, "train_step_flops": flops_step,
+    }
+    return fig, clk.summary()
+
+
+def run_learned(args, world):
+    """c4: the learned warm start pipeline on one GPU (replicas only)."""
+    fig, clocks = learned_figures(args.c4_train, args.c4_test, args.c4_pdhg, args.c4_pdhg_iters, args.c4_epochs)
     peak_tf = None
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
             peak_tf = float(json.load(f)["bf16_tflops"])
     except Exception:
         peak_tf = 1590.0
+    us_step, flops_step = fig["train_step_us"], fig["train_step_flops"]
     tf = flops_step / (us_step * 1e-6) / 1e12 if us_step > 0 else None
-    pdhg_reached = all(s_ == pdhg.OPTIMAL for s_ in stpl)
+    warm_s = fig["learned_warm_mixed_s"]
     line = {
         "metric": METRIC, "value": warm_s, "unit": "s", "n_gpus": world, "steps": args.c4_test, "warmup": 0,
         "ms_per_step": 1000 * warm_s, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32+f64 (PDLP), bf16 x fp32 (network)", "data": "synthetic (seeded blending family)",
-        "config": {"workload": WORKLOADS["c4"]["label"], "m": fam.m, "n": fam.n, "nnz": fam.base.nnz,
-                   "train_instances": args.c4_train, "test_instances": args.c4_test, "network": "per-column and per-row 3 x 512 ReLU MLPs (shared weights)",
+        "dtype": "f32 values + f64 iterates (PDLP), bf16 x fp32 (network)", "data": "synthetic (seeded blending family)",
+        "config": {"workload": WORKLOADS["c4"]["label"], "m": fig["m"], "n": fig["n"], "nnz": fig["nnz"],
+                   "train_instances": args.c4_train, "test_instances": args.c4_test, "network": fig["network"],
                    "tol": 1e-6, "parallelism": "single gpu"},
-        "learned": {**summ, "train_generation_s": t_gen, "train_fit_s": t_fit,
-                    "train_loss_first_last": [float(losses[0]), float(losses[-1])],
-                    "row_loss_first_last": [float(fit["row_loss"][0]), float(fit["row_loss"][-1])],
-                    "col_samples": fit["col_samples"], "row_samples": fit["row_samples"],
-                    "train_solutions_optimal": int((train.status == pdhg.OPTIMAL).sum())},
-        "baselines": {"cold_mixed_pdlp_s": summ["cold_seconds_mean"], "cold_fp64_pdlp_s": float(np.mean(t64)),
-                      "plain_fp64_pdhg_s": float(np.mean(tpl)), "plain_fp64_pdhg_iterations": float(np.mean(itpl)),
-                      "plain_fp64_pdhg_reached_tol": pdhg_reached, "subset": len(sub),
-                      "plain_fp64_pdhg_over_learned_warm": float(np.mean(tpl)) / warm_s,
-                      "note": None if pdhg_reached else
-                      "plain PDHG hit its iteration cap on some instances: its time is a lower bound"},
+        "learned": fig["learned"],
+        "baselines": {k: fig[k] for k in ("cold_mixed_pdlp_s", "cold_fp64_pdlp_s", "plain_fp64_pdhg_s",
+                                          "plain_fp64_pdhg_iterations", "plain_fp64_pdhg_reached_tol",
+                                          "baseline_subset", "ratio_plain_fp64_pdhg_over_learned_warm", "note")},
         "roofline": {"bound": "tensor", "achieved": tf, "peak": peak_tf, "unit": "TFLOP/s",
                      "frac": (tf / peak_tf) if tf else None, "traffic": None,
-                     "kernel": "column network training step (k_gemm mma.sync BF16, FP32 accumulate), 8192-sample batch",
+                     "kernel": "column network training step (k_gemm BF16, FP32 accumulate), 8192-sample batch",
                      "us_per_step": us_step, "flops_per_step": flops_step},
         "cpu_baseline": None,
-        "clocks": clk.summary(),
+        "clocks": clocks,
     }
     print(json.dumps(line))
+
+
+def run_blocks(args, local):
+    """The headline figures of the other configurations, measured in the
+    same run as the c2 line (one GPU), within the bench's time budget:
+      batch    c3: the 256 instances as one batch, time to 1e-6 for all of
+               them (mean of 2 solves after 1 warm-up), and the cold plain
+               SpMV of the block-diagonal batch matrix;
+      learned  c4: learned warm start vs cold mixed PDLP vs plain FP64 PDHG
+               (fewer training and held-out instances than --workload c4;
+               the counts are in the block);
+      c5       the badly scaled LP: one mixed and one FP64 solve;
+      c1       the 2,000 x 5,000 random LP: mean of 5 solves."""
+    import numpy as np
+    import scipy.sparse as sp
+    import torch
+
+    from nirnaya_b200 import batch as B
+    from nirnaya_b200 import lp as L
+    from nirnaya_b200 import pdhg
+
+    out = {}
+    flush = torch.empty(2 * L2_BYTES, dtype=torch.uint8, device=f"cuda:{local}")
+    # c3
+    lps = batch_instances(WORKLOADS["c3"])
+    p = pdhg.default_params(tol=1e-6, max_iters=args.max_iters)
+    t0 = time.perf_counter()
+    with B.BatchEngine(lps, local) as eng:
+        t_create = time.perf_counter() - t0
+        eng.solve(p)
+        times = []
+        for _ in range(2):
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            res, total = eng.solve(p)
+            b.record()
+            torch.cuda.synchronize()
+            times.append(a.elapsed_time(b) / 1000.0)
+    st = [r[2].status for r in res]
+    its = [r[2].iterations for r in res]
+    alg = sum(r[2].iterations * (12.0 * lp.nnz + 8 * 9 * lp.ncol + 8 * 8 * lp.nrow) for lp, r in zip(lps, res))
+    tts = float(np.mean(times))
+    out["batch"] = {"workload": WORKLOADS["c3"]["label"], "instances": len(lps),
+                    "nnz": int(sum(lp.nnz for lp in lps)), "time_to_tol_s": tts, "instances_per_s": len(lps) / tts,
+                    "create_s": t_create, "status_counts": {str(k): st.count(k) for k in sorted(set(st))},
+                    "iterations_max": int(max(its)), "iterations_median": float(np.median(its)),
+                    "rel_kkt_max": float(max(r[2].rel_kkt for r in res)),
+                    "loop_algorithmic_GBs": alg / tts / 1e9,
+                    "note": "algorithmic bytes of the iterations each instance ran, counted at FP32 values with "
+                            "FP64 vectors, over the device time of the whole solve"}
+    # the batch matrix as one block-diagonal LP: cold plain SpMV GB/s
+    Ab = sp.block_diag([sp.csc_matrix((lp.value, lp.row_index, lp.col_start), shape=(lp.nrow, lp.ncol))
+                        for lp in lps], format="csc")
+    big = L.LP(Ab.shape[0], Ab.shape[1], Ab.indptr.astype(np.int64), Ab.indices.astype(np.int32), Ab.data,
+               np.concatenate([lp.cost for lp in lps]), np.concatenate([lp.collo for lp in lps]),
+               np.concatenate([lp.colup for lp in lps]), np.concatenate([lp.rowlo for lp in lps]),
+               np.concatenate([lp.rowup for lp in lps]))
+    del Ab
+    with pdhg.Engine(big, local) as eng:
+        sp_fig = {}
+        for tr, side in ((False, "A"), (True, "At")):
+            for kname, kind, vw, xw in (("cta_f32", pdhg.K_CTA32, 4, 4), ("cta_f32val_f64x", pdhg.K_CTA_MIXED, 4, 8),
+                                        ("cta_f64", pdhg.K_CTA64, 8, 8),
+                                        ("ceiling_gather_f32", pdhg.K_CEIL_GATHER32, 4, 4)):
+                best = None
+                for cap in ((1024, 2048) if kind < pdhg.K_CEIL_GATHER64 else (0,)):
+                    us = eng.time_kernel(tr, kind, cap, reps=10, flush_l2=True)
+                    if best is None or us < best[0]:
+                        best = (us, cap)
+                by = spmv_bytes_w(big, tr, vw, xw)
+                sp_fig[f"{side}_{kname}"] = {"us": best[0], "GBs": by / (best[0] * 1e-6) / 1e9, "block_nnz": best[1]}
+        out["batch"]["spmv_cold"] = sp_fig
+    del big
+    # c4
+    fig, _ = learned_figures(args.block_c4_train, args.block_c4_test, args.block_c4_pdhg, args.c4_pdhg_iters,
+                             args.c4_epochs)
+    out["learned"] = {k: v for k, v in fig.items() if k not in ("train_step_us", "train_step_flops")}
+    # c5 and c1
+    for key in ("c5", "c1"):
+        wl = WORKLOADS[key]
+        lp = L.generate(wl["kind"], wl["seed"], **wl["kw"])
+        rec = {"workload": wl["label"]}
+        with pdhg.Engine(lp, local) as eng:
+            for tag, prec in (("mixed", pdhg.PREC_MIXED), ("fp64", pdhg.PREC_FP64)):
+                pp = pdhg.default_params(precision=prec, tol=1e-6, max_iters=args.max_iters)
+                eng.solve(pp)  # warm-up (layout tuning, graph capture)
+                ts = []
+                for _ in range(5 if key == "c1" else 1):
+                    flush.fill_(1)
+                    torch.cuda.synchronize()
+                    t1 = time.perf_counter()
+                    _, _, inf = eng.solve(pp)
+                    ts.append(time.perf_counter() - t1)
+                rec[tag] = {"seconds": float(np.mean(ts)), "status": inf.status, "iterations": inf.iterations,
+                            "iterations_fp64": inf.iterations_fp64, "rel_kkt": inf.rel_kkt,
+                            "objective": inf.objective, "parallel_groups": inf.parallel_groups}
+        out[key] = rec
+    return out
 
 
 def mlp_perf(args):
@@ -838,12 +997,18 @@ def main():
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--max-iters", type=int, default=1000000)
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0,
+                    help="reference CPU sample: half of it at 1 thread, half at all host threads")
+    ap.add_argument("--no-blocks", action="store_true",
+                    help="c2: leave out the batch (c3), learned (c4), badly scaled (c5) and c1 figures")
     ap.add_argument("--c4-train", type=int, default=4096)
     ap.add_argument("--c4-test", type=int, default=512)
     ap.add_argument("--c4-pdhg", type=int, default=16)
     ap.add_argument("--c4-pdhg-iters", type=int, default=400000)
     ap.add_argument("--c4-epochs", type=int, default=4)
+    ap.add_argument("--block-c4-train", type=int, default=512, help="c2 run's learned block: training instances")
+    ap.add_argument("--block-c4-test", type=int, default=64, help="c2 run's learned block: held-out instances")
+    ap.add_argument("--block-c4-pdhg", type=int, default=4, help="c2 run's learned block: plain-PDHG subset")
     ap.add_argument("--ref-iterations", type=int, default=0,
                     help="count the reference loop's iterations to its stopping rule (cap), then exit")
     ap.add_argument("--ref-seconds", type=float, default=600.0)
@@ -929,23 +1094,25 @@ def main():
                                       "d2h_bytes_per_step": 0}}))
             return
         lp = L.generate(wl["kind"], wl["seed"], **wl["kw"])
-        vals = []
-        for _ in range(args.warmup):
-            pass
-        res = None
-        for _ in range(args.steps):
-            res = cpu_baseline(lp, wl["label"], seconds=max(1.0, args.cpu_seconds / max(1, args.steps)))
-            if res is None:
-                print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_nirnaya.so was not built "
-                                  "from the reference sources"}))
-                return
-            vals.append(res["value"])
+        # one sample of at least 5 s per thread count, whatever --steps says:
+        # the reference runs for hours to this tolerance, so its time is the
+        # iteration count it needs over its measured rate
+        res = cpu_baseline(lp, wl["label"], seconds=max(10.0, args.cpu_seconds))
+        if res is None:
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_nirnaya.so was not built "
+                              "from the reference sources"}))
+            return
         v = res["value"]
         line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": None if v is None else 1000 * v,
                 "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded generator, include/nir_lpgen.h)",
                 "config": {"workload": wl["label"], "tol": 1e-6, "threads": res["cores"]},
+                "lower_bound": bool(res.get("lower_bound")),
+                "per_iteration_s": 1.0 / res["iterations_per_s"],
+                "how": "value = iterations the reference algorithm needs to 1e-6 relative KKT on this instance "
+                       "(counted with its bit-identical GPU restatement; a lower bound when that count did not "
+                       "reach the tolerance) / the reference's own measured iterations per second here",
                 "cpu_baseline": res,
                 "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
@@ -974,33 +1141,53 @@ def run_arm(args, wl, rank, world, local):
             print(json.dumps(batch_line(args, r, world)))
         return
     r = run_ours(args, rank, world, local)
+    blocks = {}
+    if args.workload == "c2" and world == 1 and not args.no_blocks:
+        # the other configurations' headline figures, in the same run
+        blocks = run_blocks(args, local)
     if rank != 0:
         return
+    from nirnaya_b200 import pdhg
+
     lp, infos = r["lp"], r["infos"]
     last = infos[-1]
     peak, peak_kind = peaks()
-    kt, lay = r["kt"], r["lay"]
-    # dominant kernel of the solve: mean launch time x launches, per kernel
-    # and iterate precision (FP32 chunks, FP64 chunks)
+    kt = r["kt"]
+    # dominant kernel of the solve: steady-state launch time x launches, per
+    # kernel and precision (the first phase, then the FP64 polish)
     it64 = last["iterations_fp64"]
-    it32 = last["iterations"] - it64
+    it_first = last["iterations"] - it64
+    first = WORKLOADS[args.workload]["precision"]
     kernels = {}
-    for q, (tag, w, its) in enumerate((("f32", 4, it32), ("f64", 8, it64))):
-        if kt.samples[q] == 0 or its == 0:
+    phases = [(first, it_first)] if first != pdhg.PREC_FP64 else []
+    phases.append((pdhg.PREC_FP64, it64 if first != pdhg.PREC_FP64 else last["iterations"]))
+    for prec, its in phases:
+        if its <= 0 or prec not in kt:
             continue
-        for kname, us, alg in (("k_primal", kt.primal_us[q], primal_bytes(lp, w)),
-                               ("k_dual", kt.dual_us[q], dual_bytes(lp, w))):
-            kernels[f"{kname}<{'float' if w == 4 else 'double'}>"] = {
+        vw, xw = {pdhg.PREC_FP64: (8, 8), pdhg.PREC_MIXED: (4, 8), pdhg.PREC_FP32: (4, 4)}[prec]
+        tv = "double" if vw == 8 else "float"
+        tx = "double" if xw == 8 else "float"
+        p_us, d_us, pair_us = kt[prec]
+        for kname, us, alg in (("k_primal", p_us, primal_bytes(lp, xw, vw)), ("k_dual", d_us, dual_bytes(lp, xw, vw))):
+            kernels[f"{kname}<{tv},{tx}>"] = {
                 "launch_us": us, "launches": its, "share_s": us * its * 1e-6,
                 "algorithmic_bytes_per_launch": alg, "achieved_GBs": alg / (us * 1e-6) / 1e9,
-                "iteration_us": kt.iter_us[q], "tag": tag}
+                "pair_us": pair_us}
     if kernels:
         dom_name, dom = max(kernels.items(), key=lambda kv: kv[1]["share_s"])
-    else:  # no timed chunk (a solve that ended inside its first chunk)
+    else:
         dom_name, dom = "none", {"achieved_GBs": None, "algorithmic_bytes_per_launch": None, "launch_us": None}
     achieved = dom["achieved_GBs"]
+    wl = WORKLOADS[args.workload]
     traffic = committed_traffic(f"{dom_name}:{wl['label']}")
     cpu = cpu_baseline(lp, wl["label"], seconds=args.cpu_seconds)
+    fp64 = r["fp64"]
+    if cpu and fp64 and fp64["iterations"]:
+        # seconds per iteration: the reference on the host cores vs the FP64 GPU solve
+        gpu_it_s = fp64["seconds"] / fp64["iterations"]
+        cpu["per_iteration_s"] = 1.0 / cpu["iterations_per_s"]
+        cpu["gpu_fp64_per_iteration_s"] = gpu_it_s
+        cpu["per_iteration_ratio_fp64"] = cpu["per_iteration_s"] / gpu_it_s
     line = {
         "metric": METRIC,
         "value": r["ms"] / 1000.0,
@@ -1012,33 +1199,44 @@ def run_arm(args, wl, rank, world, local):
         "higher_is_better": False,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32+f64",
+        "dtype": "f32 values + f64 iterates, f64 polish" if first == pdhg.PREC_MIXED else
+                 ("f64" if first == pdhg.PREC_FP64 else "f32"),
         "data": "synthetic (seeded generator, include/nir_lpgen.h)",
         "config": {"workload": wl["label"], "m": lp.nrow, "n": lp.ncol, "nnz": lp.nnz, "tol": 1e-6,
-                   "algorithm": "pdlp (restarted reflected Halpern PDHG)", "precision": "mixed (fp32 + fp64 polish)",
+                   "algorithm": "pdlp (restarted reflected Halpern PDHG)",
+                   "precision": "mixed: fp32 matrix values with fp64 iterates, then fp64 values (polish)",
+                   "block_nnz": r["lay"].block_nnz,
                    "parallelism": f"replicas x{world}" if world > 1 else "single gpu",
                    "l2": "flushed (2x L2 write) before every solve; inside a solve the working set stays resident"},
         "status": last["status"],
         "iterations": last["iterations"],
         "iterations_fp64": last["iterations_fp64"],
+        "fp64_iteration_share": (last["iterations_fp64"] / last["iterations"]) if last["iterations"] else None,
         "rel_kkt": last["rel_kkt"],
         "objective": last["objective"],
         "setup_s": last["setup_seconds"],
+        "fp64_solve": None if fp64 is None else {
+            **fp64, "mixed_speedup": (fp64["seconds"] / (r["ms"] / 1000.0)) if fp64["seconds"] else None,
+            "note": "the same workload with FP64 values and iterates throughout, one solve with a cold L2, "
+                    "host clock around the synchronous call"},
         "e2e": {"value": r["e2e"], "unit": "s", "h2d_bytes_per_step": lp.host_bytes(),
                 "d2h_bytes_per_step": 8 * (lp.ncol + lp.nrow)},
         "gpu_launches": r["launches"],
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                     "kernel": f"{dom_name} (fused CSR-adaptive SpMV + update), dominant by time in the solve",
+                     "kernel": f"{dom_name} (fused CTA-block SpMV + update), dominant by time in the solve",
                      "algorithmic_bytes_per_launch": dom["algorithmic_bytes_per_launch"],
                      "launch_us": dom["launch_us"],
+                     "timing": "steady state: 100 back-to-back launches on the solved state, CUDA events on "
+                               "the engine's stream (nir_pdhg_time_iteration)",
                      "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
                      "kernels": kernels,
-                     "spmv_fp32_cold_At_GBs": spmv_bytes(lp, True, 4) / (r["spmv_t_us"] * 1e-6) / 1e9,
-                     "spmv_fp32_cold_A_GBs": spmv_bytes(lp, False, 4) / (r["spmv_a_us"] * 1e-6) / 1e9},
+                     "kernel_share_sum_s": sum(k["share_s"] for k in kernels.values()),
+                     "spmv_cold": r["spmv"]},
         "cpu_baseline": cpu,
         "clocks": r["clocks"],
     }
+    line.update(blocks)
     print(json.dumps(line))
 
 

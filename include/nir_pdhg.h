@@ -64,8 +64,12 @@ enum {
 enum { NIR_ALGO_REFERENCE = 0, NIR_ALGO_PDHG = 1, NIR_ALGO_PDLP = 2 };
 
 /* Precision of matrix, iterates and SpMV.  KKT residuals, restart
- * criterion, primal weight and objective are always FP64.  MIXED = FP32
- * iterations followed by an FP64 polish phase when FP32 stalls. */
+ * criterion, primal weight and objective are always FP64, on the FP64
+ * matrix.  FP64: FP64 matrix values and iterates.  MIXED: FP32 matrix
+ * values (8 instead of 12 bytes per nonzero streamed) with FP64 iterates and
+ * accumulation, then the FP64 values as a polish when the KKT error stops
+ * improving (the iterates carry on).  FP32: FP32 values, iterates and
+ * accumulation throughout. */
 enum { NIR_PREC_FP64 = 0, NIR_PREC_MIXED = 1, NIR_PREC_FP32 = 2 };
 
 typedef struct nir_pdhg_params {
@@ -88,7 +92,8 @@ typedef struct nir_pdhg_params {
     int32_t polish_stall_checks;  /* MIXED: FP64 polish after this many checks
                                      without a 0.8x improvement of the best KKT   (40)   */
     double polish_switch_kkt;     /* MIXED: ... or as soon as KKT <= this        (0)     */
-    int32_t spmv_block_nnz;       /* nonzeros per warp row block, 1..256; 0 = autotuned (0) */
+    int32_t spmv_block_nnz;       /* nonzeros per CTA block of the SpMV: 256, 512, 1024 or
+                                     2048 (256 threads x 1, 2, 4, 8); 0 = autotuned   (0) */
     int32_t use_graphs;           /* capture launch chunks in CUDA graphs        (1)     */
     int32_t verbose;              /* 1 = one line per check on stderr            (0)     */
     int32_t restart_anchor;       /* residual the restart tests compare with: 0 = first
@@ -126,7 +131,8 @@ typedef struct nir_pdhg_info {
     double solve_seconds;         /* iterations until the returned point                 */
     double time_to_fp64_seconds;  /* when the FP64 polish began (MIXED), else 0          */
     int32_t kernel_launches;      /* engine kernels launched by this solve               */
-    int32_t pad_;
+    int32_t parallel_groups;      /* groups of parallel columns re-expressed for the solve
+                                     (each adds one row; 0 = the LP as given)             */
     int64_t iterations_to_tol;    /* NIR_ALGO_REFERENCE with tol > 0: first iteration (a
                                      multiple of 32) whose iterate has rel KKT <= tol,
                                      -1 if none; the iterates are not changed by the probe.
@@ -143,6 +149,20 @@ int nir_pdhg_default_params(nir_pdhg_params* p);
  * Errors: NIR_STATUS_INPUT_ERROR (malformed LP), NIR_STATUS_INTERNAL_ERROR
  * (no device / out of device memory). */
 int nir_pdhg_create(const nir_lp_view* lp, int device, nir_pdhg** out);
+
+/* Groups of parallel columns the handle re-expresses before a PDHG / PDLP
+ * solve: column j' joins the group of the earlier column j when both have
+ * the same row pattern and A_j' = lambda A_j + eps with max|eps| at most
+ * 1e-6 max|A_j'|.  Each group adds one row to the LP the iterations run on
+ * (x_j = v - sum lambda x_j' with x_j's bounds) and moves the split of the
+ * group out of the matrix, where PDHG cannot resolve it; the result is
+ * mapped back and its KKT error evaluated on the LP as given.  Host only,
+ * no device needed.  rep_of (ncol, or NULL): each column's representative,
+ * -1 for none; lambda (ncol, or NULL): its factor; *groups: the number of
+ * groups.  Setting NIR_PDHG_PARALLEL_COLUMNS=0 in the environment turns the
+ * re-expression off for handles created afterwards.  No counterpart in the
+ * reference (its presolve has no parallel-column rule). */
+int nir_pdhg_parallel_groups(const nir_lp_view* lp, int32_t* rep_of, double* lambda, int32_t* groups);
 
 /* Replaces cost, column and row bounds of an existing handle (same
  * matrix); NULL leaves an array unchanged.  Used by families of LPs that
@@ -180,6 +200,21 @@ int nir_pdhg_spmv(nir_pdhg* h, int transpose, int kernel, const double* x, doubl
  * in microseconds measured with CUDA events on the launching stream. */
 int nir_pdhg_time_spmv(nir_pdhg* h, int transpose, int kernel, int reps, int flush_l2, double* usec);
 
+/* The same two, with more kernel kinds and the CTA-block capacity:
+ *   0-2  as nir_pdhg_spmv (block_nnz ignored)
+ *   3    CTA-block SpMV (segmented reduction, aligned 128-bit stream loads), FP64
+ *   4    CTA-block SpMV, FP32 values, x and accumulation
+ *   5    CTA-block SpMV, FP32 values with FP64 x and accumulation
+ *   6-9  (timing only) the row-less ceilings: the stream of indices and
+ *        values with the gathers of x (6 FP64, 7 FP32) or without them
+ *        (8 FP64, 9 FP32), with no row structure at all
+ * block_nnz: CTA-block capacity for 3-5 (256, 512, 1024 or 2048; 0 = 2048).
+ * No counterpart in the reference: measurement of the SpMV kernels that
+ * replace CscMatrix::spmv / spmv_transpose (src/core/csc_matrix.hpp:99-120). */
+int nir_pdhg_spmv_kernel(nir_pdhg* h, int transpose, int kernel, int block_nnz, const double* x, double* y);
+int nir_pdhg_time_kernel(nir_pdhg* h, int transpose, int kernel, int block_nnz, int reps, int flush_l2,
+                         double* usec);
+
 typedef struct nir_pdhg_kernel_time {
     /* index 0: chunks iterating in FP32, index 1: chunks iterating in FP64 */
     double primal_us[2]; /* mean duration of the fused A'y + primal-update kernel */
@@ -193,6 +228,17 @@ typedef struct nir_pdhg_kernel_time {
 int nir_pdhg_set_profiling(nir_pdhg* h, int on);
 int nir_pdhg_kernel_times(nir_pdhg* h, nir_pdhg_kernel_time* out);
 
+/* Steady-state CUDA-event timing of the two fused iteration kernels (A' y
+ * + primal step, A x-bar + dual step) after a PDHG/PDLP solve on this handle:
+ * `reps` back-to-back launches of each kernel alone and of the pair, on the
+ * last solve's layout and state.  precision: NIR_PREC_FP64 (FP64 values and
+ * iterates), NIR_PREC_MIXED (FP32 values, FP64 iterates) or NIR_PREC_FP32.
+ * The kernels overwrite the handle's iterates (not x_out / y_out of the
+ * solve, nor the point nir_pdhg_verify checks); the next solve starts anew.
+ * No counterpart in the reference. */
+int nir_pdhg_time_iteration(nir_pdhg* h, int precision, int reps, double* primal_us, double* dual_us,
+                            double* pair_us);
+
 /* KKT history of the last PDHG/PDLP solve, one entry per check, oldest
  * first: 8 doubles per entry (iteration, rel KKT, rel primal, rel dual,
  * rel gap, fixed-point residual, primal weight, phase).  Returns the number
@@ -203,8 +249,8 @@ int nir_pdhg_history(nir_pdhg* h, double* out, int max_entries);
 typedef struct nir_pdhg_layout {
     int32_t nrow, ncol;
     int64_t nnz;
-    int32_t blocks_a, blocks_at;        /* CSR-adaptive row blocks of A and A' */
-    int32_t block_nnz;                  /* row-block capacity in nonzeros      */
+    int32_t blocks_a, blocks_at;        /* CTA blocks of A and A' of the last solve */
+    int32_t block_nnz;                  /* their capacity in nonzeros             */
     int64_t device_bytes;               /* device memory held by the handle    */
 } nir_pdhg_layout;
 int nir_pdhg_get_layout(nir_pdhg* h, nir_pdhg_layout* out);

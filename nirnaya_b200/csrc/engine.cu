@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <limits>
 #include <memory>
 #include <mutex>
@@ -31,6 +32,8 @@
 #include "k_reference.cuh"
 #include "k_setup.cuh"
 #include "k_verify.cuh"
+#include "k_cta.cuh"
+#include "k_iter.cuh"
 #include "k_batch.cuh"
 #include "nir_pdhg.h"
 
@@ -99,6 +102,14 @@ struct DevBuf {
     size_t bytes = 0;
 };
 
+// Groups of parallel columns of an LP (engine_parallel.cuh).
+struct ParallelGroups {
+    std::vector<int> rep_of;  // per column: its representative, or -1
+    std::vector<double> lam;  // per partner column: lambda (A_j' ~ lambda A_rep)
+    std::vector<int> row_of;  // per representative: its new row (>= m), or -1
+    int groups = 0;
+};
+
 }  // namespace
 
 // ---------------------------------------------------------------- handle
@@ -121,6 +132,25 @@ struct Orient {
         int2* blk;
     };
     std::vector<Layout> layouts;  // every layout built so far, one per capacity used
+    // CTA-block layouts (k_cta.cuh), one per capacity used: descriptors and
+    // the padded stream of indices and values.  `it` is the one the
+    // iteration and KKT kernels use (a deque keeps references stable).
+    struct Cta {
+        int cap = 0, nblk = 0;
+        long long qlen = 0;
+        int4* blk = nullptr;
+        int* ci = nullptr;
+        double* v64 = nullptr;     // scaled FP64 values (refreshed after each preconditioning)
+        float* v32 = nullptr;      // scaled FP32 values
+        double* vorig = nullptr;   // original values (kernel measurement entry points, on demand)
+        float* v32orig = nullptr;  // original values rounded to FP32
+    };
+    std::deque<Cta> ctas;
+    int it = -1;
+    const Cta& cur() const {
+        if (it < 0) throw std::logic_error("internal: no CTA layout in use");
+        return ctas[size_t(it)];
+    }
 };
 
 struct Snapshot {
@@ -163,11 +193,13 @@ struct nir_pdhg {
     Snapshot snap;
     unsigned char* flush = nullptr;
     size_t flush_bytes = 0;
+    double* ceil_out = nullptr;        // one running sum per thread of the ceiling kernels
+    nir::DevState* st_time = nullptr;  // running copy of the state for nir_pdhg_time_iteration
     std::vector<DevBuf> bufs;
     long long device_bytes = 0;
     ChunkGraph graphs[3];
     long long last_iters = 0;
-    int tuned_cap[2] = {0, 0};  // autotuned warp row-block capacity (FP32, FP64)
+    int tuned_cap[3] = {0, 0, 0};  // autotuned CTA-block capacity per NIR_PREC_*
     int sms = 148;
     struct Occ {
         const void* fn;
@@ -182,6 +214,10 @@ struct nir_pdhg {
     int* gs_err = nullptr;
     int launches = 0;
     const double* last_x = nullptr;  // the point the last solve returned, still on the device (null before one)
+    // the equivalent LP the PDHG / PDLP solves run on when the LP has
+    // parallel columns (engine_parallel.cuh), and its column groups
+    std::unique_ptr<nir_pdhg> inner;
+    std::unique_ptr<ParallelGroups> par;
     // the device solution check's buffers, allocated by its first call
     struct Verify {
         bool ready = false;
@@ -223,6 +259,7 @@ struct nir_pdhg {
         for (auto& b : bufs) cudaFree(b.p);
         if (snap.ring) cudaFreeHost(snap.ring);
         if (stream) cudaStreamDestroy(stream);
+        inner.reset();
     }
 };
 
@@ -263,6 +300,66 @@ void set_blocks(nir_pdhg* h, Orient& o, int cap) {
     h2d(h, o.blk, b.data(), b.size() * sizeof(int2));
     o.cap = cap;
     o.layouts.push_back({cap, o.nblk, o.blk});
+}
+
+// The CTA-block layout of an orientation for capacity `cap` (256 E), built
+// on first use: descriptors checked on the host, then the padded stream of
+// column indices filled on the device; the value streams are filled by
+// pad_scaled (scaled values) or cta_orig_values (original values).
+Orient::Cta& cta_layout(nir_pdhg* h, Orient& o, int cap) {
+    for (auto& c : o.ctas)
+        if (c.cap == cap) return c;
+    std::vector<int4> b = nir::build_cta_blocks(o.h_rp, cap);
+    nir::check_cta_blocks(b, o.h_rp, cap);
+    Orient::Cta c;
+    c.cap = cap;
+    c.nblk = int(b.size()) - 1;
+    c.qlen = b.back().z;
+    c.blk = h->alloc<int4>(b.size());
+    h2d(h, c.blk, b.data(), b.size() * sizeof(int4));
+    // 8 spare entries keep every allocation non-empty
+    c.ci = h->allocz<int>(size_t(c.qlen), 8);
+    c.v64 = h->allocz<double>(size_t(c.qlen), 8);
+    c.v32 = h->allocz<float>(size_t(c.qlen), 8);
+    cudaStream_t s = h->stream;
+    if (c.nblk > 0 && o.nnz > 0) {
+        const unsigned g = unsigned(std::max(1, std::min(c.nblk, 4 * h->sms)));
+        nir::k_pad_stream<double><<<g, nir::kBlock, 0, s>>>(c.blk, c.nblk, o.ci, o.v_orig, c.ci, c.v64);
+        NIR_LAUNCHED();
+    }
+    NIR_CUDA(cudaStreamSynchronize(s));
+    o.ctas.push_back(c);
+    return o.ctas.back();
+}
+
+// The original values in a CTA layout's padded stream (FP64 and rounded to
+// FP32), for the kernel measurement entry points.
+void cta_orig_values(nir_pdhg* h, Orient& o, Orient::Cta& c) {
+    if (c.vorig) return;
+    cudaStream_t s = h->stream;
+    c.vorig = h->allocz<double>(size_t(c.qlen), 8);
+    c.v32orig = h->allocz<float>(size_t(c.qlen), 8);
+    if (c.nblk > 0 && o.nnz > 0) {
+        if (!o.v32_orig) {
+            o.v32_orig = h->allocz<float>(o.nnz);
+            nir::k_to_float<<<grid_for(o.nnz), nir::kBlock, 0, s>>>(o.nnz, o.v_orig, o.v32_orig);
+            NIR_LAUNCHED();
+        }
+        const unsigned g = unsigned(std::max(1, std::min(c.nblk, 4 * h->sms)));
+        nir::k_pad_stream<double><<<g, nir::kBlock, 0, s>>>(c.blk, c.nblk, o.ci, o.v_orig, nullptr, c.vorig);
+        nir::k_pad_stream<float><<<g, nir::kBlock, 0, s>>>(c.blk, c.nblk, o.ci, o.v32_orig, nullptr, c.v32orig);
+        NIR_LAUNCHED();
+    }
+    NIR_CUDA(cudaStreamSynchronize(s));
+}
+
+// CTA-block capacity without timing: the largest of 256 E (E = 1, 2, 4, 8)
+// that still gives every SM about four blocks.
+int auto_cta_cap(const nir_pdhg* h) {
+    const long long per = h->nnz / (4LL * std::max(h->sms, 1));
+    int cap = 256;
+    while (cap < 2048 && cap * 2 <= per) cap *= 2;
+    return cap;
 }
 
 // Warp row-block capacity: 256 nonzeros (8 per lane) when the matrix gives
@@ -516,13 +613,12 @@ PartLayout part_layout(nir_pdhg* h) {
 
 // ---------------------------------------------------------------- precision views
 
-template <typename T>
-struct View;
+// Iterate vectors by type: FP32 (x32 ...) or FP64 (x64 ...).
+template <typename TX>
+struct Vec;
 
 template <>
-struct View<float> {
-    static const float* valA(nir_pdhg* h) { return h->A.v32; }
-    static const float* valAt(nir_pdhg* h) { return h->At.v32; }
+struct Vec<float> {
     static float* x(nir_pdhg* h) { return h->x32; }
     static float* xb(nir_pdhg* h) { return h->xb32; }
     static float* x0(nir_pdhg* h) { return h->x032; }
@@ -538,9 +634,7 @@ struct View<float> {
 };
 
 template <>
-struct View<double> {
-    static const double* valA(nir_pdhg* h) { return h->A.v64; }
-    static const double* valAt(nir_pdhg* h) { return h->At.v64; }
+struct Vec<double> {
     static double* x(nir_pdhg* h) { return h->x64; }
     static double* xb(nir_pdhg* h) { return h->xb64; }
     static double* x0(nir_pdhg* h) { return h->x064; }
@@ -554,6 +648,101 @@ struct View<double> {
     static const double* rl(nir_pdhg* h) { return h->rl64; }
     static const double* ru(nir_pdhg* h) { return h->ru64; }
 };
+
+// Scaled values of a CTA layout's padded stream by type.
+template <typename TV>
+const TV* vals(const Orient::Cta& L);
+template <>
+const float* vals<float>(const Orient::Cta& L) {
+    return L.v32;
+}
+template <>
+const double* vals<double>(const Orient::Cta& L) {
+    return L.v64;
+}
+
+// Persistent grid of a CTA-block kernel: the resident CTAs, at most one per
+// block.  The occupancy query runs once per kernel (outside any capture).
+template <typename K>
+int cta_grid(nir_pdhg* h, K* kernel, int nblk) {
+    int per = 0;
+    for (auto& e : h->occ)
+        if (e.fn == (const void*)kernel && e.smem == 0) per = e.per_sm;
+    if (per == 0) {
+        NIR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, nir::kBlock, 0));
+        per = std::max(per, 1);
+        h->occ.push_back({(const void*)kernel, 0, per});
+    }
+    return std::max(1, std::min(nblk, per * h->sms));
+}
+
+// Run length of a CTA-block capacity.
+inline int run_len(int cap) {
+    if (cap != 256 && cap != 512 && cap != 1024 && cap != 2048)
+        throw std::invalid_argument("CTA block capacity must be 256, 512, 1024 or 2048");
+    return cap / nir::kBlock;
+}
+
+// Calls f(std::integral_constant<int, E>{}) for the run length of cap.
+template <class F>
+void with_run_len(int cap, F&& f) {
+    switch (run_len(cap)) {
+        case 1: f(std::integral_constant<int, 1>{}); break;
+        case 2: f(std::integral_constant<int, 2>{}); break;
+        case 4: f(std::integral_constant<int, 4>{}); break;
+        default: f(std::integral_constant<int, 8>{}); break;
+    }
+}
+
+// The CTA layouts the iteration kernels use: capacity `cap` in both
+// orientations (built on first use).
+void use_cta(nir_pdhg* h, int cap) {
+    for (Orient* o : {&h->A, &h->At}) {
+        cta_layout(h, *o, cap);
+        for (size_t k = 0; k < o->ctas.size(); ++k)
+            if (o->ctas[k].cap == cap) o->it = int(k);
+    }
+}
+
+// Copies the scaled values (written by precondition) into the padded
+// streams of the layouts in use.
+void pad_scaled(nir_pdhg* h) {
+    cudaStream_t s = h->stream;
+    for (Orient* o : {&h->A, &h->At}) {
+        const Orient::Cta& L = o->cur();
+        if (L.nblk <= 0 || o->nnz <= 0) continue;
+        const unsigned g = unsigned(std::max(1, std::min(L.nblk, 4 * h->sms)));
+        nir::k_pad_stream<double><<<g, nir::kBlock, 0, s>>>(L.blk, L.nblk, o->ci, o->v64, nullptr, L.v64);
+        nir::k_pad_stream<float><<<g, nir::kBlock, 0, s>>>(L.blk, L.nblk, o->ci, o->v32, nullptr, L.v32);
+        NIR_LAUNCHED();
+        h->launches += 2;
+    }
+}
+
+// The two FP64 KKT passes of a check over the layouts in use, at (xp, yp)
+// of type TX; returns their grids (the number of partials each wrote).
+template <typename TX, int E>
+void launch_kkt_e(nir_pdhg* h, int phase, double* partKR, double* partKC, const TX* xp, const TX* yp, int* gkr,
+                  int* gkc) {
+    cudaStream_t s = h->stream;
+    const Orient::Cta& LA = h->A.cur();
+    const Orient::Cta& LT = h->At.cur();
+    *gkr = cta_grid(h, nir::k_kkt_rows<TX, E>, LA.nblk);
+    *gkc = cta_grid(h, nir::k_kkt_cols<TX, E>, LT.nblk);
+    nir::KktArgs kr{LA.blk, LA.nblk, h->A.rp, LA.ci, LA.v64, partKR, h->st, phase};
+    nir::k_kkt_rows<TX, E><<<*gkr, nir::kBlock, 0, s>>>(kr, xp, yp, h->dr, h->rl, h->ru);
+    nir::KktArgs kc{LT.blk, LT.nblk, h->At.rp, LT.ci, LT.v64, partKC, h->st, phase};
+    nir::k_kkt_cols<TX, E><<<*gkc, nir::kBlock, 0, s>>>(kc, xp, yp, h->dc, h->c, h->l, h->u);
+    NIR_LAUNCHED();
+    h->launches += 2;
+}
+
+template <typename TX>
+void launch_kkt(nir_pdhg* h, int phase, double* partKR, double* partKC, const TX* xp, const TX* yp, int* gkr,
+                int* gkc) {
+    with_run_len(h->A.cur().cap,
+                 [&](auto e) { launch_kkt_e<TX, decltype(e)::value>(h, phase, partKR, partKC, xp, yp, gkr, gkc); });
+}
 
 struct SolveCfg {
     nir_pdhg_params p;
@@ -571,90 +760,84 @@ struct ChunkTimer {
     cudaEvent_t e[4] = {nullptr, nullptr, nullptr, nullptr};
     bool armed = false;
     int K = 1;
-    int prec = 0;  // 0: the timed chunk iterates in FP32, 1: FP64
+    int prec = 0;  // 0: the timed chunk streams FP32 values, 1: FP64
 };
 
-template <typename T>
-void launch_fast_chunk(nir_pdhg* h, const SolveCfg& cfg, int phase, ChunkTimer* tm) {
-    if (tm) tm->prec = (sizeof(T) == 8) ? 1 : 0;
+// One launch chunk: K iterations (the last one a check), the KKT passes,
+// the controller, the restart copy and the status snapshot.  TV = type of
+// the matrix values, TX = type of the iterates, E = run length.
+template <typename TV, typename TX, int E>
+void launch_fast_chunk_e(nir_pdhg* h, const SolveCfg& cfg, int phase, ChunkTimer* tm) {
+    if (tm) tm->prec = (sizeof(TV) == 8) ? 1 : 0;
     cudaStream_t s = h->stream;
     const PartLayout L = part_layout(h);
     const int K = cfg.K;
-    const int cap = h->A.cap;
-    const LaunchCfg cp1 = warp_cfg<T>(h, nir::k_primal<T, true>, h->At.nblk);
-    const LaunchCfg cp0 = warp_cfg<T>(h, nir::k_primal<T, false>, h->At.nblk);
-    const LaunchCfg cd1 = warp_cfg<T>(h, nir::k_dual<T, true>, h->A.nblk);
-    const LaunchCfg cd0 = warp_cfg<T>(h, nir::k_dual<T, false>, h->A.nblk);
-    const LaunchCfg ckr = warp_cfg<double>(h, nir::k_kkt_rows<T>, h->A.nblk);
-    const LaunchCfg ckc = warp_cfg<double>(h, nir::k_kkt_cols<T>, h->At.nblk);
-    const size_t smem = cp1.smem, smem64 = ckr.smem;
+    const Orient::Cta& LA = h->A.cur();
+    const Orient::Cta& LT = h->At.cur();
+    const int gp1 = cta_grid(h, nir::k_primal<TV, TX, E, true>, LT.nblk);
+    const int gp0 = cta_grid(h, nir::k_primal<TV, TX, E, false>, LT.nblk);
+    const int gd1 = cta_grid(h, nir::k_dual<TV, TX, E, true>, LA.nblk);
+    const int gd0 = cta_grid(h, nir::k_dual<TV, TX, E, false>, LA.nblk);
     int i_first = 0;
     if (cfg.persistent && K > 1) {
         // iterations 0..K-2 in one cooperative launch; the check pair below
-        const LaunchCfg pc = warp_cfg<T>(h, nir::k_chunk<T>, std::max(h->A.nblk, h->At.nblk));
-        nir::IterArgs ap{h->At.blk, h->At.nblk, cap, h->At.rp, h->At.ci, L.P, h->st, 0, cfg.halpern, phase,
-                         cfg.p.reflection};
-        nir::IterArgs ad{h->A.blk, h->A.nblk, cap, h->A.rp, h->A.ci, L.D, h->st, 0, cfg.halpern, phase,
-                         cfg.p.reflection};
-        nir::ChunkPtrs<T> v{View<T>::valAt(h), View<T>::valA(h), View<T>::x(h), View<T>::xb(h), View<T>::xp(h),
-                            View<T>::y(h),     View<T>::yp(h),   View<T>::c(h), View<T>::l(h),  View<T>::u(h),
-                            View<T>::x0(h),    View<T>::rl(h),   View<T>::ru(h), View<T>::y0(h)};
+        const int gc = cta_grid(h, nir::k_chunk<TV, TX, E>, std::max(LA.nblk, LT.nblk));
+        nir::IterArgs ap{LT.blk, LT.nblk, h->At.rp, LT.ci, L.P, h->st, 0, cfg.halpern, phase, cfg.p.reflection};
+        nir::IterArgs ad{LA.blk, LA.nblk, h->A.rp, LA.ci, L.D, h->st, 0, cfg.halpern, phase, cfg.p.reflection};
+        nir::ChunkPtrs<TV, TX> v{vals<TV>(LT),   vals<TV>(LA),   Vec<TX>::x(h),  Vec<TX>::xb(h), Vec<TX>::xp(h),
+                                 Vec<TX>::y(h),  Vec<TX>::yp(h), Vec<TX>::c(h),  Vec<TX>::l(h),  Vec<TX>::u(h),
+                                 Vec<TX>::x0(h), Vec<TX>::rl(h), Vec<TX>::ru(h), Vec<TX>::y0(h)};
         // ~1 s of SM clock per wait; 0.1 s and one CTA too many in the test
-        nir::GridSync gs{h->gs_count, h->gs_gen, h->gs_err, unsigned(pc.grid) + (cfg.barrier_test ? 1u : 0u),
+        nir::GridSync gs{h->gs_count, h->gs_gen, h->gs_err, unsigned(gc) + (cfg.barrier_test ? 1u : 0u),
                          cfg.barrier_test ? 200000000LL : 2000000000LL};
         nir::DevState* st = h->st;
         int i0 = 0, iters = K - 1;
         void* args[] = {&ap, &ad, &v, &i0, &iters, &gs, &st};
-        NIR_CUDA(cudaLaunchCooperativeKernel((const void*)nir::k_chunk<T>, dim3(pc.grid), dim3(nir::kBlock), args,
-                                             pc.smem, s));
+        NIR_CUDA(cudaLaunchCooperativeKernel((const void*)nir::k_chunk<TV, TX, E>, dim3(gc), dim3(nir::kBlock), args,
+                                             0, s));
         h->launches += 1;
         i_first = K - 1;
     }
     for (int i = i_first; i < K; ++i) {
         const bool check = (i == K - 1);
-        nir::IterArgs ap{h->At.blk, h->At.nblk, cap, h->At.rp, h->At.ci, L.P, h->st, i, cfg.halpern, phase,
-                         cfg.p.reflection};
-        nir::IterArgs ad{h->A.blk, h->A.nblk, cap, h->A.rp, h->A.ci, L.D, h->st, i, cfg.halpern, phase,
-                         cfg.p.reflection};
+        nir::IterArgs ap{LT.blk, LT.nblk, h->At.rp, LT.ci, L.P, h->st, i, cfg.halpern, phase, cfg.p.reflection};
+        nir::IterArgs ad{LA.blk, LA.nblk, h->A.rp, LA.ci, L.D, h->st, i, cfg.halpern, phase, cfg.p.reflection};
         const bool timed = tm && tm->armed && i == 0 && !cfg.persistent;
         if (timed) NIR_CUDA(cudaEventRecord(tm->e[0], s));
         if (check)
-            nir::k_primal<T, true><<<cp1.grid, nir::kBlock, smem, s>>>(
-                ap, View<T>::valAt(h), View<T>::y(h), View<T>::x(h), View<T>::xb(h), View<T>::xp(h), View<T>::c(h),
-                View<T>::l(h), View<T>::u(h), View<T>::x0(h));
+            nir::k_primal<TV, TX, E, true><<<gp1, nir::kBlock, 0, s>>>(
+                ap, vals<TV>(LT), Vec<TX>::y(h), Vec<TX>::x(h), Vec<TX>::xb(h), Vec<TX>::xp(h), Vec<TX>::c(h),
+                Vec<TX>::l(h), Vec<TX>::u(h), Vec<TX>::x0(h));
         else
-            nir::k_primal<T, false><<<cp0.grid, nir::kBlock, smem, s>>>(
-                ap, View<T>::valAt(h), View<T>::y(h), View<T>::x(h), View<T>::xb(h), View<T>::xp(h), View<T>::c(h),
-                View<T>::l(h), View<T>::u(h), View<T>::x0(h));
+            nir::k_primal<TV, TX, E, false><<<gp0, nir::kBlock, 0, s>>>(
+                ap, vals<TV>(LT), Vec<TX>::y(h), Vec<TX>::x(h), Vec<TX>::xb(h), Vec<TX>::xp(h), Vec<TX>::c(h),
+                Vec<TX>::l(h), Vec<TX>::u(h), Vec<TX>::x0(h));
         NIR_LAUNCHED();
         if (timed) NIR_CUDA(cudaEventRecord(tm->e[1], s));
         if (check)
-            nir::k_dual<T, true><<<cd1.grid, nir::kBlock, smem, s>>>(ad, View<T>::valA(h), View<T>::xb(h), View<T>::y(h),
-                                                                      View<T>::yp(h), View<T>::rl(h), View<T>::ru(h),
-                                                                      View<T>::y0(h));
+            nir::k_dual<TV, TX, E, true><<<gd1, nir::kBlock, 0, s>>>(ad, vals<TV>(LA), Vec<TX>::xb(h), Vec<TX>::y(h),
+                                                                     Vec<TX>::yp(h), Vec<TX>::rl(h), Vec<TX>::ru(h),
+                                                                     Vec<TX>::y0(h));
         else
-            nir::k_dual<T, false><<<cd0.grid, nir::kBlock, smem, s>>>(ad, View<T>::valA(h), View<T>::xb(h), View<T>::y(h),
-                                                                       View<T>::yp(h), View<T>::rl(h), View<T>::ru(h),
-                                                                       View<T>::y0(h));
+            nir::k_dual<TV, TX, E, false><<<gd0, nir::kBlock, 0, s>>>(ad, vals<TV>(LA), Vec<TX>::xb(h), Vec<TX>::y(h),
+                                                                      Vec<TX>::yp(h), Vec<TX>::rl(h), Vec<TX>::ru(h),
+                                                                      Vec<TX>::y0(h));
         NIR_LAUNCHED();
         if (timed) NIR_CUDA(cudaEventRecord(tm->e[2], s));
         h->launches += 2;
     }
-    nir::KktArgs kr{h->A.blk, h->A.nblk, cap, h->A.rp, h->A.ci, h->A.v64, L.KR, h->st, phase};
-    nir::k_kkt_rows<T><<<ckr.grid, nir::kBlock, smem64, s>>>(kr, View<T>::xp(h), View<T>::yp(h), h->dr, h->rl, h->ru);
-    NIR_LAUNCHED();
-    nir::KktArgs kc{h->At.blk, h->At.nblk, cap, h->At.rp, h->At.ci, h->At.v64, L.KC, h->st, phase};
-    nir::k_kkt_cols<T><<<ckc.grid, nir::kBlock, smem64, s>>>(kc, View<T>::xp(h), View<T>::yp(h), h->dc, h->c, h->l, h->u);
-    NIR_LAUNCHED();
+    int gkr = 0, gkc = 0;
+    launch_kkt_e<TX, E>(h, phase, L.KR, L.KC, Vec<TX>::xp(h), Vec<TX>::yp(h), &gkr, &gkc);
+    h->launches -= 2;  // counted with the chunk below
     nir::CtlArgs ca;
     ca.partP = L.P;
     ca.partD = L.D;
     ca.partKR = L.KR;
     ca.partKC = L.KC;
-    ca.nP = cp1.grid;
-    ca.nD = cd1.grid;
-    ca.nKR = ckr.grid;
-    ca.nKC = ckc.grid;
+    ca.nP = gp1;
+    ca.nD = gd1;
+    ca.nKR = gkr;
+    ca.nKC = gkc;
     ca.bnorm = cfg.bnorm;
     ca.cnorm = cfg.cnorm;
     ca.offset = h->offset;
@@ -676,9 +859,9 @@ void launch_fast_chunk(nir_pdhg* h, const SolveCfg& cfg, int phase, ChunkTimer* 
     nir::k_control<<<1, nir::kBlock, 0, s>>>(ca, h->st);
     NIR_LAUNCHED();
     const int nm = std::max(h->n, h->m);
-    nir::k_apply_restart<T><<<grid_for(nm), nir::kBlock, 0, s>>>(h->n, h->m, h->st, phase, View<T>::x(h), View<T>::x0(h),
-                                                                  View<T>::xp(h), View<T>::y(h), View<T>::y0(h),
-                                                                  View<T>::yp(h));
+    nir::k_apply_restart<TX><<<grid_for(nm), nir::kBlock, 0, s>>>(h->n, h->m, h->st, phase, Vec<TX>::x(h),
+                                                                   Vec<TX>::x0(h), Vec<TX>::xp(h), Vec<TX>::y(h),
+                                                                   Vec<TX>::y0(h), Vec<TX>::yp(h));
     NIR_LAUNCHED();
     nir::k_snap<<<1, 32, 0, s>>>(h->st, h->snap.ring, h->snap.d_seq);
     NIR_LAUNCHED();
@@ -686,15 +869,25 @@ void launch_fast_chunk(nir_pdhg* h, const SolveCfg& cfg, int phase, ChunkTimer* 
     h->launches += 5;
 }
 
+template <typename TV, typename TX>
+void launch_fast_chunk(nir_pdhg* h, const SolveCfg& cfg, int phase, ChunkTimer* tm) {
+    with_run_len(h->A.cur().cap, [&](auto e) { launch_fast_chunk_e<TV, TX, decltype(e)::value>(h, cfg, phase, tm); });
+}
+
 // Runs the occupancy queries of a chunk's kernels before any capture.
-template <typename T>
+template <typename TV, typename TX>
 void warm_cfgs(nir_pdhg* h) {
-    warp_cfg<T>(h, nir::k_primal<T, true>, h->At.nblk);
-    warp_cfg<T>(h, nir::k_primal<T, false>, h->At.nblk);
-    warp_cfg<T>(h, nir::k_dual<T, true>, h->A.nblk);
-    warp_cfg<T>(h, nir::k_dual<T, false>, h->A.nblk);
-    warp_cfg<double>(h, nir::k_kkt_rows<T>, h->A.nblk);
-    warp_cfg<double>(h, nir::k_kkt_cols<T>, h->At.nblk);
+    with_run_len(h->A.cur().cap, [&](auto e) {
+        constexpr int E = decltype(e)::value;
+        const int na = h->A.cur().nblk, nt = h->At.cur().nblk;
+        cta_grid(h, nir::k_primal<TV, TX, E, true>, nt);
+        cta_grid(h, nir::k_primal<TV, TX, E, false>, nt);
+        cta_grid(h, nir::k_dual<TV, TX, E, true>, na);
+        cta_grid(h, nir::k_dual<TV, TX, E, false>, na);
+        cta_grid(h, nir::k_kkt_rows<TX, E>, na);
+        cta_grid(h, nir::k_kkt_cols<TX, E>, nt);
+        cta_grid(h, nir::k_chunk<TV, TX, E>, std::max(na, nt));
+    });
 }
 
 // Identity of everything a captured chunk bakes into its kernel arguments
@@ -712,12 +905,14 @@ struct KeyHash {
     }
 };
 
-unsigned long long chunk_key(const nir_pdhg* h, const SolveCfg& c, int phase, bool f64) {
+// prec: 0 = FP32 values and iterates, 1 = FP32 values with FP64 iterates,
+// 2 = FP64 values and iterates.
+unsigned long long chunk_key(const nir_pdhg* h, const SolveCfg& c, int phase, int prec) {
     KeyHash k;
-    k.add(phase).add(f64).add(c.K).add(c.halpern).add(c.restarts).add(c.mixed).add(c.bnorm).add(c.cnorm);
+    k.add(phase).add(prec).add(c.K).add(c.halpern).add(c.restarts).add(c.mixed).add(c.bnorm).add(c.cnorm);
     k.add(c.p.reflection).add(c.p.restart_sufficient).add(c.p.restart_necessary).add(c.p.restart_artificial);
     k.add(c.p.primal_weight_smoothing).add(c.p.polish_stall_checks).add(c.p.polish_switch_kkt).add(c.p.tol);
-    k.add(c.p.feas_tol).add(c.p.restart_anchor).add(c.p.primal_weight_decades).add(c.p.polish_fresh).add(h->offset).add(h->A.cap).add(h->A.blk).add(h->At.blk).add(h->part).add(h->hist);
+    k.add(c.p.feas_tol).add(c.p.restart_anchor).add(c.p.primal_weight_decades).add(c.p.polish_fresh).add(h->offset).add(h->A.cur().cap).add(h->A.cur().blk).add(h->At.cur().blk).add(h->part).add(h->hist);
     k.add(c.persistent).add(c.barrier_test);
     return k.h;
 }
@@ -748,16 +943,12 @@ void launch_ref_chunk(nir_pdhg* h, int K, const RefProbe* probe) {
     }
     if (probe) {
         // KKT of (x, y) on the unscaled matrix (dr = dc = 1): reads only
-        const LaunchCfg ckr = warp_cfg<double>(h, nir::k_kkt_rows<double>, h->A.nblk);
-        const LaunchCfg ckc = warp_cfg<double>(h, nir::k_kkt_cols<double>, h->At.nblk);
-        nir::KktArgs kr{h->A.blk, h->A.nblk, h->A.cap, h->A.rp, h->A.ci, h->A.v64, L.KR, h->st, 0};
-        nir::k_kkt_rows<double><<<ckr.grid, nir::kBlock, ckr.smem, s>>>(kr, h->x64, h->y64, h->dr, h->rl, h->ru);
-        nir::KktArgs kc{h->At.blk, h->At.nblk, h->At.cap, h->At.rp, h->At.ci, h->At.v64, L.KC, h->st, 0};
-        nir::k_kkt_cols<double><<<ckc.grid, nir::kBlock, ckc.smem, s>>>(kc, h->x64, h->y64, h->dc, h->c, h->l, h->u);
-        nir::k_ref_probe<<<1, nir::kBlock, 0, s>>>(L.KR, ckr.grid, L.KC, ckc.grid, probe->bnorm, probe->cnorm,
-                                                   h->offset, probe->tol, h->st);
+        int gkr = 0, gkc = 0;
+        launch_kkt<double>(h, 0, L.KR, L.KC, h->x64, h->y64, &gkr, &gkc);
+        nir::k_ref_probe<<<1, nir::kBlock, 0, s>>>(L.KR, gkr, L.KC, gkc, probe->bnorm, probe->cnorm, h->offset,
+                                                   probe->tol, h->st);
         NIR_LAUNCHED();
-        h->launches += 3;
+        h->launches += 1;
     }
     nir::k_snap<<<1, 32, 0, s>>>(h->st, h->snap.ring, h->snap.d_seq);
     NIR_LAUNCHED();
@@ -906,12 +1097,14 @@ int solve_reference(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), v
     const bool probing = p.tol > 0.0;
     RefProbe probe{0.0, 0.0, p.tol};
     if (probing) {
+        use_cta(h, auto_cta_cap(h));
         precondition(h, p, false);
-        const int cap = auto_cap(h->nnz, std::max(h->m, h->n));
-        set_blocks(h, h->A, cap);
-        set_blocks(h, h->At, cap);
-        warp_cfg<double>(h, nir::k_kkt_rows<double>, h->A.nblk);
-        warp_cfg<double>(h, nir::k_kkt_cols<double>, h->At.nblk);
+        pad_scaled(h);
+        with_run_len(h->A.cur().cap, [&](auto e) {
+            constexpr int E = decltype(e)::value;
+            cta_grid(h, nir::k_kkt_rows<double, E>, h->A.cur().nblk);
+            cta_grid(h, nir::k_kkt_cols<double, E>, h->At.cur().nblk);
+        });
         probe.bnorm = rhs_norm(h);
         probe.cnorm = norm2(h->h_c);
     }
@@ -939,7 +1132,8 @@ int solve_reference(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), v
         if (p.use_graphs) {
             KeyHash key;
             key.add(1000).add(probing).add(probe.bnorm).add(probe.cnorm).add(probe.tol).add(h->offset);
-            key.add(h->A.blk).add(h->At.blk).add(h->A.cap).add(h->part);
+            if (probing) key.add(h->A.cur().blk).add(h->At.cur().blk).add(h->A.cur().cap);
+            key.add(h->part);
             cudaGraphExec_t ge = chunk_graph(h, 0, key.h, launch);
             const int per = launches_per_chunk(K, true) + (probing ? 3 : 0);
             R = run_chunks(h, p, poll, ctx, t0, 0, per, [&]() { NIR_CUDA(cudaGraphLaunch(ge, s)); }, nullptr);
@@ -1059,43 +1253,42 @@ double rhs_norm(const nir_pdhg* h) {
     return std::sqrt(s.hi + s.lo);
 }
 
-// The autotuner: picks the warp row-block capacity (nonzeros per warp
-// block, hence also how many rows a warp takes) for this matrix by timing
-// each candidate layout with the plain SpMV kernels of the precision in
-// use, both orientations, on scratch vectors.  The choice is cached per
-// handle and precision.
-template <typename T>
+// The autotuner: picks the CTA-block capacity 256 E (E = 1, 2, 4, 8
+// nonzeros per thread) for this matrix by timing the plain CTA SpMV of
+// each candidate layout in the value and iterate precision the solve
+// starts in, both orientations, on scratch vectors.  The choice is cached
+// per handle and precision.
+template <typename TV, typename TX>
 double time_layout(nir_pdhg* h, int cap) {
-    set_blocks(h, h->A, cap);
-    set_blocks(h, h->At, cap);
+    Orient::Cta& LA = cta_layout(h, h->A, cap);
+    Orient::Cta& LT = cta_layout(h, h->At, cap);
     cudaStream_t s = h->stream;
-    T* in_n = reinterpret_cast<T*>(h->tmp_n);
-    T* in_m = reinterpret_cast<T*>(h->tmp_m);
-    T* out_n = reinterpret_cast<T*>(h->out_x);
-    T* out_m = reinterpret_cast<T*>(h->out_y);
-    const T* vA = std::is_same<T, float>::value ? (const T*)h->A.v32 : (const T*)h->A.v64;
-    const T* vAt = std::is_same<T, float>::value ? (const T*)h->At.v32 : (const T*)h->At.v64;
-    const LaunchCfg la = warp_cfg<T>(h, nir::k_spmv_adaptive<T, T, T>, h->A.nblk);
-    const LaunchCfg lt = warp_cfg<T>(h, nir::k_spmv_adaptive<T, T, T>, h->At.nblk);
-    cudaEvent_t a, b;
-    NIR_CUDA(cudaEventCreate(&a));
-    NIR_CUDA(cudaEventCreate(&b));
+    TX* in_n = reinterpret_cast<TX*>(std::is_same<TX, float>::value ? (void*)h->tmp_n32 : (void*)h->tmp_n);
+    TX* in_m = reinterpret_cast<TX*>(std::is_same<TX, float>::value ? (void*)h->tmp_m32 : (void*)h->tmp_m);
+    TX* out_n = reinterpret_cast<TX*>(h->out_x);
+    TX* out_m = reinterpret_cast<TX*>(h->out_y);
     float best = 1e30f;
-    for (int rep = 0; rep < 4; ++rep) {
-        NIR_CUDA(cudaEventRecord(a, s));
-        nir::k_spmv_adaptive<T, T, T><<<la.grid, nir::kBlock, la.smem, s>>>(h->A.blk, h->A.nblk, cap, h->A.rp, h->A.ci, vA,
-                                                                           in_n, out_m);
-        nir::k_spmv_adaptive<T, T, T><<<lt.grid, nir::kBlock, lt.smem, s>>>(h->At.blk, h->At.nblk, cap, h->At.rp,
-                                                                           h->At.ci, vAt, in_m, out_n);
-        NIR_LAUNCHED();
-        NIR_CUDA(cudaEventRecord(b, s));
-        NIR_CUDA(cudaEventSynchronize(b));
-        float ms = 0.0f;
-        NIR_CUDA(cudaEventElapsedTime(&ms, a, b));
-        if (rep > 0) best = std::min(best, ms);  // the first launch warms up
-    }
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
+    with_run_len(cap, [&](auto e) {
+        constexpr int E = decltype(e)::value;
+        auto* kern = nir::k_spmv_cta<TX, TV, TX, E>;
+        const int ga = cta_grid(h, kern, LA.nblk), gt = cta_grid(h, kern, LT.nblk);
+        cudaEvent_t a, b;
+        NIR_CUDA(cudaEventCreate(&a));
+        NIR_CUDA(cudaEventCreate(&b));
+        for (int rep = 0; rep < 4; ++rep) {
+            NIR_CUDA(cudaEventRecord(a, s));
+            kern<<<ga, nir::kBlock, 0, s>>>(LA.blk, LA.nblk, h->A.rp, LA.ci, vals<TV>(LA), in_n, out_m);
+            kern<<<gt, nir::kBlock, 0, s>>>(LT.blk, LT.nblk, h->At.rp, LT.ci, vals<TV>(LT), in_m, out_n);
+            NIR_LAUNCHED();
+            NIR_CUDA(cudaEventRecord(b, s));
+            NIR_CUDA(cudaEventSynchronize(b));
+            float ms = 0.0f;
+            NIR_CUDA(cudaEventElapsedTime(&ms, a, b));
+            if (rep > 0) best = std::min(best, ms);  // the first launch warms up
+        }
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+    });
     return best;
 }
 
@@ -1106,20 +1299,23 @@ double time_layout(nir_pdhg* h, int cap) {
 std::mutex g_tune_mu;
 std::vector<std::pair<unsigned long long, int>> g_tuned;
 
-unsigned long long structure_key(const nir_pdhg* h, bool f64) {
+unsigned long long structure_key(const nir_pdhg* h, int prec) {
     KeyHash k;
-    k.add(h->device).add(h->m).add(h->n).add(h->nnz).add(f64);
+    k.add(h->device).add(h->m).add(h->n).add(h->nnz).add(prec).add(2);  // 2: CTA-block layouts
     for (int v : h->A.h_rp) k.add(v);
     for (int v : h->At.h_rp) k.add(v);
     return k.h;
 }
 
 int pick_cap(nir_pdhg* h, const nir_pdhg_params& p) {
-    if (p.spmv_block_nnz > 0) return p.spmv_block_nnz;
-    const bool f64 = (p.precision == NIR_PREC_FP64);
-    int& cached = h->tuned_cap[f64 ? 1 : 0];
+    if (p.spmv_block_nnz > 0) {
+        run_len(p.spmv_block_nnz);  // throws on a capacity the kernels do not have
+        return p.spmv_block_nnz;
+    }
+    const int prec = p.precision;  // NIR_PREC_*: FP64 starts with FP64 values, MIXED and FP32 with FP32 values
+    int& cached = h->tuned_cap[prec];
     if (cached > 0) return cached;
-    const unsigned long long key = structure_key(h, f64);
+    const unsigned long long key = structure_key(h, prec);
     {
         std::lock_guard<std::mutex> g(g_tune_mu);
         for (auto& e : g_tuned)
@@ -1128,12 +1324,16 @@ int pick_cap(nir_pdhg* h, const nir_pdhg_params& p) {
     // the scratch inputs only need to hold finite values
     nir::k_fill<<<grid_for(h->n), nir::kBlock, 0, h->stream>>>(h->n, 0.5, h->tmp_n);
     nir::k_fill<<<grid_for(h->m), nir::kBlock, 0, h->stream>>>(h->m, 0.5, h->tmp_m);
+    nir::k_to_float<<<grid_for(h->n), nir::kBlock, 0, h->stream>>>(h->n, h->tmp_n, h->tmp_n32);
+    nir::k_to_float<<<grid_for(h->m), nir::kBlock, 0, h->stream>>>(h->m, h->tmp_m, h->tmp_m32);
     NIR_LAUNCHED();
     double best = 1e300;
-    int arg = auto_cap(h->nnz, std::max(h->m, h->n));
-    for (int cap : {32, 64, 128, 256}) {
-        if (cap > nir::kWarpCapMax) continue;
-        const double t = f64 ? time_layout<double>(h, cap) : time_layout<float>(h, cap);
+    int arg = auto_cta_cap(h);
+    for (int cap : {256, 512, 1024, 2048}) {
+        double t;
+        if (prec == NIR_PREC_FP64) t = time_layout<double, double>(h, cap);
+        else if (prec == NIR_PREC_MIXED) t = time_layout<float, double>(h, cap);
+        else t = time_layout<float, float>(h, cap);
         if (t <= best * 1.02) {  // near-ties go to the larger capacity
             arg = cap;
             best = std::min(best, t);
@@ -1151,14 +1351,14 @@ int solve_fast(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), void* 
     const double t0 = now_sec();
     const int n = h->n, m = h->m;
     const bool pdlp = p.algorithm == NIR_ALGO_PDLP;
-    if (p.spmv_block_nnz > nir::kWarpCapMax)
-        throw std::invalid_argument("spmv_block_nnz must be at most " + std::to_string(nir::kWarpCapMax));
     const int cap = pick_cap(h, p);
-    set_blocks(h, h->A, cap);
-    set_blocks(h, h->At, cap);
+    use_cta(h, cap);
     ensure_partials(h);
-    warm_cfgs<float>(h);
-    warm_cfgs<double>(h);
+    // value / iterate precision of each phase: FP64 (double, double); MIXED
+    // (float, double) then the FP64 polish; FP32 (float, float)
+    if (p.precision == NIR_PREC_FP32) warm_cfgs<float, float>(h);
+    if (p.precision == NIR_PREC_MIXED) warm_cfgs<float, double>(h);
+    if (p.precision != NIR_PREC_FP32) warm_cfgs<double, double>(h);
     SolveCfg cfg;
     cfg.p = p;
     cfg.K = std::max(1, p.check_every);
@@ -1186,6 +1386,7 @@ int solve_fast(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), void* 
 
     NIR_CUDA(cudaMemsetAsync(h->hist, 0, sizeof(double) * 8 * nir::kHist, s));
     precondition(h, p, pdlp && (p.ruiz_iters > 0 || p.pock_chambolle));
+    pad_scaled(h);
     nir::DevState st0{};
     st0.max_iters = p.max_iters;
     st0.best_kkt = INFINITY;
@@ -1270,45 +1471,41 @@ int solve_fast(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), void* 
     }
     const bool fp64_first = (p.precision == NIR_PREC_FP64);
     LoopResult R;
-    int final_phase = 0;
     double t_switch = 0.0;
     try {
-        auto run_phase = [&](int phase, bool f64) {
-            auto launch = [&, phase, f64]() {
-                if (f64) launch_fast_chunk<double>(h, cfg, phase, h->profiling ? &tm : nullptr);
-                else launch_fast_chunk<float>(h, cfg, phase, h->profiling ? &tm : nullptr);
+        // prec: 0 = (float values, float iterates), 1 = (float, double), 2 = (double, double)
+        auto run_phase = [&](int phase, int prec) {
+            auto launch = [&, phase, prec]() {
+                ChunkTimer* t = h->profiling ? &tm : nullptr;
+                if (prec == 2) launch_fast_chunk<double, double>(h, cfg, phase, t);
+                else if (prec == 1) launch_fast_chunk<float, double>(h, cfg, phase, t);
+                else launch_fast_chunk<float, float>(h, cfg, phase, t);
             };
             const int per = launches_per_chunk(cfg.K, false);
             if (p.use_graphs && !h->profiling && !cfg.persistent) {
-                cudaGraphExec_t ge = chunk_graph(h, 1 + phase, chunk_key(h, cfg, phase, f64), launch);
+                cudaGraphExec_t ge = chunk_graph(h, 1 + phase, chunk_key(h, cfg, phase, prec), launch);
                 return run_chunks(h, p, poll, ctx, t0, phase, per, [&]() { NIR_CUDA(cudaGraphLaunch(ge, s)); }, nullptr);
             }
             return run_chunks(h, p, poll, ctx, t0, phase, 0, launch, h->profiling ? &tm : nullptr);
         };
         if (p.max_iters > 0) {
-            R = run_phase(0, fp64_first);
+            R = run_phase(0, fp64_first ? 2 : (p.precision == NIR_PREC_MIXED ? 1 : 0));
             if (!R.stopped_by_host && cfg.mixed && !R.last.done && R.last.phase == 1) {
-                // FP32 stalled: polish in FP64 from the last evaluated point
+                // the FP32 values stopped improving the KKT error: polish with
+                // the FP64 values from the last evaluated point.  The iterates
+                // are FP64 in both phases.
                 t_switch = now_sec() - t_setup;
                 nir::DevState cur;
                 d2h(h, &cur, h->st, sizeof(cur));
-                if (p.polish_fresh == 2) {
-                    // a pure change of precision: the Halpern iterate, its anchor
-                    // and every counter carry on unchanged
-                    const long long nm = std::max(n, m);
-                    nir::k_to_double<<<grid_for(n), nir::kBlock, 0, s>>>(n, h->x32, h->x64);
-                    nir::k_to_double<<<grid_for(n), nir::kBlock, 0, s>>>(n, h->x032, h->x064);
-                    nir::k_to_double<<<grid_for(n), nir::kBlock, 0, s>>>(n, h->xp32, h->xp64);
-                    nir::k_to_double<<<grid_for(m), nir::kBlock, 0, s>>>(m, h->y32, h->y64);
-                    nir::k_to_double<<<grid_for(m), nir::kBlock, 0, s>>>(m, h->y032, h->y064);
-                    nir::k_to_double<<<grid_for(m), nir::kBlock, 0, s>>>(m, h->yp32, h->yp64);
-                    (void)nm;
-                } else {
-                    nir::k_promote<<<std::max(grid_for(std::max(n, m)), 1u), nir::kBlock, 0, s>>>(
-                        n, m, h->xp32, h->yp32, h->l64, h->u64, h->x64, h->x064, h->xp64, h->y64, h->y064, h->yp64);
+                if (p.polish_fresh != 2) {
+                    // a fresh start at (x+, y+): iterate and anchor both there
+                    nir::k_restart_at<<<std::max(grid_for(std::max(n, m)), 1u), nir::kBlock, 0, s>>>(
+                        n, m, h->xp64, h->yp64, h->x64, h->x064, h->y64, h->y064);
                     cur.k_base = 0;
                     cur.have_anchor = 0;
                 }
+                // polish_fresh == 2: a pure change of the matrix precision; the
+                // Halpern iterate, its anchor and every counter carry on
                 NIR_LAUNCHED();
                 cur.apply_restart = 0;
                 cur.switch_request = 0;
@@ -1322,9 +1519,8 @@ int solve_fast(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), void* 
                     cur.it_phase = cur.iter;
                 }
                 h2d(h, h->st, &cur, sizeof(cur));
-                final_phase = 1;
                 long long it_switch = cur.iter;
-                R = run_phase(1, true);
+                R = run_phase(1, 2);
                 info->iterations_fp64 = 0;
                 nir::DevState fin;
                 d2h(h, &fin, h->st, sizeof(fin));
@@ -1340,7 +1536,7 @@ int solve_fast(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), void* 
         for (auto& e : tm.e) cudaEventDestroy(e);
     nir::DevState st;
     d2h(h, &st, h->st, sizeof(st));
-    const bool out64 = fp64_first || final_phase == 1;
+    const bool out64 = p.precision != NIR_PREC_FP32;
     const unsigned g = std::max(grid_for(std::max(n, m)), 1u);
     if (out64) nir::k_unscale_out<double><<<g, nir::kBlock, 0, s>>>(n, m, h->xp64, h->yp64, h->dc, h->dr, h->out_x, h->out_y);
     else nir::k_unscale_out<float><<<g, nir::kBlock, 0, s>>>(n, m, h->xp32, h->yp32, h->dc, h->dr, h->out_x, h->out_y);
@@ -1372,6 +1568,8 @@ int solve_fast(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), void* 
 }
 
 }  // namespace
+
+#include "engine_parallel.cuh"
 
 // ---------------------------------------------------------------- C ABI
 
@@ -1429,6 +1627,7 @@ int nir_pdhg_create(const nir_lp_view* lp, int device, nir_pdhg** out) {
     h->device = -1;
     try {
         create_impl(h.get(), lp, device);
+        build_parallel(h.get(), lp, device);
     } catch (const std::invalid_argument& e) {
         g_err = e.what();
         return NIR_STATUS_INPUT_ERROR;
@@ -1438,6 +1637,24 @@ int nir_pdhg_create(const nir_lp_view* lp, int device, nir_pdhg** out) {
     }
     *out = h.release();
     return 0;
+}
+
+int nir_pdhg_parallel_groups(const nir_lp_view* lp, int32_t* rep_of, double* lambda, int32_t* groups) {
+    if (!groups) {
+        g_err = "null output";
+        return NIR_STATUS_INPUT_ERROR;
+    }
+    try {
+        validate_lp(lp);
+        const ParallelGroups g = find_parallel(lp);
+        *groups = g.groups;
+        if (rep_of) std::copy(g.rep_of.begin(), g.rep_of.end(), rep_of);
+        if (lambda) std::copy(g.lam.begin(), g.lam.end(), lambda);
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return NIR_STATUS_INPUT_ERROR;
+    }
 }
 
 int nir_pdhg_update_vectors(nir_pdhg* h, const double* cost, const double* collo, const double* colup,
@@ -1452,6 +1669,7 @@ int nir_pdhg_update_vectors(nir_pdhg* h, const double* cost, const double* collo
             for (int j = 0; j < h->n; ++j)
                 if (!std::isfinite(cost[j])) throw std::invalid_argument("non-finite cost");
         upload_vectors(h, cost, collo, colup, rowlo, rowup);
+        if (h->inner) parallel_update_vectors(h);
         return 0;
     } catch (const std::invalid_argument& e) {
         g_err = e.what();
@@ -1485,6 +1703,7 @@ int nir_pdhg_solve(nir_pdhg* h, const nir_pdhg_params* p_in, int (*poll)(void*),
         h->last_x = nullptr;  // out_x and x64 serve as scratch until the solve's end
         int st;
         if (p.algorithm == NIR_ALGO_REFERENCE) st = solve_reference(h, p, poll, poll_ctx, x_out, y_out, info);
+        else if (h->inner) st = solve_parallel(h, p, poll, poll_ctx, x_out, y_out, info);
         else st = solve_fast(h, p, poll, poll_ctx, x_out, y_out, info);
         info->kernel_launches = h->launches - before;
         return st;
@@ -1623,6 +1842,182 @@ int nir_pdhg_time_spmv(nir_pdhg* h, int transpose, int kernel, int reps, int flu
     }
 }
 
+}  // extern "C"
+
+namespace {
+
+// Launches k_spmv_cta for the run length of the layout with a persistent
+// grid of the resident CTAs.
+template <typename TA, typename TV, typename TX>
+void launch_spmv_cta(nir_pdhg* h, const Orient::Cta& c, const int* rp, const TV* val, const TX* x, TA* y) {
+    with_run_len(c.cap, [&](auto e) {
+        constexpr int E = decltype(e)::value;
+        auto* kern = nir::k_spmv_cta<TA, TV, TX, E>;
+        const int grid = cta_grid(h, kern, c.nblk);
+        kern<<<grid, nir::kBlock, 0, h->stream>>>(c.blk, c.nblk, rp, c.ci, val, x, y);
+        NIR_LAUNCHED();
+    });
+}
+
+// One launch of a measured SpMV kind (nir_pdhg_time_kernel) on the
+// handle's device vectors: din/fin inputs, dout/fout outputs.
+void launch_kernel_kind(nir_pdhg* h, Orient& o, int kernel, int cap, const double* din, const float* fin, double* dout,
+                        float* fout) {
+    cudaStream_t s = h->stream;
+    const int nout = o.rows;
+    switch (kernel) {
+        case 0:
+            nir::k_ref_spmv<<<std::max(grid_for(nout), 1u), nir::kBlock, 0, s>>>(nout, o.rp, o.ci, o.v_orig, din, dout);
+            NIR_LAUNCHED();
+            return;
+        case 1:
+        case 2: {
+            if (kernel == 1) {
+                const LaunchCfg lc = warp_cfg<double>(h, nir::k_spmv_adaptive<double, double, double>, o.nblk);
+                nir::k_spmv_adaptive<double, double, double><<<lc.grid, nir::kBlock, lc.smem, s>>>(
+                    o.blk, o.nblk, o.cap, o.rp, o.ci, o.v_orig, din, dout);
+            } else {
+                const LaunchCfg lc = warp_cfg<float>(h, nir::k_spmv_adaptive<float, float, float>, o.nblk);
+                nir::k_spmv_adaptive<float, float, float><<<lc.grid, nir::kBlock, lc.smem, s>>>(
+                    o.blk, o.nblk, o.cap, o.rp, o.ci, o.v32_orig, fin, fout);
+            }
+            NIR_LAUNCHED();
+            return;
+        }
+        case 3:
+        case 4:
+        case 5: {
+            Orient::Cta& c = cta_layout(h, o, cap);
+            cta_orig_values(h, o, c);
+            if (kernel == 3) launch_spmv_cta<double, double, double>(h, c, o.rp, c.vorig, din, dout);
+            else if (kernel == 4) launch_spmv_cta<float, float, float>(h, c, o.rp, c.v32orig, fin, fout);
+            else launch_spmv_cta<double, float, double>(h, c, o.rp, c.v32orig, din, dout);
+            return;
+        }
+        default: break;
+    }
+    // the row-less ceilings over the CSR stream itself (groups of 8 from 0)
+    const int groups = int(o.nnz / 8);
+    const unsigned grid = unsigned(8 * h->sms);
+    if (!h->ceil_out) h->ceil_out = h->alloc<double>(size_t(grid) * nir::kBlock);
+    double* out = h->ceil_out;
+    switch (kernel) {
+        case 6: nir::k_stream_ceiling<double, double, double, true><<<grid, nir::kBlock, 0, s>>>(groups, o.ci, o.v_orig, din, out); break;
+        case 7: nir::k_stream_ceiling<float, float, float, true><<<grid, nir::kBlock, 0, s>>>(groups, o.ci, o.v32_orig, fin, reinterpret_cast<float*>(out)); break;
+        case 8: nir::k_stream_ceiling<double, double, double, false><<<grid, nir::kBlock, 0, s>>>(groups, o.ci, o.v_orig, din, out); break;
+        case 9: nir::k_stream_ceiling<float, float, float, false><<<grid, nir::kBlock, 0, s>>>(groups, o.ci, o.v32_orig, fin, reinterpret_cast<float*>(out)); break;
+        default: throw std::invalid_argument("kernel kind out of range");
+    }
+    NIR_LAUNCHED();
+}
+
+// FP32 copy of the original values (the FP32 kernel kinds).
+void ensure_v32_orig(nir_pdhg* h, Orient& o) {
+    if (o.v32_orig) return;
+    o.v32_orig = h->allocz<float>(o.nnz);
+    nir::k_to_float<<<grid_for(o.nnz), nir::kBlock, 0, h->stream>>>(o.nnz, o.v_orig, o.v32_orig);
+    NIR_LAUNCHED();
+}
+
+}  // namespace
+
+extern "C" {
+
+int nir_pdhg_spmv_kernel(nir_pdhg* h, int transpose, int kernel, int block_nnz, const double* x, double* y) {
+    if (!h || !x || !y || kernel < 0 || kernel > 5) {
+        g_err = "invalid arguments";
+        return NIR_STATUS_INPUT_ERROR;
+    }
+    try {
+        NIR_CUDA(cudaSetDevice(h->device));
+        cudaStream_t s = h->stream;
+        Orient& o = transpose ? h->At : h->A;
+        const int nin = o.cols, nout = o.rows;
+        if (!o.blk) set_blocks(h, o, auto_cap(h->nnz, nout));
+        ensure_v32_orig(h, o);
+        double* din = transpose ? h->tmp_m : h->tmp_n;
+        double* dout = transpose ? h->tmp_n : h->tmp_m;
+        float* fin = transpose ? h->tmp_m32 : h->tmp_n32;
+        float* fout = transpose ? h->tmp_n32 : h->tmp_m32;
+        NIR_CUDA(cudaMemcpyAsync(din, x, nin * sizeof(double), cudaMemcpyHostToDevice, s));
+        nir::k_to_float<<<std::max(grid_for(nin), 1u), nir::kBlock, 0, s>>>(nin, din, fin);
+        NIR_LAUNCHED();
+        launch_kernel_kind(h, o, kernel, block_nnz > 0 ? block_nnz : 2048, din, fin, dout, fout);
+        if (kernel == 2 || kernel == 4) {
+            nir::k_to_double<<<std::max(grid_for(nout), 1u), nir::kBlock, 0, s>>>(nout, fout, dout);
+            NIR_LAUNCHED();
+        }
+        NIR_CUDA(cudaMemcpyAsync(y, dout, nout * sizeof(double), cudaMemcpyDeviceToHost, s));
+        NIR_CUDA(cudaStreamSynchronize(s));
+        return 0;
+    } catch (const std::invalid_argument& e) {
+        g_err = e.what();
+        return NIR_STATUS_INPUT_ERROR;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return NIR_STATUS_INTERNAL_ERROR;
+    }
+}
+
+int nir_pdhg_time_kernel(nir_pdhg* h, int transpose, int kernel, int block_nnz, int reps, int flush_l2,
+                         double* usec) {
+    if (!h || !usec || reps < 1 || kernel < 0 || kernel > 9) {
+        g_err = "invalid arguments";
+        return NIR_STATUS_INPUT_ERROR;
+    }
+    try {
+        NIR_CUDA(cudaSetDevice(h->device));
+        cudaStream_t s = h->stream;
+        Orient& o = transpose ? h->At : h->A;
+        const int nin = o.cols;
+        if (!o.blk) set_blocks(h, o, auto_cap(h->nnz, o.rows));
+        ensure_v32_orig(h, o);
+        const int cap = block_nnz > 0 ? block_nnz : 2048;
+        if (kernel >= 3 && kernel <= 5) cta_orig_values(h, o, cta_layout(h, o, cap));
+        double* din = transpose ? h->tmp_m : h->tmp_n;
+        double* dout = transpose ? h->tmp_n : h->tmp_m;
+        float* fin = transpose ? h->tmp_m32 : h->tmp_n32;
+        float* fout = transpose ? h->tmp_n32 : h->tmp_m32;
+        nir::k_fill<<<std::max(grid_for(nin), 1u), nir::kBlock, 0, s>>>(nin, 1.0, din);
+        nir::k_to_float<<<std::max(grid_for(nin), 1u), nir::kBlock, 0, s>>>(nin, din, fin);
+        NIR_LAUNCHED();
+        if (flush_l2 && !h->flush) {
+            h->flush_bytes = size_t(512) << 20;
+            h->flush = h->alloc<unsigned char>(h->flush_bytes);
+        }
+        cudaEvent_t a, b;
+        NIR_CUDA(cudaEventCreate(&a));
+        NIR_CUDA(cudaEventCreate(&b));
+        double total_ms = 0.0;
+        try {
+            for (int r = 0; r < reps + 1; ++r) {
+                if (flush_l2) NIR_CUDA(cudaMemsetAsync(h->flush, r & 0xff, h->flush_bytes, s));
+                NIR_CUDA(cudaEventRecord(a, s));
+                launch_kernel_kind(h, o, kernel, cap, din, fin, dout, fout);
+                NIR_CUDA(cudaEventRecord(b, s));
+                NIR_CUDA(cudaEventSynchronize(b));
+                float ms = 0.0f;
+                NIR_CUDA(cudaEventElapsedTime(&ms, a, b));
+                if (r > 0) total_ms += ms;  // the first launch is a warm-up
+            }
+        } catch (...) {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+            throw;
+        }
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        *usec = 1000.0 * total_ms / reps;
+        return 0;
+    } catch (const std::invalid_argument& e) {
+        g_err = e.what();
+        return NIR_STATUS_INPUT_ERROR;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return NIR_STATUS_INTERNAL_ERROR;
+    }
+}
+
 int nir_pdhg_set_profiling(nir_pdhg* h, int on) {
     if (!h) return NIR_STATUS_INPUT_ERROR;
     h->profiling = on != 0;
@@ -1642,8 +2037,103 @@ int nir_pdhg_kernel_times(nir_pdhg* h, nir_pdhg_kernel_time* out) {
     return 0;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Steady-state timing of the fused iteration kernels of one precision on
+// the handle's current state: `reps` back-to-back launches of k_primal
+// alone, of k_dual alone, and of reps (k_primal, k_dual) pairs, each batch
+// bracketed by CUDA events on the handle's stream.  The kernels run against
+// a copy of the solver state marked running, on the layout and scaled
+// values of the last solve; they overwrite the iterates, which a finished
+// solve no longer needs (its result is in out_x / out_y).
+template <typename TV, typename TX, int E>
+void time_iteration_e(nir_pdhg* h, int reps, double* primal_us, double* dual_us, double* pair_us) {
+    cudaStream_t s = h->stream;
+    const PartLayout L = part_layout(h);
+    const Orient::Cta& LA = h->A.cur();
+    const Orient::Cta& LT = h->At.cur();
+    if (!h->st_time) h->st_time = h->alloc<nir::DevState>(1);
+    nir::DevState st;
+    d2h(h, &st, h->st, sizeof(st));
+    st.done = 0;
+    st.phase = 0;
+    h2d(h, h->st_time, &st, sizeof(st));
+    const int gp = cta_grid(h, nir::k_primal<TV, TX, E, false>, LT.nblk);
+    const int gd = cta_grid(h, nir::k_dual<TV, TX, E, false>, LA.nblk);
+    nir::IterArgs ap{LT.blk, LT.nblk, h->At.rp, LT.ci, L.P, h->st_time, 1, 1, 0, 1.0};
+    nir::IterArgs ad{LA.blk, LA.nblk, h->A.rp, LA.ci, L.D, h->st_time, 1, 1, 0, 1.0};
+    auto primal = [&]() {
+        nir::k_primal<TV, TX, E, false><<<gp, nir::kBlock, 0, s>>>(
+            ap, vals<TV>(LT), Vec<TX>::y(h), Vec<TX>::x(h), Vec<TX>::xb(h), Vec<TX>::xp(h), Vec<TX>::c(h),
+            Vec<TX>::l(h), Vec<TX>::u(h), Vec<TX>::x0(h));
+    };
+    auto dual = [&]() {
+        nir::k_dual<TV, TX, E, false><<<gd, nir::kBlock, 0, s>>>(ad, vals<TV>(LA), Vec<TX>::xb(h), Vec<TX>::y(h),
+                                                                 Vec<TX>::yp(h), Vec<TX>::rl(h), Vec<TX>::ru(h),
+                                                                 Vec<TX>::y0(h));
+    };
+    cudaEvent_t a, b;
+    NIR_CUDA(cudaEventCreate(&a));
+    NIR_CUDA(cudaEventCreate(&b));
+    auto timed = [&](int which) {
+        for (int w = 0; w < 2; ++w) {  // the first batch warms up
+            NIR_CUDA(cudaEventRecord(a, s));
+            for (int r = 0; r < reps; ++r) {
+                if (which != 1) primal();
+                if (which != 0) dual();
+            }
+            NIR_LAUNCHED();
+            NIR_CUDA(cudaEventRecord(b, s));
+            NIR_CUDA(cudaEventSynchronize(b));
+        }
+        float ms = 0.0f;
+        NIR_CUDA(cudaEventElapsedTime(&ms, a, b));
+        return 1000.0 * ms / reps;
+    };
+    *primal_us = timed(0);
+    *dual_us = timed(1);
+    *pair_us = timed(2);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    h->launches += 8 * reps;
+}
+
+}  // namespace
+
+extern "C" {
+
+int nir_pdhg_time_iteration(nir_pdhg* h, int precision, int reps, double* primal_us, double* dual_us,
+                            double* pair_us) {
+    if (!h || !primal_us || !dual_us || !pair_us || reps < 1 || precision < 0 || precision > 2) {
+        g_err = "invalid arguments";
+        return NIR_STATUS_INPUT_ERROR;
+    }
+    if (h->inner) h = h->inner.get();  // PDHG / PDLP solves ran on the equivalent LP
+    try {
+        NIR_CUDA(cudaSetDevice(h->device));
+        if (h->A.it < 0) throw std::invalid_argument("no PDHG / PDLP solve has set up the iteration kernels yet");
+        if (h->last_x == h->x64) h->last_x = nullptr;  // a reference-loop result the kernels would overwrite
+        with_run_len(h->A.cur().cap, [&](auto e) {
+            constexpr int E = decltype(e)::value;
+            if (precision == NIR_PREC_FP64) time_iteration_e<double, double, E>(h, reps, primal_us, dual_us, pair_us);
+            else if (precision == NIR_PREC_MIXED) time_iteration_e<float, double, E>(h, reps, primal_us, dual_us, pair_us);
+            else time_iteration_e<float, float, E>(h, reps, primal_us, dual_us, pair_us);
+        });
+        return 0;
+    } catch (const std::invalid_argument& e) {
+        g_err = e.what();
+        return NIR_STATUS_INPUT_ERROR;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return NIR_STATUS_INTERNAL_ERROR;
+    }
+}
+
 int nir_pdhg_history(nir_pdhg* h, double* out, int max_entries) {
     if (!h || !out || max_entries < 0) return -1;
+    if (h->inner) h = h->inner.get();  // PDHG / PDLP solves ran on the equivalent LP
     try {
         NIR_CUDA(cudaSetDevice(h->device));
         std::vector<double> ring(8 * nir::kHist);
@@ -1671,9 +2161,11 @@ int nir_pdhg_get_layout(nir_pdhg* h, nir_pdhg_layout* out) {
     out->nrow = h->m;
     out->ncol = h->n;
     out->nnz = h->nnz;
-    out->blocks_a = h->A.nblk;
-    out->blocks_at = h->At.nblk;
-    out->block_nnz = h->A.cap;
+    const nir_pdhg* src = h->inner ? h->inner.get() : h;  // PDHG / PDLP solves ran on the equivalent LP
+    const bool cta = src->A.it >= 0;
+    out->blocks_a = cta ? src->A.cur().nblk : h->A.nblk;
+    out->blocks_at = cta ? src->At.cur().nblk : h->At.nblk;
+    out->block_nnz = cta ? src->A.cur().cap : h->A.cap;
     out->device_bytes = h->device_bytes;
     return 0;
 }

@@ -13,22 +13,23 @@ struct nir_pdhg_batch {
     int* d_col_off = nullptr;
     int* d_row_inst = nullptr;
     int* d_col_inst = nullptr;
-    // warp row blocks per instance, built for one capacity
-    int cap = 0;
-    int2 *blkA = nullptr, *blkAt = nullptr;
-    int *instA = nullptr, *instAt = nullptr;
-    int nblkA = 0, nblkAt = 0;
-    int *d_a_lo = nullptr, *d_at_lo = nullptr;
-    double* part = nullptr;
-    struct Layout {
-        int cap;
-        int2 *blkA, *blkAt;
-        int *instA, *instAt;
-        int nblkA, nblkAt;
-        int *a_lo, *at_lo;
-        double* part;
+    // CTA blocks per instance (no block crosses an instance) with their
+    // padded streams, one layout per capacity used, built once each
+    struct Orient2 {
+        int4* blk = nullptr;  // .w = instance
+        int nblk = 0;
+        int* lo = nullptr;    // first block of each instance (count + 1)
+        int* ci = nullptr;    // padded column indices
+        double* v64 = nullptr;
+        float* v32 = nullptr;
     };
-    std::vector<Layout> layouts;  // one per capacity used, built once each
+    struct Layout {
+        int cap = 0;
+        Orient2 a, at;        // A (rows) and A' (columns)
+        double* part = nullptr;
+    };
+    std::deque<Layout> layouts;
+    Layout* cur = nullptr;
     nir::DevState* insts = nullptr;
     double *d_bnorm = nullptr, *d_cnorm = nullptr, *d_offset = nullptr, *d_norm = nullptr;
     ChunkGraph graphs[2];
@@ -45,75 +46,131 @@ struct nir_pdhg_batch {
 
 namespace {
 
-// Warp row blocks of one orientation, built instance by instance so that
-// no block crosses an instance; also the instance of every block and each
-// instance's first block.
-void batch_blocks(nir_pdhg_batch* B, const std::vector<int>& rp, const std::vector<int>& off, int cap, int2** blk,
-                  int** inst, int* nblk, int** d_lo) {
+// CTA blocks of one orientation, built instance by instance so that no
+// block crosses an instance, and the padded stream of its column indices
+// (values are padded after each preconditioning, batch_pad_values).
+void batch_blocks(nir_pdhg_batch* B, const Orient& o, const std::vector<int>& off, int cap,
+                  nir_pdhg_batch::Orient2* out) {
     nir_pdhg* h = B->h;
-    std::vector<int> owner, lo;
-    const std::vector<int2> all = nir::build_batch_row_blocks(rp, off, cap, &owner, &lo);
-    *nblk = int(owner.size());
-    *blk = h->alloc<int2>(all.size());
-    h2d(h, *blk, all.data(), all.size() * sizeof(int2));
-    *inst = h->alloc<int>(std::max<size_t>(owner.size(), 1));
-    if (!owner.empty()) h2d(h, *inst, owner.data(), owner.size() * sizeof(int));
-    *d_lo = h->alloc<int>(lo.size());
-    h2d(h, *d_lo, lo.data(), lo.size() * sizeof(int));
+    std::vector<int> lo;
+    const std::vector<int4> all = nir::build_batch_cta_blocks(o.h_rp, off, cap, &lo);
+    out->nblk = int(all.size()) - 1;
+    out->blk = h->alloc<int4>(all.size());
+    h2d(h, out->blk, all.data(), all.size() * sizeof(int4));
+    out->lo = h->alloc<int>(lo.size());
+    h2d(h, out->lo, lo.data(), lo.size() * sizeof(int));
+    const size_t q = size_t(all.back().z);
+    out->ci = h->allocz<int>(q, 8);
+    out->v64 = h->allocz<double>(q, 8);
+    out->v32 = h->allocz<float>(q, 8);
+    if (out->nblk > 0 && o.nnz > 0) {
+        const unsigned g = unsigned(std::max(1, std::min(out->nblk, 4 * h->sms)));
+        nir::k_pad_stream<double><<<g, nir::kBlock, 0, h->stream>>>(out->blk, out->nblk, o.ci, o.v_orig, out->ci,
+                                                                    out->v64);
+        NIR_LAUNCHED();
+    }
+    NIR_CUDA(cudaStreamSynchronize(h->stream));
+}
+
+// The scaled values (written by precondition) into the padded streams.
+void batch_pad_values(nir_pdhg_batch* B) {
+    nir_pdhg* h = B->h;
+    for (int t = 0; t < 2; ++t) {
+        const nir_pdhg_batch::Orient2& L = t ? B->cur->at : B->cur->a;
+        const Orient& o = t ? h->At : h->A;
+        if (L.nblk <= 0 || o.nnz <= 0) continue;
+        const unsigned g = unsigned(std::max(1, std::min(L.nblk, 4 * h->sms)));
+        nir::k_pad_stream<double><<<g, nir::kBlock, 0, h->stream>>>(L.blk, L.nblk, o.ci, o.v64, nullptr, L.v64);
+        nir::k_pad_stream<float><<<g, nir::kBlock, 0, h->stream>>>(L.blk, L.nblk, o.ci, o.v32, nullptr, L.v32);
+        NIR_LAUNCHED();
+    }
+}
+
+template <typename TV>
+const TV* bvals(const nir_pdhg_batch::Orient2& L);
+template <>
+const float* bvals<float>(const nir_pdhg_batch::Orient2& L) {
+    return L.v32;
+}
+template <>
+const double* bvals<double>(const nir_pdhg_batch::Orient2& L) {
+    return L.v64;
 }
 
 nir::BatchArgs bargs(nir_pdhg_batch* B, bool transpose, double* part, int i, int halpern, int phase, double rho) {
     nir_pdhg* h = B->h;
     const Orient& o = transpose ? h->At : h->A;
-    return nir::BatchArgs{transpose ? B->blkAt : B->blkA, transpose ? B->nblkAt : B->nblkA, B->cap, o.rp, o.ci,
-                          transpose ? B->instAt : B->instA, part, B->insts, i, halpern, phase, rho};
+    const nir_pdhg_batch::Orient2& L = transpose ? B->cur->at : B->cur->a;
+    return nir::BatchArgs{L.blk, L.nblk, o.rp, L.ci, part, B->insts, i, halpern, phase, rho};
 }
 
-template <typename T>
-void launch_batch_chunk(nir_pdhg_batch* B, const SolveCfg& cfg, int phase) {
+// One launch chunk of the batch; TV = value type, TX = iterate type.
+template <typename TV, typename TX, int E>
+void launch_batch_chunk_e(nir_pdhg_batch* B, const SolveCfg& cfg, int phase) {
     nir_pdhg* h = B->h;
     cudaStream_t s = h->stream;
     const int K = cfg.K;
-    double* P = B->part;
-    double* D = P + 2 * size_t(std::max(B->nblkAt, 1));
-    double* KR = D + 2 * size_t(std::max(B->nblkA, 1));
-    double* KC = KR + 4 * size_t(std::max(B->nblkA, 1));
-    const LaunchCfg cp1 = warp_cfg<T>(h, nir::k_bprimal<T, true>, B->nblkAt);
-    const LaunchCfg cp0 = warp_cfg<T>(h, nir::k_bprimal<T, false>, B->nblkAt);
-    const LaunchCfg cd1 = warp_cfg<T>(h, nir::k_bdual<T, true>, B->nblkA);
-    const LaunchCfg cd0 = warp_cfg<T>(h, nir::k_bdual<T, false>, B->nblkA);
-    const LaunchCfg ckr = warp_cfg<double>(h, nir::k_bkkt_rows<T>, B->nblkA);
-    const LaunchCfg ckc = warp_cfg<double>(h, nir::k_bkkt_cols<T>, B->nblkAt);
-    for (int i = 0; i < K; ++i) {
+    const nir_pdhg_batch::Orient2& LA = B->cur->a;
+    const nir_pdhg_batch::Orient2& LT = B->cur->at;
+    double* P = B->cur->part;
+    double* D = P + 2 * size_t(std::max(LT.nblk, 1));
+    double* KR = D + 2 * size_t(std::max(LA.nblk, 1));
+    double* KC = KR + 4 * size_t(std::max(LA.nblk, 1));
+    const int gp1 = cta_grid(h, nir::k_bprimal<TV, TX, E, true>, LT.nblk);
+    const int gp0 = cta_grid(h, nir::k_bprimal<TV, TX, E, false>, LT.nblk);
+    const int gd1 = cta_grid(h, nir::k_bdual<TV, TX, E, true>, LA.nblk);
+    const int gd0 = cta_grid(h, nir::k_bdual<TV, TX, E, false>, LA.nblk);
+    const int gkr = cta_grid(h, nir::k_bkkt_rows<TX, E>, LA.nblk);
+    const int gkc = cta_grid(h, nir::k_bkkt_cols<TX, E>, LT.nblk);
+    int i_first = 0;
+    if (cfg.persistent && K > 1) {
+        // iterations 0..K-2 in one cooperative launch; the check pair below
+        const int gc = cta_grid(h, nir::k_bchunk<TV, TX, E>, std::max(LA.nblk, LT.nblk));
+        nir::BatchArgs ap = bargs(B, true, P, 0, cfg.halpern, phase, cfg.p.reflection);
+        nir::BatchArgs ad = bargs(B, false, D, 0, cfg.halpern, phase, cfg.p.reflection);
+        nir::ChunkPtrs<TV, TX> v{bvals<TV>(LT),  bvals<TV>(LA),  Vec<TX>::x(h),  Vec<TX>::xb(h), Vec<TX>::xp(h),
+                                 Vec<TX>::y(h),  Vec<TX>::yp(h), Vec<TX>::c(h),  Vec<TX>::l(h),  Vec<TX>::u(h),
+                                 Vec<TX>::x0(h), Vec<TX>::rl(h), Vec<TX>::ru(h), Vec<TX>::y0(h)};
+        nir::GridSync gs{h->gs_count, h->gs_gen, h->gs_err, unsigned(gc) + (cfg.barrier_test ? 1u : 0u),
+                         cfg.barrier_test ? 200000000LL : 2000000000LL};
+        nir::DevState* insts = B->insts;
+        int i0 = 0, iters = K - 1, count = B->count;
+        void* args[] = {&ap, &ad, &v, &i0, &iters, &gs, &insts, &count};
+        NIR_CUDA(cudaLaunchCooperativeKernel((const void*)nir::k_bchunk<TV, TX, E>, dim3(gc), dim3(nir::kBlock), args,
+                                             0, s));
+        h->launches += 1;
+        i_first = K - 1;
+    }
+    for (int i = i_first; i < K; ++i) {
         const bool check = (i == K - 1);
         nir::BatchArgs ap = bargs(B, true, P, i, cfg.halpern, phase, cfg.p.reflection);
         nir::BatchArgs ad = bargs(B, false, D, i, cfg.halpern, phase, cfg.p.reflection);
         if (check)
-            nir::k_bprimal<T, true><<<cp1.grid, nir::kBlock, cp1.smem, s>>>(
-                ap, View<T>::valAt(h), View<T>::y(h), View<T>::x(h), View<T>::xb(h), View<T>::xp(h), View<T>::c(h),
-                View<T>::l(h), View<T>::u(h), View<T>::x0(h));
+            nir::k_bprimal<TV, TX, E, true><<<gp1, nir::kBlock, 0, s>>>(
+                ap, bvals<TV>(LT), Vec<TX>::y(h), Vec<TX>::x(h), Vec<TX>::xb(h), Vec<TX>::xp(h), Vec<TX>::c(h),
+                Vec<TX>::l(h), Vec<TX>::u(h), Vec<TX>::x0(h));
         else
-            nir::k_bprimal<T, false><<<cp0.grid, nir::kBlock, cp0.smem, s>>>(
-                ap, View<T>::valAt(h), View<T>::y(h), View<T>::x(h), View<T>::xb(h), View<T>::xp(h), View<T>::c(h),
-                View<T>::l(h), View<T>::u(h), View<T>::x0(h));
+            nir::k_bprimal<TV, TX, E, false><<<gp0, nir::kBlock, 0, s>>>(
+                ap, bvals<TV>(LT), Vec<TX>::y(h), Vec<TX>::x(h), Vec<TX>::xb(h), Vec<TX>::xp(h), Vec<TX>::c(h),
+                Vec<TX>::l(h), Vec<TX>::u(h), Vec<TX>::x0(h));
         NIR_LAUNCHED();
         if (check)
-            nir::k_bdual<T, true><<<cd1.grid, nir::kBlock, cd1.smem, s>>>(ad, View<T>::valA(h), View<T>::xb(h),
-                                                                        View<T>::y(h), View<T>::yp(h), View<T>::rl(h),
-                                                                        View<T>::ru(h), View<T>::y0(h));
+            nir::k_bdual<TV, TX, E, true><<<gd1, nir::kBlock, 0, s>>>(ad, bvals<TV>(LA), Vec<TX>::xb(h), Vec<TX>::y(h),
+                                                                      Vec<TX>::yp(h), Vec<TX>::rl(h), Vec<TX>::ru(h),
+                                                                      Vec<TX>::y0(h));
         else
-            nir::k_bdual<T, false><<<cd0.grid, nir::kBlock, cd0.smem, s>>>(ad, View<T>::valA(h), View<T>::xb(h),
-                                                                         View<T>::y(h), View<T>::yp(h), View<T>::rl(h),
-                                                                         View<T>::ru(h), View<T>::y0(h));
+            nir::k_bdual<TV, TX, E, false><<<gd0, nir::kBlock, 0, s>>>(ad, bvals<TV>(LA), Vec<TX>::xb(h),
+                                                                       Vec<TX>::y(h), Vec<TX>::yp(h), Vec<TX>::rl(h),
+                                                                       Vec<TX>::ru(h), Vec<TX>::y0(h));
         NIR_LAUNCHED();
         h->launches += 2;
     }
     nir::BatchArgs kr = bargs(B, false, KR, 0, 0, phase, 0.0);
-    nir::k_bkkt_rows<T><<<ckr.grid, nir::kBlock, ckr.smem, s>>>(kr, h->A.v64, View<T>::xp(h), View<T>::yp(h), h->dr,
-                                                                h->rl, h->ru);
+    nir::k_bkkt_rows<TX, E><<<gkr, nir::kBlock, 0, s>>>(kr, LA.v64, Vec<TX>::xp(h), Vec<TX>::yp(h), h->dr, h->rl,
+                                                        h->ru);
     nir::BatchArgs kc = bargs(B, true, KC, 0, 0, phase, 0.0);
-    nir::k_bkkt_cols<T><<<ckc.grid, nir::kBlock, ckc.smem, s>>>(kc, h->At.v64, View<T>::xp(h), View<T>::yp(h), h->dc,
-                                                                h->c, h->l, h->u);
+    nir::k_bkkt_cols<TX, E><<<gkc, nir::kBlock, 0, s>>>(kc, LT.v64, Vec<TX>::xp(h), Vec<TX>::yp(h), h->dc, h->c,
+                                                        h->l, h->u);
     NIR_LAUNCHED();
     nir::CtlArgs ca{};
     ca.K = K;
@@ -131,14 +188,35 @@ void launch_batch_chunk(nir_pdhg_batch* B, const SolveCfg& cfg, int phase) {
     ca.anchor_at_restart = cfg.p.restart_anchor ? 1 : 0;
     ca.weight_decades = cfg.p.primal_weight_decades;
     ca.hist = nullptr;
-    nir::BatchCtlArgs cb{P, D, KR, KC, B->nblkAt, B->nblkA, B->d_at_lo, B->d_a_lo, B->d_bnorm, B->d_cnorm, B->d_offset};
+    nir::BatchCtlArgs cb{P, D, KR, KC, LT.nblk, LA.nblk, LT.lo, LA.lo, B->d_bnorm, B->d_cnorm, B->d_offset};
     nir::k_bcontrol<<<B->count, nir::kBlock, 0, s>>>(ca, cb, B->insts);
-    nir::k_bapply_restart<T><<<grid_for(std::max(h->n, h->m)), nir::kBlock, 0, s>>>(
-        h->n, h->m, B->d_col_inst, B->d_row_inst, B->insts, phase, View<T>::x(h), View<T>::x0(h), View<T>::xp(h),
-        View<T>::y(h), View<T>::y0(h), View<T>::yp(h));
+    nir::k_bapply_restart<TX><<<grid_for(std::max(h->n, h->m)), nir::kBlock, 0, s>>>(
+        h->n, h->m, B->d_col_inst, B->d_row_inst, B->insts, phase, Vec<TX>::x(h), Vec<TX>::x0(h), Vec<TX>::xp(h),
+        Vec<TX>::y(h), Vec<TX>::y0(h), Vec<TX>::yp(h));
     nir::k_bsnap<<<1, nir::kBlock, 0, s>>>(B->count, B->insts, h->snap.ring, h->snap.d_seq);
     NIR_LAUNCHED();
     h->launches += 7;
+}
+
+template <typename TV, typename TX>
+void launch_batch_chunk(nir_pdhg_batch* B, const SolveCfg& cfg, int phase) {
+    with_run_len(B->cur->cap, [&](auto e) { launch_batch_chunk_e<TV, TX, decltype(e)::value>(B, cfg, phase); });
+}
+
+template <typename TV, typename TX>
+void warm_batch_cfgs(nir_pdhg_batch* B) {
+    nir_pdhg* h = B->h;
+    with_run_len(B->cur->cap, [&](auto e) {
+        constexpr int E = decltype(e)::value;
+        const int na = B->cur->a.nblk, nt = B->cur->at.nblk;
+        cta_grid(h, nir::k_bprimal<TV, TX, E, true>, nt);
+        cta_grid(h, nir::k_bprimal<TV, TX, E, false>, nt);
+        cta_grid(h, nir::k_bdual<TV, TX, E, true>, na);
+        cta_grid(h, nir::k_bdual<TV, TX, E, false>, na);
+        cta_grid(h, nir::k_bkkt_rows<TX, E>, na);
+        cta_grid(h, nir::k_bkkt_cols<TX, E>, nt);
+        cta_grid(h, nir::k_bchunk<TV, TX, E>, std::max(na, nt));
+    });
 }
 
 void batch_create_impl(nir_pdhg_batch* B, const nir_lp_view* lps, int count, int device) {
@@ -224,33 +302,22 @@ int batch_solve_impl(nir_pdhg_batch* B, const nir_pdhg_params& p, int (*poll)(vo
     const int n = h->n, m = h->m, I = B->count;
     B->solved = false;  // out_x serves as scratch until the final unscale
     if (p.algorithm != NIR_ALGO_PDLP) throw std::invalid_argument("the batch runs NIR_ALGO_PDLP only");
-    if (p.spmv_block_nnz > nir::kWarpCapMax) throw std::invalid_argument("spmv_block_nnz must be in [1, 256]");
     if (p.check_every < 1 || p.reflection < 0.0 || p.reflection > 1.0 || !(p.tol >= 0.0))
         throw std::invalid_argument("invalid parameters");
     const int cap = pick_cap(h, p);  // timed on the block-diagonal matrix
-    if (B->cap != cap) {
-        bool found = false;
-        for (const auto& l : B->layouts)
-            if (l.cap == cap) {
-                B->blkA = l.blkA;
-                B->blkAt = l.blkAt;
-                B->instA = l.instA;
-                B->instAt = l.instAt;
-                B->nblkA = l.nblkA;
-                B->nblkAt = l.nblkAt;
-                B->d_a_lo = l.a_lo;
-                B->d_at_lo = l.at_lo;
-                B->part = l.part;
-                found = true;
-            }
-        if (!found) {
-            batch_blocks(B, h->A.h_rp, B->row_off, cap, &B->blkA, &B->instA, &B->nblkA, &B->d_a_lo);
-            batch_blocks(B, h->At.h_rp, B->col_off, cap, &B->blkAt, &B->instAt, &B->nblkAt, &B->d_at_lo);
-            B->part = h->alloc<double>(6 * size_t(std::max(B->nblkA, 1)) + 6 * size_t(std::max(B->nblkAt, 1)));
-            B->layouts.push_back({cap, B->blkA, B->blkAt, B->instA, B->instAt, B->nblkA, B->nblkAt, B->d_a_lo,
-                                  B->d_at_lo, B->part});
+    if (!B->cur || B->cur->cap != cap) {
+        B->cur = nullptr;
+        for (auto& l : B->layouts)
+            if (l.cap == cap) B->cur = &l;
+        if (!B->cur) {
+            B->layouts.emplace_back();
+            nir_pdhg_batch::Layout& l = B->layouts.back();
+            l.cap = cap;
+            batch_blocks(B, h->A, B->row_off, cap, &l.a);
+            batch_blocks(B, h->At, B->col_off, cap, &l.at);
+            l.part = h->alloc<double>(6 * size_t(std::max(l.a.nblk, 1)) + 6 * size_t(std::max(l.at.nblk, 1)));
+            B->cur = &l;
         }
-        B->cap = cap;
     }
     SolveCfg cfg;
     cfg.p = p;
@@ -258,7 +325,22 @@ int batch_solve_impl(nir_pdhg_batch* B, const nir_pdhg_params& p, int (*poll)(vo
     cfg.halpern = 1;
     cfg.restarts = 1;
     cfg.mixed = (p.precision == NIR_PREC_MIXED) ? 1 : 0;
+    {
+        // persistent chunks on request, as for one LP
+        int coop = 0;
+        NIR_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, h->device));
+        const bool want = p.persistent == 1 || p.persistent == 2;
+        if (want && !coop) throw std::invalid_argument("persistent chunks need cooperative launch support");
+        cfg.persistent = want ? 1 : 0;
+        cfg.barrier_test = (want && p.persistent == 2) ? 1 : 0;
+        if (cfg.persistent) {
+            NIR_CUDA(cudaMemsetAsync(h->gs_count, 0, sizeof(unsigned), s));
+            NIR_CUDA(cudaMemsetAsync(h->gs_gen, 0, sizeof(unsigned), s));
+            NIR_CUDA(cudaMemsetAsync(h->gs_err, 0, sizeof(int), s));
+        }
+    }
     precondition(h, p, p.ruiz_iters > 0 || p.pock_chambolle);
+    batch_pad_values(B);
     // per-instance ||A_i||_2 by power iteration on the block-diagonal matrix
     const unsigned gwm = grid_for((long long)m * 32), gwn = grid_for((long long)n * 32);
     nir::k_power_start_batch<<<grid_for(n), nir::kBlock, 0, s>>>(n, B->d_col_inst, B->d_col_off, h->tmp_n);
@@ -313,30 +395,23 @@ int batch_solve_impl(nir_pdhg_batch* B, const nir_pdhg_params& p, int (*poll)(vo
         h->y32, h->y032, h->l32, h->u32);
     NIR_LAUNCHED();
     // occupancy queries before any capture
-    warp_cfg<float>(h, nir::k_bprimal<float, true>, B->nblkAt);
-    warp_cfg<float>(h, nir::k_bprimal<float, false>, B->nblkAt);
-    warp_cfg<float>(h, nir::k_bdual<float, true>, B->nblkA);
-    warp_cfg<float>(h, nir::k_bdual<float, false>, B->nblkA);
-    warp_cfg<double>(h, nir::k_bprimal<double, true>, B->nblkAt);
-    warp_cfg<double>(h, nir::k_bprimal<double, false>, B->nblkAt);
-    warp_cfg<double>(h, nir::k_bdual<double, true>, B->nblkA);
-    warp_cfg<double>(h, nir::k_bdual<double, false>, B->nblkA);
-    warp_cfg<double>(h, nir::k_bkkt_rows<float>, B->nblkA);
-    warp_cfg<double>(h, nir::k_bkkt_cols<float>, B->nblkAt);
-    warp_cfg<double>(h, nir::k_bkkt_rows<double>, B->nblkA);
-    warp_cfg<double>(h, nir::k_bkkt_cols<double>, B->nblkAt);
+    if (p.precision == NIR_PREC_FP32) warm_batch_cfgs<float, float>(B);
+    if (p.precision == NIR_PREC_MIXED) warm_batch_cfgs<float, double>(B);
+    if (p.precision != NIR_PREC_FP32) warm_batch_cfgs<double, double>(B);
     NIR_CUDA(cudaStreamSynchronize(s));
     const double t_setup = now_sec();
     const bool fp64_first = (p.precision == NIR_PREC_FP64);
-    auto run_phase = [&](int phase, bool f64) {
-        auto launch = [&, phase, f64]() {
-            if (f64) launch_batch_chunk<double>(B, cfg, phase);
-            else launch_batch_chunk<float>(B, cfg, phase);
+    // prec: 0 = (float values, float iterates), 1 = (float, double), 2 = (double, double)
+    auto run_phase = [&](int phase, int prec) {
+        auto launch = [&, phase, prec]() {
+            if (prec == 2) launch_batch_chunk<double, double>(B, cfg, phase);
+            else if (prec == 1) launch_batch_chunk<float, double>(B, cfg, phase);
+            else launch_batch_chunk<float, float>(B, cfg, phase);
         };
         const int per = 2 * cfg.K + 7;
-        if (p.use_graphs) {
+        if (p.use_graphs && !cfg.persistent) {
             KeyHash k;
-            k.add(chunk_key(h, cfg, phase, f64)).add(B->blkA).add(B->blkAt).add(B->part).add(B->insts);
+            k.add(chunk_key(h, cfg, phase, prec)).add(B->cur->a.blk).add(B->cur->at.blk).add(B->cur->part).add(B->insts);
             ChunkGraph& g = B->graphs[phase];
             if (!(g.ge && g.valid && g.key == k.h)) {
                 // capture into the handle's slot, then keep it with the batch
@@ -352,27 +427,22 @@ int batch_solve_impl(nir_pdhg_batch* B, const nir_pdhg_params& p, int (*poll)(vo
     LoopResult R;
     std::vector<long long> it_switch(I, -1);  // iteration of each instance's FP32->FP64 hand-over
     if (p.max_iters > 0) {
-        R = run_phase(0, fp64_first);
+        R = run_phase(0, fp64_first ? 2 : (p.precision == NIR_PREC_MIXED ? 1 : 0));
         if (!R.stopped_by_host && cfg.mixed && !R.last.done && R.last.phase == 1) {
             std::vector<nir::DevState> sw(I);
             d2h(h, sw.data(), B->insts, I * sizeof(nir::DevState));
             for (int i = 0; i < I; ++i)
                 if (!sw[i].done && sw[i].phase == 1) it_switch[i] = sw[i].iter;
-            // instances that stalled in FP32 carry on in FP64 (pure precision change)
-            nir::k_to_double<<<grid_for(n), nir::kBlock, 0, s>>>(n, h->x32, h->x64);
-            nir::k_to_double<<<grid_for(n), nir::kBlock, 0, s>>>(n, h->x032, h->x064);
-            nir::k_to_double<<<grid_for(n), nir::kBlock, 0, s>>>(n, h->xp32, h->xp64);
-            nir::k_to_double<<<grid_for(m), nir::kBlock, 0, s>>>(m, h->y32, h->y64);
-            nir::k_to_double<<<grid_for(m), nir::kBlock, 0, s>>>(m, h->y032, h->y064);
-            nir::k_to_double<<<grid_for(m), nir::kBlock, 0, s>>>(m, h->yp32, h->yp64);
-            NIR_LAUNCHED();
-            R = run_phase(1, true);
+            // instances whose FP32-value phase stalled carry on with the FP64
+            // values; their iterates are FP64 already (a pure precision change)
+            R = run_phase(1, 2);
         }
     }
     std::vector<nir::DevState> st(I);
     d2h(h, st.data(), B->insts, I * sizeof(nir::DevState));
     nir::k_bunscale_out<<<grid_for(std::max(n, m)), nir::kBlock, 0, s>>>(
-        n, m, B->d_col_inst, B->d_row_inst, B->insts, h->xp32, h->yp32, h->xp64, h->yp64, fp64_first ? 1 : 0, h->dc,
+        n, m, B->d_col_inst, B->d_row_inst, B->insts, h->xp32, h->yp32, h->xp64, h->yp64,
+        p.precision != NIR_PREC_FP32 ? 1 : 0, h->dc,
         h->dr, h->out_x, h->out_y);
     NIR_LAUNCHED();
     std::vector<double> x(n), y(m);

@@ -305,7 +305,7 @@ __global__ void __launch_bounds__(kBlock, iter_min_blocks<TA>()) k_spmv_adaptive
 // Scalars every iteration kernel needs, derived from DevState at launch.
 template <typename T>
 struct StepScalars {
-    T tau, sigma, w, onemw, rho;
+    T tau, sigma, isigma, w, onemw, rho;  // isigma = 1 / sigma: the dual step multiplies
 };
 
 template <typename T>
@@ -313,6 +313,7 @@ __device__ __forceinline__ StepScalars<T> step_scalars(const DevState* st, int i
     StepScalars<T> s;
     s.tau = T(st->tau);
     s.sigma = T(st->sigma);
+    s.isigma = T(1.0 / st->sigma);
     if (halpern) {
         const double k = double(st->k_base + i_in_chunk);
         s.w = T((k + 1.0) / (k + 2.0));
@@ -394,7 +395,7 @@ struct DualEpi {
     }
     __device__ void row(int i, T ax, const Pre& p) {
         const T yi = p.y;
-        const T pr = clamp_box(ax - yi / s.sigma, p.rl, p.ru);
+        const T pr = clamp_box(ax - yi * s.isigma, p.rl, p.ru);
         const T yp = yi + s.sigma * (pr - ax);
         T yn = yp;
         if (halpern) yn = s.w * ((T(1) + s.rho) * yp - s.rho * yi) + s.onemw * p.y0;
@@ -408,78 +409,6 @@ struct DualEpi {
         }
     }
 };
-
-struct IterArgs {
-    const int2* blk;
-    int nblk;
-    int cap;
-    const int* rp;
-    const int* ci;
-    double* part;
-    const DevState* st;
-    int i_in_chunk;
-    int halpern;
-    int phase;     // the kernel runs only while st->phase == phase
-    double rho;
-};
-
-// One primal / dual half-iteration over all warp row blocks (the body of
-// k_primal / k_dual and of the persistent chunk kernel's phases).
-template <typename T, bool CHECK, bool COH>
-__device__ __forceinline__ void primal_phase(const IterArgs& a, const T* __restrict__ val, const T* __restrict__ y,
-                                             T* __restrict__ x, T* __restrict__ xbar, T* __restrict__ xplus,
-                                             const T* __restrict__ c, const T* __restrict__ lo,
-                                             const T* __restrict__ up, const T* __restrict__ x0, double* s_red) {
-    PrimalEpi<T, CHECK> epi;
-    epi.x = x;
-    epi.xbar = xbar;
-    epi.xplus = xplus;
-    epi.c = c;
-    epi.lo = lo;
-    epi.up = up;
-    epi.x0 = x0;
-    epi.s = step_scalars<T>(a.st, a.i_in_chunk, a.halpern, a.rho);
-    epi.halpern = a.halpern;
-    rowblock_spmv<T, T, T, PrimalEpi<T, CHECK>, COH>(a.blk, a.nblk, a.cap, a.rp, a.ci, val, y, epi,
-                                                       reinterpret_cast<T*>(s_red));
-    if (CHECK) write_partials(epi, a.part, s_red);
-}
-
-template <typename T, bool CHECK, bool COH>
-__device__ __forceinline__ void dual_phase(const IterArgs& a, const T* __restrict__ val, const T* __restrict__ xbar,
-                                           T* __restrict__ y, T* __restrict__ yplus, const T* __restrict__ rl,
-                                           const T* __restrict__ ru, const T* __restrict__ y0, double* s_red) {
-    DualEpi<T, CHECK> epi;
-    epi.y = y;
-    epi.yplus = yplus;
-    epi.rl = rl;
-    epi.ru = ru;
-    epi.y0 = y0;
-    epi.s = step_scalars<T>(a.st, a.i_in_chunk, a.halpern, a.rho);
-    epi.halpern = a.halpern;
-    rowblock_spmv<T, T, T, DualEpi<T, CHECK>, COH>(a.blk, a.nblk, a.cap, a.rp, a.ci, val, xbar, epi,
-                                                     reinterpret_cast<T*>(s_red));
-    if (CHECK) write_partials(epi, a.part, s_red);
-}
-
-template <typename T, bool CHECK>
-__global__ void __launch_bounds__(kBlock, iter_min_blocks<T>()) k_primal(IterArgs a, const T* __restrict__ val, const T* __restrict__ y,
-                                                   T* __restrict__ x, T* __restrict__ xbar, T* __restrict__ xplus,
-                                                   const T* __restrict__ c, const T* __restrict__ lo,
-                                                   const T* __restrict__ up, const T* __restrict__ x0) {
-    __shared__ double s_red[kWarps];
-    if (a.st->done || a.st->phase != a.phase) return;
-    primal_phase<T, CHECK, false>(a, val, y, x, xbar, xplus, c, lo, up, x0, s_red);
-}
-
-template <typename T, bool CHECK>
-__global__ void __launch_bounds__(kBlock, iter_min_blocks<T>()) k_dual(IterArgs a, const T* __restrict__ val, const T* __restrict__ xbar,
-                                                 T* __restrict__ y, T* __restrict__ yplus, const T* __restrict__ rl,
-                                                 const T* __restrict__ ru, const T* __restrict__ y0) {
-    __shared__ double s_red[kWarps];
-    if (a.st->done || a.st->phase != a.phase) return;
-    dual_phase<T, CHECK, false>(a, val, xbar, y, yplus, rl, ru, y0, s_red);
-}
 
 // ---------------------------------------------------------------- KKT (FP64)
 
@@ -562,49 +491,6 @@ struct KktColEpi {
         q[3] += xv * xv;
     }
 };
-
-struct KktArgs {
-    const int2* blk;
-    int nblk;
-    int cap;
-    const int* rp;
-    const int* ci;
-    const double* val;  // scaled FP64 values
-    double* part;
-    const DevState* st;
-    int phase;
-};
-
-template <typename TX>
-__global__ void __launch_bounds__(kBlock) k_kkt_rows(KktArgs a, const TX* __restrict__ xplus, const TX* __restrict__ yplus,
-                                                     const double* __restrict__ dr, const double* __restrict__ rl,
-                                                     const double* __restrict__ ru) {
-    __shared__ double s_red[kWarps];
-    if (a.st->done || a.st->phase != a.phase) return;
-    KktRowEpi<TX> epi;
-    epi.dr = dr;
-    epi.rl = rl;
-    epi.ru = ru;
-    epi.yplus = yplus;
-    rowblock_spmv<double, double, TX>(a.blk, a.nblk, a.cap, a.rp, a.ci, a.val, xplus, epi, s_red);
-    write_partials(epi, a.part, s_red);
-}
-
-template <typename TX>
-__global__ void __launch_bounds__(kBlock) k_kkt_cols(KktArgs a, const TX* __restrict__ xplus, const TX* __restrict__ yplus,
-                                                     const double* __restrict__ dc, const double* __restrict__ c,
-                                                     const double* __restrict__ l, const double* __restrict__ u) {
-    __shared__ double s_red[kWarps];
-    if (a.st->done || a.st->phase != a.phase) return;
-    KktColEpi<TX> epi;
-    epi.dc = dc;
-    epi.c = c;
-    epi.l = l;
-    epi.u = u;
-    epi.xplus = xplus;
-    rowblock_spmv<double, double, TX>(a.blk, a.nblk, a.cap, a.rp, a.ci, a.val, yplus, epi, s_red);
-    write_partials(epi, a.part, s_red);
-}
 
 // ---------------------------------------------------------------- controller
 

@@ -2,28 +2,27 @@
 //
 // The instances are laid out block-diagonally in one handle: instance i
 // owns rows [row_off[i], row_off[i+1]) and columns [col_off[i],
-// col_off[i+1]), and its warp row blocks (which never cross an instance)
-// are contiguous.  Every instance keeps its own DevState on the device:
+// col_off[i+1]), and its CTA blocks (which never cross an instance) are
+// contiguous.  Every instance keeps its own DevState on the device:
 // step sizes, primal weight, Halpern counter, restart anchor, precision
 // phase and convergence flag.  The iteration kernels look up the instance
-// of each warp row block, skip converged instances, and in a check launch
+// of each CTA block, skip converged instances, and in a check launch
 // leave one partial sum per quantity and block; the controller then runs
 // one CTA per instance, reducing that instance's block range in a fixed
 // order (deterministic) and applying the same update as the single-LP
 // controller.
 #pragma once
 
-#include "k_adaptive.cuh"
+#include "k_iter.cuh"
+#include "k_setup.cuh"
 
 namespace nir {
 
 struct BatchArgs {
-    const int2* blk;
+    const int4* blk;      // CTA-block descriptors; .w = the block's instance
     int nblk;
-    int cap;
     const int* rp;
-    const int* ci;
-    const int* blk_inst;  // instance of each warp row block
+    const int* ci;        // padded column indices
     double* part;         // per-block partials: part[q * nblk + block]
     const DevState* inst;
     int i_in_chunk;
@@ -34,74 +33,46 @@ struct BatchArgs {
 
 __device__ __forceinline__ bool inst_active(const DevState& s, int phase) { return !s.done && s.phase == phase; }
 
+// Reduces each per-thread quantity over the CTA into the block's partial
+// slot and clears it for the next block.
 template <class Epi>
-__device__ __forceinline__ void flush_block_partials(Epi& epi, double* __restrict__ part, int nblk, int b) {
-    const int lane = threadIdx.x & 31;
+__device__ __forceinline__ void flush_block_partials(Epi& epi, double* __restrict__ part, int nblk, int b,
+                                                     double* s_red) {
 #pragma unroll
     for (int q = 0; q < Epi::NQ; ++q) {
-        const double v = (Epi::kLastIsMax && q == Epi::NQ - 1) ? warp_max(epi.q[q]) : warp_sum(epi.q[q]);
-        if (lane == 0) part[q * nblk + b] = v;
+        const double v = (Epi::kLastIsMax && q == Epi::NQ - 1) ? block_max(epi.q[q], s_red) : block_sum(epi.q[q], s_red);
+        if (threadIdx.x == 0) part[q * nblk + b] = v;
         epi.q[q] = 0.0;
     }
 }
 
-// rowblock_spmv over the batch: per block, the instance decides whether the
-// block runs and with which scalars (SetFn(epi, DevState&)).
-template <typename TA, typename TV, typename TX, class Epi, class SetFn>
-__device__ __forceinline__ void rowblock_spmv_batch(const BatchArgs& a, const TV* __restrict__ val,
-                                                    const TX* __restrict__ x, Epi& epi, SetFn set) {
-    extern __shared__ __align__(16) unsigned char nir_smem[];
-    const int w = threadIdx.x >> 5;
-    TA* s_prod = reinterpret_cast<TA*>(nir_smem) + w * kWarpCapMax;
-    const int G = gridDim.x * kWarps;
-    int b = blockIdx.x * kWarps + w;
-    if (b >= a.nblk) return;
-    int2 d0 = __ldg(a.blk + b), d1 = __ldg(a.blk + b + 1);
-    int inst = __ldg(a.blk_inst + b);
-    bool act = inst_active(a.inst[inst], a.phase);
-    int c[kWarpU];
-    TV v[kWarpU];
-    stream_load<TV>(d0, d1, act ? a.cap : -1, a.ci, val, c, v);
-    for (;;) {
-        const int bn = b + G;
-        const bool has_next = bn < a.nblk;
-        int2 n0 = make_int2(0, 0), n1 = make_int2(0, 0);
-        int inst_n = 0;
-        bool act_n = false;
-        if (has_next) {
-            n0 = __ldg(a.blk + bn);
-            n1 = __ldg(a.blk + bn + 1);
-            inst_n = __ldg(a.blk_inst + bn);
-            act_n = inst_active(a.inst[inst_n], a.phase);
-        }
-        int cn[kWarpU];
-        TV vn[kWarpU];
-        stream_load<TV>(n0, n1, act_n ? a.cap : -1, a.ci, val, cn, vn);
-        if (act) {
-            set(epi, a.inst[inst]);
-            warp_process<TA, TV, TX>(d0, d1, a.cap, a.rp, a.ci, val, x, epi, s_prod, c, v);
-            if (Epi::NQ > 0) flush_block_partials(epi, a.part, a.nblk, b);
-        }
-        if (!has_next) break;
-#pragma unroll
-        for (int q = 0; q < kWarpU; ++q) {
-            c[q] = cn[q];
-            v[q] = vn[q];
-        }
-        d0 = n0;
-        d1 = n1;
-        inst = inst_n;
-        act = act_n;
-        b = bn;
+// cta_spmv over the batch: per block, the instance decides whether the
+// block runs and with which scalars (SetFn(epi, DevState&)).  The decision
+// is the same for every thread of the CTA.
+template <typename TA, typename TV, typename TX, int E, class Epi, bool COH = false, class SetFn>
+__device__ __forceinline__ void cta_spmv_batch(const BatchArgs& a, const TV* __restrict__ val,
+                                               const TX* __restrict__ x, Epi& epi, SetFn set, CtaShared<TA>* sm,
+                                               double* s_red) {
+    int k = 0;
+    for (int b = blockIdx.x; b < a.nblk; b += gridDim.x) {
+        const int4 d0 = __ldg(a.blk + b), d1 = __ldg(a.blk + b + 1);
+        const DevState& s = a.inst[d0.w];
+        if (!inst_active(s, a.phase)) continue;
+        set(epi, s);
+        cta_block<TA, TV, TX, E, Epi, COH>(d0, d1, a.rp, a.ci, val, x, epi, sm[k & 1]);
+        ++k;
+        if (Epi::NQ > 0) flush_block_partials(epi, a.part, a.nblk, b, s_red);
     }
 }
 
-template <typename T, bool CHECK>
-__global__ void __launch_bounds__(kBlock, iter_min_blocks<T>()) k_bprimal(BatchArgs a, const T* __restrict__ val, const T* __restrict__ y,
-                                                    T* __restrict__ x, T* __restrict__ xbar, T* __restrict__ xplus,
-                                                    const T* __restrict__ c, const T* __restrict__ lo,
-                                                    const T* __restrict__ up, const T* __restrict__ x0) {
-    PrimalEpi<T, CHECK> epi;
+template <typename TV, typename TX, int E, bool CHECK>
+__global__ void __launch_bounds__(kBlock, cta_min_blocks<TX, E>())
+    k_bprimal(BatchArgs a, const TV* __restrict__ val, const TX* __restrict__ y, TX* __restrict__ x,
+              TX* __restrict__ xbar, TX* __restrict__ xplus, const TX* __restrict__ c, const TX* __restrict__ lo,
+              const TX* __restrict__ up, const TX* __restrict__ x0) {
+    __shared__ CtaShared<TX> sm[2];
+    __shared__ double s_red[kWarps];
+    PrimalEpi<TX, CHECK> epi;
     epi.x = x;
     epi.xbar = xbar;
     epi.xplus = xplus;
@@ -110,52 +81,58 @@ __global__ void __launch_bounds__(kBlock, iter_min_blocks<T>()) k_bprimal(BatchA
     epi.up = up;
     epi.x0 = x0;
     epi.halpern = a.halpern;
-    rowblock_spmv_batch<T, T, T>(a, val, y, epi, [&](PrimalEpi<T, CHECK>& e, const DevState& s) {
-        e.s = step_scalars<T>(&s, a.i_in_chunk, a.halpern, a.rho);
-    });
+    cta_spmv_batch<TX, TV, TX, E>(a, val, y, epi, [&](PrimalEpi<TX, CHECK>& e, const DevState& s) {
+        e.s = step_scalars<TX>(&s, a.i_in_chunk, a.halpern, a.rho);
+    }, sm, s_red);
 }
 
-template <typename T, bool CHECK>
-__global__ void __launch_bounds__(kBlock, iter_min_blocks<T>()) k_bdual(BatchArgs a, const T* __restrict__ val, const T* __restrict__ xbar,
-                                                  T* __restrict__ y, T* __restrict__ yplus, const T* __restrict__ rl,
-                                                  const T* __restrict__ ru, const T* __restrict__ y0) {
-    DualEpi<T, CHECK> epi;
+template <typename TV, typename TX, int E, bool CHECK>
+__global__ void __launch_bounds__(kBlock, cta_min_blocks<TX, E>())
+    k_bdual(BatchArgs a, const TV* __restrict__ val, const TX* __restrict__ xbar, TX* __restrict__ y,
+            TX* __restrict__ yplus, const TX* __restrict__ rl, const TX* __restrict__ ru, const TX* __restrict__ y0) {
+    __shared__ CtaShared<TX> sm[2];
+    __shared__ double s_red[kWarps];
+    DualEpi<TX, CHECK> epi;
     epi.y = y;
     epi.yplus = yplus;
     epi.rl = rl;
     epi.ru = ru;
     epi.y0 = y0;
     epi.halpern = a.halpern;
-    rowblock_spmv_batch<T, T, T>(a, val, xbar, epi, [&](DualEpi<T, CHECK>& e, const DevState& s) {
-        e.s = step_scalars<T>(&s, a.i_in_chunk, a.halpern, a.rho);
-    });
+    cta_spmv_batch<TX, TV, TX, E>(a, val, xbar, epi, [&](DualEpi<TX, CHECK>& e, const DevState& s) {
+        e.s = step_scalars<TX>(&s, a.i_in_chunk, a.halpern, a.rho);
+    }, sm, s_red);
 }
 
-template <typename TX>
-__global__ void __launch_bounds__(kBlock) k_bkkt_rows(BatchArgs a, const double* __restrict__ val,
-                                                      const TX* __restrict__ xplus, const TX* __restrict__ yplus,
-                                                      const double* __restrict__ dr, const double* __restrict__ rl,
-                                                      const double* __restrict__ ru) {
+template <typename TX, int E>
+__global__ void __launch_bounds__(kBlock, cta_min_blocks<double, E>())
+    k_bkkt_rows(BatchArgs a, const double* __restrict__ val, const TX* __restrict__ xplus,
+                const TX* __restrict__ yplus, const double* __restrict__ dr, const double* __restrict__ rl,
+                const double* __restrict__ ru) {
+    __shared__ CtaShared<double> sm[2];
+    __shared__ double s_red[kWarps];
     KktRowEpi<TX> epi;
     epi.dr = dr;
     epi.rl = rl;
     epi.ru = ru;
     epi.yplus = yplus;
-    rowblock_spmv_batch<double, double, TX>(a, val, xplus, epi, [](KktRowEpi<TX>&, const DevState&) {});
+    cta_spmv_batch<double, double, TX, E>(a, val, xplus, epi, [](KktRowEpi<TX>&, const DevState&) {}, sm, s_red);
 }
 
-template <typename TX>
-__global__ void __launch_bounds__(kBlock) k_bkkt_cols(BatchArgs a, const double* __restrict__ val,
-                                                      const TX* __restrict__ xplus, const TX* __restrict__ yplus,
-                                                      const double* __restrict__ dc, const double* __restrict__ c,
-                                                      const double* __restrict__ l, const double* __restrict__ u) {
+template <typename TX, int E>
+__global__ void __launch_bounds__(kBlock, cta_min_blocks<double, E>())
+    k_bkkt_cols(BatchArgs a, const double* __restrict__ val, const TX* __restrict__ xplus,
+                const TX* __restrict__ yplus, const double* __restrict__ dc, const double* __restrict__ c,
+                const double* __restrict__ l, const double* __restrict__ u) {
+    __shared__ CtaShared<double> sm[2];
+    __shared__ double s_red[kWarps];
     KktColEpi<TX> epi;
     epi.dc = dc;
     epi.c = c;
     epi.l = l;
     epi.u = u;
     epi.xplus = xplus;
-    rowblock_spmv_batch<double, double, TX>(a, val, yplus, epi, [](KktColEpi<TX>&, const DevState&) {});
+    cta_spmv_batch<double, double, TX, E>(a, val, yplus, epi, [](KktColEpi<TX>&, const DevState&) {}, sm, s_red);
 }
 
 struct BatchCtlArgs {

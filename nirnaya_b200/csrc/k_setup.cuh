@@ -263,6 +263,22 @@ __global__ void k_promote(int n, int m, const float* __restrict__ xp32, const fl
     }
 }
 
+// Fresh start of the FP64 polish at the last evaluated point: iterate and
+// anchor become (x+, y+).
+__global__ void k_restart_at(int n, int m, const double* __restrict__ xp, const double* __restrict__ yp,
+                             double* __restrict__ x, double* __restrict__ x0, double* __restrict__ y,
+                             double* __restrict__ y0) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) {
+        x[t] = xp[t];
+        x0[t] = xp[t];
+    }
+    if (t < m) {
+        y[t] = yp[t];
+        y0[t] = yp[t];
+    }
+}
+
 // Original-space output: x = dc * x^, y = dr * y^.
 template <typename T>
 __global__ void k_unscale_out(int n, int m, const T* __restrict__ xp, const T* __restrict__ yp,

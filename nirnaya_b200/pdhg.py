@@ -63,7 +63,7 @@ class Info(C.Structure):
         ("rel_primal", C.c_double), ("rel_dual", C.c_double), ("rel_gap", C.c_double),
         ("max_rel_row_viol", C.c_double), ("primal_weight", C.c_double), ("step_size", C.c_double),
         ("setup_seconds", C.c_double), ("solve_seconds", C.c_double), ("time_to_fp64_seconds", C.c_double),
-        ("kernel_launches", C.c_int32), ("pad_", C.c_int32), ("iterations_to_tol", C.c_int64),
+        ("kernel_launches", C.c_int32), ("parallel_groups", C.c_int32), ("iterations_to_tol", C.c_int64),
     ]
 
     def as_dict(self):
@@ -88,8 +88,13 @@ EXPORTED = [
     "nir_pdhg_solve_lp", "nir_pdhg_free", "nir_pdhg_last_error", "nir_pdhg_spmv", "nir_pdhg_time_spmv",
     "nir_pdhg_set_profiling", "nir_pdhg_kernel_times", "nir_pdhg_get_layout", "nir_pdhg_history",
     "nir_pdhg_reference_solve_noalloc", "nir_pdhg_batch_create", "nir_pdhg_batch_solve", "nir_pdhg_batch_free",
-    "nir_pdhg_verify", "nir_pdhg_batch_verify",
+    "nir_pdhg_verify", "nir_pdhg_batch_verify", "nir_pdhg_spmv_kernel", "nir_pdhg_time_kernel",
+    "nir_pdhg_time_iteration", "nir_pdhg_parallel_groups",
 ]
+
+# Kernel kinds of nir_pdhg_spmv_kernel / nir_pdhg_time_kernel.
+K_REF, K_WARP64, K_WARP32, K_CTA64, K_CTA32, K_CTA_MIXED = 0, 1, 2, 3, 4, 5
+K_CEIL_GATHER64, K_CEIL_GATHER32, K_CEIL_STREAM64, K_CEIL_STREAM32 = 6, 7, 8, 9
 
 _lib = None
 
@@ -112,6 +117,10 @@ def lib():
         L.nir_pdhg_last_error.restype = C.c_char_p
         L.nir_pdhg_spmv.argtypes = [C.c_void_p, C.c_int, C.c_int, D, D]
         L.nir_pdhg_time_spmv.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, D]
+        L.nir_pdhg_spmv_kernel.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, D, D]
+        L.nir_pdhg_time_kernel.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, D]
+        L.nir_pdhg_time_iteration.argtypes = [C.c_void_p, C.c_int, C.c_int, D, D, D]
+        L.nir_pdhg_parallel_groups.argtypes = [VP, C.POINTER(C.c_int32), D, C.POINTER(C.c_int32)]
         L.nir_pdhg_set_profiling.argtypes = [C.c_void_p, C.c_int]
         L.nir_pdhg_kernel_times.argtypes = [C.c_void_p, C.POINTER(KernelTime)]
         L.nir_pdhg_get_layout.argtypes = [C.c_void_p, C.POINTER(Layout)]
@@ -132,6 +141,20 @@ def default_params(**overrides) -> Params:
     for k, v in overrides.items():
         setattr(p, k, v)
     return p
+
+
+def parallel_groups(lp: LP):
+    """(rep_of, lam, groups): the parallel-column groups the engine
+    re-expresses before a PDHG / PDLP solve (nir_pdhg_parallel_groups;
+    host only)."""
+    rep = np.zeros(lp.ncol, np.int32)
+    lam = np.zeros(lp.ncol)
+    g = C.c_int32()
+    rc = lib().nir_pdhg_parallel_groups(C.byref(lp.view()), rep.ctypes.data_as(C.POINTER(C.c_int32)),
+                                        lam.ctypes.data_as(C.POINTER(C.c_double)), C.byref(g))
+    if rc != 0:
+        raise RuntimeError(last_error())
+    return rep, lam, g.value
 
 
 def _dptr(a):
@@ -213,6 +236,35 @@ class Engine:
         if rc != 0:
             raise RuntimeError(last_error())
         return us.value
+
+    def spmv_kernel(self, x, transpose: bool, kernel: int, block_nnz: int = 0):
+        """One SpMV of the unscaled matrix with a chosen kernel kind (K_*)."""
+        nout = self.lp.ncol if transpose else self.lp.nrow
+        y = np.zeros(nout)
+        rc = lib().nir_pdhg_spmv_kernel(self._h, int(transpose), kernel, block_nnz,
+                                        _dptr(np.ascontiguousarray(x, np.float64)), _dptr(y))
+        if rc != 0:
+            raise RuntimeError(last_error())
+        return y
+
+    def time_kernel(self, transpose: bool, kernel: int, block_nnz: int = 0, reps: int = 20,
+                    flush_l2: bool = True) -> float:
+        """Mean CUDA-event time (us) of one launch of a kernel kind (K_*),
+        including the row-less ceilings."""
+        us = C.c_double()
+        rc = lib().nir_pdhg_time_kernel(self._h, int(transpose), kernel, block_nnz, reps, int(flush_l2), C.byref(us))
+        if rc != 0:
+            raise RuntimeError(last_error())
+        return us.value
+
+    def time_iteration(self, precision: int, reps: int = 200):
+        """(primal_us, dual_us, pair_us): steady-state event times of the
+        fused iteration kernels after a solve (nir_pdhg_time_iteration)."""
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        rc = lib().nir_pdhg_time_iteration(self._h, precision, reps, C.byref(a), C.byref(b), C.byref(c))
+        if rc != 0:
+            raise RuntimeError(last_error())
+        return a.value, b.value, c.value
 
     def set_profiling(self, on: bool):
         lib().nir_pdhg_set_profiling(self._h, int(on))

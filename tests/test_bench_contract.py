@@ -25,8 +25,12 @@ def test_algorithmic_bytes_of_the_fused_kernels():
     assert bench.dual_bytes(_Lp, 8) == 74461612
     assert bench.primal_bytes(_Lp, 4) == 58841076
     assert bench.dual_bytes(_Lp, 4) == 47641076
+    # FP32 values with FP64 vectors: 8 bytes per nonzero streamed, vectors at 8
+    assert bench.dual_bytes(_Lp, 8, 4) == bench.dual_bytes(_Lp, 8) - 4 * 5005134
+    assert bench.primal_bytes(_Lp, 8, 4) == bench.primal_bytes(_Lp, 8) - 4 * 5005134
     # plain SpMV: (index + value) per nonzero, row pointers, x read, y written
     assert bench.spmv_bytes(_Lp, False, 4) == 8 * 5005134 + 4 * 200001 + 4 * 500000 + 4 * 200000
+    assert bench.spmv_bytes_w(_Lp, False, 4, 8) == 8 * 5005134 + 4 * 200001 + 8 * 500000 + 8 * 200000
 
 
 def test_committed_profile_lookups():
@@ -55,6 +59,7 @@ def test_reference_arm_prints_one_contract_line():
     assert line["impl"] == "reference" and line["unit"] == "s" and line["higher_is_better"] is False
     assert line["value"] > 0 and line["e2e"]["value"] == line["value"]
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+    assert line["lower_bound"] in (True, False) and line["per_iteration_s"] > 0
     cb = line["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["cores"] >= 1 and "PdhgSolver::solve" in cb["sample"]
     assert set(cb["iterations_per_s_by_threads"]) >= {"1"}

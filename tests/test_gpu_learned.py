@@ -20,7 +20,7 @@ pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not has_gpu(), reason="needs a
 
 def test_warm_start_reaches_the_same_tolerance_in_fewer_iterations():
     fam = LW.BlendFamily(m=2000, n=5000, nnz=40000, family_seed=0)
-    p = pdhg.default_params(tol=1e-6, max_iters=200000, spmv_block_nnz=64)
+    p = pdhg.default_params(tol=1e-6, max_iters=200000, spmv_block_nnz=256)
     with pdhg.Engine(fam.base) as eng:
         train = LW.solve_family(fam, range(1000, 1512), p, engine=eng)
         assert (train.status == pdhg.OPTIMAL).all()
