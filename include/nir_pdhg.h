@@ -92,8 +92,10 @@ typedef struct nir_pdhg_params {
     int32_t polish_stall_checks;  /* MIXED: FP64 polish after this many checks
                                      without a 0.8x improvement of the best KKT   (40)   */
     double polish_switch_kkt;     /* MIXED: ... or as soon as KKT <= this        (0)     */
-    int32_t spmv_block_nnz;       /* nonzeros per CTA block of the SpMV: 256, 512, 1024 or
-                                     2048 (256 threads x 1, 2, 4, 8); 0 = autotuned   (0) */
+    int32_t spmv_block_nnz;       /* SpMV layout of both orientations: 32, 64, 128 or 256 =
+                                     warp row blocks of that many nonzeros, 1024 = CTA
+                                     blocks with a segmented reduction; 0 = autotuned
+                                     per orientation                               (0) */
     int32_t use_graphs;           /* capture launch chunks in CUDA graphs        (1)     */
     int32_t verbose;              /* 1 = one line per check on stderr            (0)     */
     int32_t restart_anchor;       /* residual the restart tests compare with: 0 = first
@@ -249,9 +251,12 @@ int nir_pdhg_history(nir_pdhg* h, double* out, int max_entries);
 typedef struct nir_pdhg_layout {
     int32_t nrow, ncol;
     int64_t nnz;
-    int32_t blocks_a, blocks_at;        /* CTA blocks of A and A' of the last solve */
-    int32_t block_nnz;                  /* their capacity in nonzeros             */
+    int32_t blocks_a, blocks_at;        /* SpMV blocks of A and A' of the last solve */
+    int32_t block_nnz;                  /* nonzeros per block of A: 32..256 for warp row
+                                           blocks, 1024 for CTA blocks               */
     int64_t device_bytes;               /* device memory held by the handle    */
+    int32_t block_nnz_at;               /* the same for A'                         */
+    int32_t pad_;
 } nir_pdhg_layout;
 int nir_pdhg_get_layout(nir_pdhg* h, nir_pdhg_layout* out);
 

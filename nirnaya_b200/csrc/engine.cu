@@ -102,6 +102,12 @@ struct DevBuf {
     size_t bytes = 0;
 };
 
+// The per-orientation layout choice of a solve.
+struct LayChoice {
+    int lay_a = nir::kLayWarp, cap_a = 256;    // A (dual half-iteration, KKT rows)
+    int lay_at = nir::kLayWarp, cap_at = 256;  // A' (primal half-iteration, KKT columns)
+};
+
 // Groups of parallel columns of an LP (engine_parallel.cuh).
 struct ParallelGroups {
     std::vector<int> rep_of;  // per column: its representative, or -1
@@ -147,6 +153,7 @@ struct Orient {
     };
     std::deque<Cta> ctas;
     int it = -1;
+    int lay = -1;  // layout the iteration and KKT kernels use: nir::kLayWarp (blk, cap) or nir::kLayCta (ctas[it])
     const Cta& cur() const {
         if (it < 0) throw std::logic_error("internal: no CTA layout in use");
         return ctas[size_t(it)];
@@ -199,7 +206,8 @@ struct nir_pdhg {
     long long device_bytes = 0;
     ChunkGraph graphs[3];
     long long last_iters = 0;
-    int tuned_cap[3] = {0, 0, 0};  // autotuned CTA-block capacity per NIR_PREC_*
+    LayChoice tuned[3];                    // autotuned layouts per NIR_PREC_*
+    bool tuned_ok[3] = {false, false, false};
     int sms = 148;
     struct Occ {
         const void* fn;
@@ -351,15 +359,6 @@ void cta_orig_values(nir_pdhg* h, Orient& o, Orient::Cta& c) {
         NIR_LAUNCHED();
     }
     NIR_CUDA(cudaStreamSynchronize(s));
-}
-
-// CTA-block capacity without timing: the largest of 256 E (E = 1, 2, 4, 8)
-// that still gives every SM about four blocks.
-int auto_cta_cap(const nir_pdhg* h) {
-    const long long per = h->nnz / (4LL * std::max(h->sms, 1));
-    int cap = 256;
-    while (cap < 2048 && cap * 2 <= per) cap *= 2;
-    return cap;
 }
 
 // Warp row-block capacity: 256 nonzeros (8 per lane) when the matrix gives
@@ -649,66 +648,91 @@ struct Vec<double> {
     static const double* ru(nir_pdhg* h) { return h->ru64; }
 };
 
-// Scaled values of a CTA layout's padded stream by type.
-template <typename TV>
-const TV* vals(const Orient::Cta& L);
-template <>
-const float* vals<float>(const Orient::Cta& L) {
-    return L.v32;
-}
-template <>
-const double* vals<double>(const Orient::Cta& L) {
-    return L.v64;
+// The layout an orientation's iteration and KKT kernels use (o.lay) as the
+// kernels see it, and its scaled values: the CSR's own arrays for the warp
+// layout, the padded stream for the CTA layout.
+nir::Lay lay_of(const Orient& o) {
+    if (o.lay == nir::kLayWarp) return nir::Lay{o.blk, o.nblk, o.cap, o.rp, o.ci};
+    const Orient::Cta& L = o.cur();
+    return nir::Lay{L.blk, L.nblk, 0, o.rp, L.ci};
 }
 
-// Persistent grid of a CTA-block kernel: the resident CTAs, at most one per
-// block.  The occupancy query runs once per kernel (outside any capture).
-template <typename K>
-int cta_grid(nir_pdhg* h, K* kernel, int nblk) {
+template <typename TV>
+const TV* vals_of(const Orient& o);
+template <>
+const float* vals_of<float>(const Orient& o) {
+    return o.lay == nir::kLayWarp ? o.v32 : o.cur().v32;
+}
+template <>
+const double* vals_of<double>(const Orient& o) {
+    return o.lay == nir::kLayWarp ? o.v64 : o.cur().v64;
+}
+
+int lay_nblk(const Orient& o) { return o.lay == nir::kLayWarp ? o.nblk : o.cur().nblk; }
+
+// Dynamic shared memory of a kernel over a layout (the warp layout's
+// product slices; the CTA layout's shared memory is static).
+template <int LAY, typename TA>
+constexpr size_t lay_smem() {
+    return LAY == nir::kLayWarp ? size_t(nir::warp_smem_bytes<TA>()) : size_t(0);
+}
+
+// Persistent grid of a layout kernel: as many CTAs as are resident at once,
+// at most one warp per warp row block (warp layout) or one CTA per block
+// (CTA layout).  The occupancy query runs once per kernel (outside any
+// stream capture).
+template <int LAY, typename TA, typename K>
+int lay_grid(nir_pdhg* h, K* kernel, int nblk) {
+    const size_t smem = lay_smem<LAY, TA>();
     int per = 0;
     for (auto& e : h->occ)
-        if (e.fn == (const void*)kernel && e.smem == 0) per = e.per_sm;
+        if (e.fn == (const void*)kernel && e.smem == smem) per = e.per_sm;
     if (per == 0) {
-        NIR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, nir::kBlock, 0));
+        NIR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, nir::kBlock, smem));
         per = std::max(per, 1);
-        h->occ.push_back({(const void*)kernel, 0, per});
+        h->occ.push_back({(const void*)kernel, smem, per});
     }
-    return std::max(1, std::min(nblk, per * h->sms));
+    const int need = LAY == nir::kLayWarp ? std::max(1, (nblk + nir::kWarps - 1) / nir::kWarps) : std::max(1, nblk);
+    return std::min(need, per * h->sms);
 }
 
-// Run length of a CTA-block capacity.
-inline int run_len(int cap) {
-    if (cap != 256 && cap != 512 && cap != 1024 && cap != 2048)
-        throw std::invalid_argument("CTA block capacity must be 256, 512, 1024 or 2048");
-    return cap / nir::kBlock;
-}
-
-// Calls f(std::integral_constant<int, E>{}) for the run length of cap.
+// Calls f(LP, LD) with the layouts of A' (primal) and A (dual) as
+// std::integral_constant values.
 template <class F>
-void with_run_len(int cap, F&& f) {
-    switch (run_len(cap)) {
-        case 1: f(std::integral_constant<int, 1>{}); break;
-        case 2: f(std::integral_constant<int, 2>{}); break;
-        case 4: f(std::integral_constant<int, 4>{}); break;
-        default: f(std::integral_constant<int, 8>{}); break;
-    }
+void with_lays(const nir_pdhg* h, F&& f) {
+    using W = std::integral_constant<int, nir::kLayWarp>;
+    using Cc = std::integral_constant<int, nir::kLayCta>;
+    const bool pc = h->At.lay == nir::kLayCta, dc = h->A.lay == nir::kLayCta;
+    if (pc && dc) f(Cc{}, Cc{});
+    else if (pc) f(Cc{}, W{});
+    else if (dc) f(W{}, Cc{});
+    else f(W{}, W{});
 }
 
-// The CTA layouts the iteration kernels use: capacity `cap` in both
-// orientations (built on first use).
-void use_cta(nir_pdhg* h, int cap) {
-    for (Orient* o : {&h->A, &h->At}) {
-        cta_layout(h, *o, cap);
-        for (size_t k = 0; k < o->ctas.size(); ++k)
-            if (o->ctas[k].cap == cap) o->it = int(k);
+constexpr int kCtaCap = 256 * nir::kLayCta;  // nonzeros per block of the CTA layout
+
+// Sets up the chosen layouts (built on first use).
+void use_layouts(nir_pdhg* h, const LayChoice& c) {
+    for (int t = 0; t < 2; ++t) {
+        Orient& o = t ? h->At : h->A;
+        const int lay = t ? c.lay_at : c.lay_a, cap = t ? c.cap_at : c.cap_a;
+        if (lay == nir::kLayWarp) {
+            set_blocks(h, o, cap);
+        } else {
+            cta_layout(h, o, kCtaCap);
+            for (size_t k = 0; k < o.ctas.size(); ++k)
+                if (o.ctas[k].cap == kCtaCap) o.it = int(k);
+        }
+        o.lay = lay;
     }
 }
 
 // Copies the scaled values (written by precondition) into the padded
-// streams of the layouts in use.
+// streams of the orientations that use the CTA layout.
 void pad_scaled(nir_pdhg* h) {
     cudaStream_t s = h->stream;
     for (Orient* o : {&h->A, &h->At}) {
+        if (o->lay != nir::kLayCta) continue;
         const Orient::Cta& L = o->cur();
         if (L.nblk <= 0 || o->nnz <= 0) continue;
         const unsigned g = unsigned(std::max(1, std::min(L.nblk, 4 * h->sms)));
@@ -721,27 +745,31 @@ void pad_scaled(nir_pdhg* h) {
 
 // The two FP64 KKT passes of a check over the layouts in use, at (xp, yp)
 // of type TX; returns their grids (the number of partials each wrote).
-template <typename TX, int E>
-void launch_kkt_e(nir_pdhg* h, int phase, double* partKR, double* partKC, const TX* xp, const TX* yp, int* gkr,
-                  int* gkc) {
-    cudaStream_t s = h->stream;
-    const Orient::Cta& LA = h->A.cur();
-    const Orient::Cta& LT = h->At.cur();
-    *gkr = cta_grid(h, nir::k_kkt_rows<TX, E>, LA.nblk);
-    *gkc = cta_grid(h, nir::k_kkt_cols<TX, E>, LT.nblk);
-    nir::KktArgs kr{LA.blk, LA.nblk, h->A.rp, LA.ci, LA.v64, partKR, h->st, phase};
-    nir::k_kkt_rows<TX, E><<<*gkr, nir::kBlock, 0, s>>>(kr, xp, yp, h->dr, h->rl, h->ru);
-    nir::KktArgs kc{LT.blk, LT.nblk, h->At.rp, LT.ci, LT.v64, partKC, h->st, phase};
-    nir::k_kkt_cols<TX, E><<<*gkc, nir::kBlock, 0, s>>>(kc, xp, yp, h->dc, h->c, h->l, h->u);
-    NIR_LAUNCHED();
-    h->launches += 2;
-}
-
 template <typename TX>
 void launch_kkt(nir_pdhg* h, int phase, double* partKR, double* partKC, const TX* xp, const TX* yp, int* gkr,
                 int* gkc) {
-    with_run_len(h->A.cur().cap,
-                 [&](auto e) { launch_kkt_e<TX, decltype(e)::value>(h, phase, partKR, partKC, xp, yp, gkr, gkc); });
+    cudaStream_t s = h->stream;
+    with_lays(h, [&](auto lp, auto ld) {
+        constexpr int LP = decltype(lp)::value, LD = decltype(ld)::value;
+        *gkr = lay_grid<LD, double>(h, nir::k_kkt_rows<LD, TX>, lay_nblk(h->A));
+        *gkc = lay_grid<LP, double>(h, nir::k_kkt_cols<LP, TX>, lay_nblk(h->At));
+        nir::KktArgs kr{lay_of(h->A), vals_of<double>(h->A), partKR, h->st, phase};
+        nir::k_kkt_rows<LD, TX><<<*gkr, nir::kBlock, lay_smem<LD, double>(), s>>>(kr, xp, yp, h->dr, h->rl, h->ru);
+        nir::KktArgs kc{lay_of(h->At), vals_of<double>(h->At), partKC, h->st, phase};
+        nir::k_kkt_cols<LP, TX><<<*gkc, nir::kBlock, lay_smem<LP, double>(), s>>>(kc, xp, yp, h->dc, h->c, h->l, h->u);
+        NIR_LAUNCHED();
+    });
+    h->launches += 2;
+}
+
+// Occupancy queries of the KKT kernels before any capture.
+template <typename TX>
+void warm_kkt(nir_pdhg* h) {
+    with_lays(h, [&](auto lp, auto ld) {
+        constexpr int LP = decltype(lp)::value, LD = decltype(ld)::value;
+        lay_grid<LD, double>(h, nir::k_kkt_rows<LD, TX>, lay_nblk(h->A));
+        lay_grid<LP, double>(h, nir::k_kkt_cols<LP, TX>, lay_nblk(h->At));
+    });
 }
 
 struct SolveCfg {
@@ -765,26 +793,31 @@ struct ChunkTimer {
 
 // One launch chunk: K iterations (the last one a check), the KKT passes,
 // the controller, the restart copy and the status snapshot.  TV = type of
-// the matrix values, TX = type of the iterates, E = run length.
-template <typename TV, typename TX, int E>
-void launch_fast_chunk_e(nir_pdhg* h, const SolveCfg& cfg, int phase, ChunkTimer* tm) {
+// the matrix values, TX = type of the iterates, LP / LD = layouts of A' / A.
+template <typename TV, typename TX, int LP, int LD>
+void launch_fast_chunk_l(nir_pdhg* h, const SolveCfg& cfg, int phase, ChunkTimer* tm) {
     if (tm) tm->prec = (sizeof(TV) == 8) ? 1 : 0;
     cudaStream_t s = h->stream;
     const PartLayout L = part_layout(h);
     const int K = cfg.K;
-    const Orient::Cta& LA = h->A.cur();
-    const Orient::Cta& LT = h->At.cur();
-    const int gp1 = cta_grid(h, nir::k_primal<TV, TX, E, true>, LT.nblk);
-    const int gp0 = cta_grid(h, nir::k_primal<TV, TX, E, false>, LT.nblk);
-    const int gd1 = cta_grid(h, nir::k_dual<TV, TX, E, true>, LA.nblk);
-    const int gd0 = cta_grid(h, nir::k_dual<TV, TX, E, false>, LA.nblk);
+    const int nbt = lay_nblk(h->At), nba = lay_nblk(h->A);
+    const nir::Lay lt = lay_of(h->At), la = lay_of(h->A);
+    const TV* valAt = vals_of<TV>(h->At);
+    const TV* valA = vals_of<TV>(h->A);
+    const size_t sp = lay_smem<LP, TX>(), sd = lay_smem<LD, TX>();
+    const int gp1 = lay_grid<LP, TX>(h, nir::k_primal<LP, TV, TX, true>, nbt);
+    const int gp0 = lay_grid<LP, TX>(h, nir::k_primal<LP, TV, TX, false>, nbt);
+    const int gd1 = lay_grid<LD, TX>(h, nir::k_dual<LD, TV, TX, true>, nba);
+    const int gd0 = lay_grid<LD, TX>(h, nir::k_dual<LD, TV, TX, false>, nba);
     int i_first = 0;
     if (cfg.persistent && K > 1) {
         // iterations 0..K-2 in one cooperative launch; the check pair below
-        const int gc = cta_grid(h, nir::k_chunk<TV, TX, E>, std::max(LA.nblk, LT.nblk));
-        nir::IterArgs ap{LT.blk, LT.nblk, h->At.rp, LT.ci, L.P, h->st, 0, cfg.halpern, phase, cfg.p.reflection};
-        nir::IterArgs ad{LA.blk, LA.nblk, h->A.rp, LA.ci, L.D, h->st, 0, cfg.halpern, phase, cfg.p.reflection};
-        nir::ChunkPtrs<TV, TX> v{vals<TV>(LT),   vals<TV>(LA),   Vec<TX>::x(h),  Vec<TX>::xb(h), Vec<TX>::xp(h),
+        const size_t sc = std::max(sp, sd);
+        const int gc = std::min(lay_grid<LP, TX>(h, nir::k_chunk<LP, LD, TV, TX>, nbt),
+                                lay_grid<LD, TX>(h, nir::k_chunk<LP, LD, TV, TX>, nba));
+        nir::IterArgs ap{lt, L.P, h->st, 0, cfg.halpern, phase, cfg.p.reflection};
+        nir::IterArgs ad{la, L.D, h->st, 0, cfg.halpern, phase, cfg.p.reflection};
+        nir::ChunkPtrs<TV, TX> v{valAt,          valA,           Vec<TX>::x(h),  Vec<TX>::xb(h), Vec<TX>::xp(h),
                                  Vec<TX>::y(h),  Vec<TX>::yp(h), Vec<TX>::c(h),  Vec<TX>::l(h),  Vec<TX>::u(h),
                                  Vec<TX>::x0(h), Vec<TX>::rl(h), Vec<TX>::ru(h), Vec<TX>::y0(h)};
         // ~1 s of SM clock per wait; 0.1 s and one CTA too many in the test
@@ -793,41 +826,41 @@ void launch_fast_chunk_e(nir_pdhg* h, const SolveCfg& cfg, int phase, ChunkTimer
         nir::DevState* st = h->st;
         int i0 = 0, iters = K - 1;
         void* args[] = {&ap, &ad, &v, &i0, &iters, &gs, &st};
-        NIR_CUDA(cudaLaunchCooperativeKernel((const void*)nir::k_chunk<TV, TX, E>, dim3(gc), dim3(nir::kBlock), args,
-                                             0, s));
+        NIR_CUDA(cudaLaunchCooperativeKernel((const void*)nir::k_chunk<LP, LD, TV, TX>, dim3(gc), dim3(nir::kBlock),
+                                             args, sc, s));
         h->launches += 1;
         i_first = K - 1;
     }
     for (int i = i_first; i < K; ++i) {
         const bool check = (i == K - 1);
-        nir::IterArgs ap{LT.blk, LT.nblk, h->At.rp, LT.ci, L.P, h->st, i, cfg.halpern, phase, cfg.p.reflection};
-        nir::IterArgs ad{LA.blk, LA.nblk, h->A.rp, LA.ci, L.D, h->st, i, cfg.halpern, phase, cfg.p.reflection};
+        nir::IterArgs ap{lt, L.P, h->st, i, cfg.halpern, phase, cfg.p.reflection};
+        nir::IterArgs ad{la, L.D, h->st, i, cfg.halpern, phase, cfg.p.reflection};
         const bool timed = tm && tm->armed && i == 0 && !cfg.persistent;
         if (timed) NIR_CUDA(cudaEventRecord(tm->e[0], s));
         if (check)
-            nir::k_primal<TV, TX, E, true><<<gp1, nir::kBlock, 0, s>>>(
-                ap, vals<TV>(LT), Vec<TX>::y(h), Vec<TX>::x(h), Vec<TX>::xb(h), Vec<TX>::xp(h), Vec<TX>::c(h),
-                Vec<TX>::l(h), Vec<TX>::u(h), Vec<TX>::x0(h));
+            nir::k_primal<LP, TV, TX, true><<<gp1, nir::kBlock, sp, s>>>(
+                ap, valAt, Vec<TX>::y(h), Vec<TX>::x(h), Vec<TX>::xb(h), Vec<TX>::xp(h), Vec<TX>::c(h), Vec<TX>::l(h),
+                Vec<TX>::u(h), Vec<TX>::x0(h));
         else
-            nir::k_primal<TV, TX, E, false><<<gp0, nir::kBlock, 0, s>>>(
-                ap, vals<TV>(LT), Vec<TX>::y(h), Vec<TX>::x(h), Vec<TX>::xb(h), Vec<TX>::xp(h), Vec<TX>::c(h),
-                Vec<TX>::l(h), Vec<TX>::u(h), Vec<TX>::x0(h));
+            nir::k_primal<LP, TV, TX, false><<<gp0, nir::kBlock, sp, s>>>(
+                ap, valAt, Vec<TX>::y(h), Vec<TX>::x(h), Vec<TX>::xb(h), Vec<TX>::xp(h), Vec<TX>::c(h), Vec<TX>::l(h),
+                Vec<TX>::u(h), Vec<TX>::x0(h));
         NIR_LAUNCHED();
         if (timed) NIR_CUDA(cudaEventRecord(tm->e[1], s));
         if (check)
-            nir::k_dual<TV, TX, E, true><<<gd1, nir::kBlock, 0, s>>>(ad, vals<TV>(LA), Vec<TX>::xb(h), Vec<TX>::y(h),
-                                                                     Vec<TX>::yp(h), Vec<TX>::rl(h), Vec<TX>::ru(h),
-                                                                     Vec<TX>::y0(h));
+            nir::k_dual<LD, TV, TX, true><<<gd1, nir::kBlock, sd, s>>>(ad, valA, Vec<TX>::xb(h), Vec<TX>::y(h),
+                                                                       Vec<TX>::yp(h), Vec<TX>::rl(h), Vec<TX>::ru(h),
+                                                                       Vec<TX>::y0(h));
         else
-            nir::k_dual<TV, TX, E, false><<<gd0, nir::kBlock, 0, s>>>(ad, vals<TV>(LA), Vec<TX>::xb(h), Vec<TX>::y(h),
-                                                                      Vec<TX>::yp(h), Vec<TX>::rl(h), Vec<TX>::ru(h),
-                                                                      Vec<TX>::y0(h));
+            nir::k_dual<LD, TV, TX, false><<<gd0, nir::kBlock, sd, s>>>(ad, valA, Vec<TX>::xb(h), Vec<TX>::y(h),
+                                                                        Vec<TX>::yp(h), Vec<TX>::rl(h), Vec<TX>::ru(h),
+                                                                        Vec<TX>::y0(h));
         NIR_LAUNCHED();
         if (timed) NIR_CUDA(cudaEventRecord(tm->e[2], s));
         h->launches += 2;
     }
     int gkr = 0, gkc = 0;
-    launch_kkt_e<TX, E>(h, phase, L.KR, L.KC, Vec<TX>::xp(h), Vec<TX>::yp(h), &gkr, &gkc);
+    launch_kkt<TX>(h, phase, L.KR, L.KC, Vec<TX>::xp(h), Vec<TX>::yp(h), &gkr, &gkc);
     h->launches -= 2;  // counted with the chunk below
     nir::CtlArgs ca;
     ca.partP = L.P;
@@ -871,23 +904,25 @@ void launch_fast_chunk_e(nir_pdhg* h, const SolveCfg& cfg, int phase, ChunkTimer
 
 template <typename TV, typename TX>
 void launch_fast_chunk(nir_pdhg* h, const SolveCfg& cfg, int phase, ChunkTimer* tm) {
-    with_run_len(h->A.cur().cap, [&](auto e) { launch_fast_chunk_e<TV, TX, decltype(e)::value>(h, cfg, phase, tm); });
+    with_lays(h, [&](auto lp, auto ld) {
+        launch_fast_chunk_l<TV, TX, decltype(lp)::value, decltype(ld)::value>(h, cfg, phase, tm);
+    });
 }
 
 // Runs the occupancy queries of a chunk's kernels before any capture.
 template <typename TV, typename TX>
 void warm_cfgs(nir_pdhg* h) {
-    with_run_len(h->A.cur().cap, [&](auto e) {
-        constexpr int E = decltype(e)::value;
-        const int na = h->A.cur().nblk, nt = h->At.cur().nblk;
-        cta_grid(h, nir::k_primal<TV, TX, E, true>, nt);
-        cta_grid(h, nir::k_primal<TV, TX, E, false>, nt);
-        cta_grid(h, nir::k_dual<TV, TX, E, true>, na);
-        cta_grid(h, nir::k_dual<TV, TX, E, false>, na);
-        cta_grid(h, nir::k_kkt_rows<TX, E>, na);
-        cta_grid(h, nir::k_kkt_cols<TX, E>, nt);
-        cta_grid(h, nir::k_chunk<TV, TX, E>, std::max(na, nt));
+    with_lays(h, [&](auto lp, auto ld) {
+        constexpr int LP = decltype(lp)::value, LD = decltype(ld)::value;
+        const int nbt = lay_nblk(h->At), nba = lay_nblk(h->A);
+        lay_grid<LP, TX>(h, nir::k_primal<LP, TV, TX, true>, nbt);
+        lay_grid<LP, TX>(h, nir::k_primal<LP, TV, TX, false>, nbt);
+        lay_grid<LD, TX>(h, nir::k_dual<LD, TV, TX, true>, nba);
+        lay_grid<LD, TX>(h, nir::k_dual<LD, TV, TX, false>, nba);
+        lay_grid<LP, TX>(h, nir::k_chunk<LP, LD, TV, TX>, nbt);
+        lay_grid<LD, TX>(h, nir::k_chunk<LP, LD, TV, TX>, nba);
     });
+    warm_kkt<TX>(h);
 }
 
 // Identity of everything a captured chunk bakes into its kernel arguments
@@ -912,7 +947,10 @@ unsigned long long chunk_key(const nir_pdhg* h, const SolveCfg& c, int phase, in
     k.add(phase).add(prec).add(c.K).add(c.halpern).add(c.restarts).add(c.mixed).add(c.bnorm).add(c.cnorm);
     k.add(c.p.reflection).add(c.p.restart_sufficient).add(c.p.restart_necessary).add(c.p.restart_artificial);
     k.add(c.p.primal_weight_smoothing).add(c.p.polish_stall_checks).add(c.p.polish_switch_kkt).add(c.p.tol);
-    k.add(c.p.feas_tol).add(c.p.restart_anchor).add(c.p.primal_weight_decades).add(c.p.polish_fresh).add(h->offset).add(h->A.cur().cap).add(h->A.cur().blk).add(h->At.cur().blk).add(h->part).add(h->hist);
+    k.add(c.p.feas_tol).add(c.p.restart_anchor).add(c.p.primal_weight_decades).add(c.p.polish_fresh).add(h->offset).add(h->part).add(h->hist);
+    // the layouts of a single LP (the batch keys its own)
+    if (h->A.lay >= 0) k.add(h->A.lay).add(lay_of(h->A).blk).add(lay_of(h->A).cap);
+    if (h->At.lay >= 0) k.add(h->At.lay).add(lay_of(h->At).blk).add(lay_of(h->At).cap);
     k.add(c.persistent).add(c.barrier_test);
     return k.h;
 }
@@ -1058,6 +1096,8 @@ LoopResult run_chunks(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*),
     return R;
 }
 
+LayChoice default_layouts(const nir_pdhg* h);
+
 double host_objective(const nir_pdhg* h, const std::vector<double>& x) {
     DD s;
     s.hi = h->offset;
@@ -1097,14 +1137,10 @@ int solve_reference(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), v
     const bool probing = p.tol > 0.0;
     RefProbe probe{0.0, 0.0, p.tol};
     if (probing) {
-        use_cta(h, auto_cta_cap(h));
+        use_layouts(h, default_layouts(h));
         precondition(h, p, false);
         pad_scaled(h);
-        with_run_len(h->A.cur().cap, [&](auto e) {
-            constexpr int E = decltype(e)::value;
-            cta_grid(h, nir::k_kkt_rows<double, E>, h->A.cur().nblk);
-            cta_grid(h, nir::k_kkt_cols<double, E>, h->At.cur().nblk);
-        });
+        warm_kkt<double>(h);
         probe.bnorm = rhs_norm(h);
         probe.cnorm = norm2(h->h_c);
     }
@@ -1132,7 +1168,7 @@ int solve_reference(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), v
         if (p.use_graphs) {
             KeyHash key;
             key.add(1000).add(probing).add(probe.bnorm).add(probe.cnorm).add(probe.tol).add(h->offset);
-            if (probing) key.add(h->A.cur().blk).add(h->At.cur().blk).add(h->A.cur().cap);
+            if (probing) key.add(lay_of(h->A).blk).add(lay_of(h->At).blk).add(h->A.lay).add(h->At.lay);
             key.add(h->part);
             cudaGraphExec_t ge = chunk_graph(h, 0, key.h, launch);
             const int per = launches_per_chunk(K, true) + (probing ? 3 : 0);
@@ -1253,73 +1289,97 @@ double rhs_norm(const nir_pdhg* h) {
     return std::sqrt(s.hi + s.lo);
 }
 
-// The autotuner: picks the CTA-block capacity 256 E (E = 1, 2, 4, 8
-// nonzeros per thread) for this matrix by timing the plain CTA SpMV of
-// each candidate layout in the value and iterate precision the solve
-// starts in, both orientations, on scratch vectors.  The choice is cached
+// Layouts without timing: warp row blocks, the capacity by size.
+LayChoice default_layouts(const nir_pdhg* h) {
+    LayChoice c;
+    c.cap_a = c.cap_at = auto_cap(h->nnz, std::max(h->m, h->n));
+    return c;
+}
+
+// The autotuner: picks, for each orientation separately, the layout of its
+// SpMV (warp row blocks of 32, 64, 128 or 256 nonzeros, or CTA blocks of
+// 1024) by timing the plain SpMV of each candidate in the value and iterate
+// precision the solve starts in, on scratch vectors.  The choice is cached
 // per handle and precision.
 template <typename TV, typename TX>
-double time_layout(nir_pdhg* h, int cap) {
-    Orient::Cta& LA = cta_layout(h, h->A, cap);
-    Orient::Cta& LT = cta_layout(h, h->At, cap);
+float time_candidate(nir_pdhg* h, Orient& o, int lay, int cap) {
     cudaStream_t s = h->stream;
-    TX* in_n = reinterpret_cast<TX*>(std::is_same<TX, float>::value ? (void*)h->tmp_n32 : (void*)h->tmp_n);
-    TX* in_m = reinterpret_cast<TX*>(std::is_same<TX, float>::value ? (void*)h->tmp_m32 : (void*)h->tmp_m);
-    TX* out_n = reinterpret_cast<TX*>(h->out_x);
-    TX* out_m = reinterpret_cast<TX*>(h->out_y);
+    const bool tr = &o == &h->At;
+    const TX* in = reinterpret_cast<const TX*>(std::is_same<TX, float>::value ? (tr ? (void*)h->tmp_m32 : (void*)h->tmp_n32)
+                                                                              : (tr ? (void*)h->tmp_m : (void*)h->tmp_n));
+    TX* out = reinterpret_cast<TX*>(tr ? h->out_x : h->out_y);
+    cudaEvent_t a, b;
+    NIR_CUDA(cudaEventCreate(&a));
+    NIR_CUDA(cudaEventCreate(&b));
     float best = 1e30f;
-    with_run_len(cap, [&](auto e) {
-        constexpr int E = decltype(e)::value;
-        auto* kern = nir::k_spmv_cta<TX, TV, TX, E>;
-        const int ga = cta_grid(h, kern, LA.nblk), gt = cta_grid(h, kern, LT.nblk);
-        cudaEvent_t a, b;
-        NIR_CUDA(cudaEventCreate(&a));
-        NIR_CUDA(cudaEventCreate(&b));
-        for (int rep = 0; rep < 4; ++rep) {
-            NIR_CUDA(cudaEventRecord(a, s));
-            kern<<<ga, nir::kBlock, 0, s>>>(LA.blk, LA.nblk, h->A.rp, LA.ci, vals<TV>(LA), in_n, out_m);
-            kern<<<gt, nir::kBlock, 0, s>>>(LT.blk, LT.nblk, h->At.rp, LT.ci, vals<TV>(LT), in_m, out_n);
-            NIR_LAUNCHED();
-            NIR_CUDA(cudaEventRecord(b, s));
-            NIR_CUDA(cudaEventSynchronize(b));
-            float ms = 0.0f;
-            NIR_CUDA(cudaEventElapsedTime(&ms, a, b));
-            if (rep > 0) best = std::min(best, ms);  // the first launch warms up
+    for (int rep = 0; rep < 4; ++rep) {
+        NIR_CUDA(cudaEventRecord(a, s));
+        if (lay == nir::kLayWarp) {
+            set_blocks(h, o, cap);
+            auto* kern = nir::k_spmv_adaptive<TX, TV, TX>;
+            const int g = lay_grid<nir::kLayWarp, TX>(h, kern, o.nblk);
+            const TV* v = std::is_same<TV, float>::value ? (const TV*)o.v32 : (const TV*)o.v64;
+            kern<<<g, nir::kBlock, lay_smem<nir::kLayWarp, TX>(), s>>>(o.blk, o.nblk, cap, o.rp, o.ci, v, in, out);
+        } else {
+            Orient::Cta& L = cta_layout(h, o, kCtaCap);
+            auto* kern = nir::k_spmv_cta<TX, TV, TX, nir::kLayCta>;
+            const int g = lay_grid<nir::kLayCta, TX>(h, kern, L.nblk);
+            const TV* v = std::is_same<TV, float>::value ? (const TV*)L.v32 : (const TV*)L.v64;
+            kern<<<g, nir::kBlock, 0, s>>>(L.blk, L.nblk, o.rp, L.ci, v, in, out);
         }
-        cudaEventDestroy(a);
-        cudaEventDestroy(b);
-    });
+        NIR_LAUNCHED();
+        NIR_CUDA(cudaEventRecord(b, s));
+        NIR_CUDA(cudaEventSynchronize(b));
+        float ms = 0.0f;
+        NIR_CUDA(cudaEventElapsedTime(&ms, a, b));
+        if (rep > 0) best = std::min(best, ms);  // the first launch warms up
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
     return best;
 }
 
-// The tuned capacity depends only on the sparsity structure, the precision
-// and the device, and the capacity fixes the per-row summation order: one
+// The tuned layouts depend only on the sparsity structure, the precision
+// and the device, and they fix the per-row summation order: one
 // process-wide table keyed by those makes every handle on the same matrix
-// use the same layout (bit-identical results across handles).
+// use the same layouts (bit-identical results across handles).
 std::mutex g_tune_mu;
-std::vector<std::pair<unsigned long long, int>> g_tuned;
+std::vector<std::pair<unsigned long long, LayChoice>> g_tuned;
 
 unsigned long long structure_key(const nir_pdhg* h, int prec) {
     KeyHash k;
-    k.add(h->device).add(h->m).add(h->n).add(h->nnz).add(prec).add(2);  // 2: CTA-block layouts
+    k.add(h->device).add(h->m).add(h->n).add(h->nnz).add(prec).add(3);  // 3: warp or CTA per orientation
     for (int v : h->A.h_rp) k.add(v);
     for (int v : h->At.h_rp) k.add(v);
     return k.h;
 }
 
-int pick_cap(nir_pdhg* h, const nir_pdhg_params& p) {
+LayChoice pick_layouts(nir_pdhg* h, const nir_pdhg_params& p) {
     if (p.spmv_block_nnz > 0) {
-        run_len(p.spmv_block_nnz);  // throws on a capacity the kernels do not have
-        return p.spmv_block_nnz;
+        LayChoice c;
+        if (p.spmv_block_nnz == kCtaCap) {
+            c.lay_a = c.lay_at = nir::kLayCta;
+            c.cap_a = c.cap_at = kCtaCap;
+        } else if (p.spmv_block_nnz == 32 || p.spmv_block_nnz == 64 || p.spmv_block_nnz == 128 ||
+                   p.spmv_block_nnz == 256) {
+            c.cap_a = c.cap_at = p.spmv_block_nnz;
+        } else {
+            throw std::invalid_argument("spmv_block_nnz must be 0, 32, 64, 128, 256 (warp row blocks) or 1024 "
+                                        "(CTA blocks)");
+        }
+        return c;
     }
-    const int prec = p.precision;  // NIR_PREC_*: FP64 starts with FP64 values, MIXED and FP32 with FP32 values
-    int& cached = h->tuned_cap[prec];
-    if (cached > 0) return cached;
+    const int prec = p.precision;  // FP64 starts with FP64 values, MIXED and FP32 with FP32 values
+    if (h->tuned_ok[prec]) return h->tuned[prec];
     const unsigned long long key = structure_key(h, prec);
     {
         std::lock_guard<std::mutex> g(g_tune_mu);
         for (auto& e : g_tuned)
-            if (e.first == key) return cached = e.second;
+            if (e.first == key) {
+                h->tuned[prec] = e.second;
+                h->tuned_ok[prec] = true;
+                return e.second;
+            }
     }
     // the scratch inputs only need to hold finite values
     nir::k_fill<<<grid_for(h->n), nir::kBlock, 0, h->stream>>>(h->n, 0.5, h->tmp_n);
@@ -1327,22 +1387,37 @@ int pick_cap(nir_pdhg* h, const nir_pdhg_params& p) {
     nir::k_to_float<<<grid_for(h->n), nir::kBlock, 0, h->stream>>>(h->n, h->tmp_n, h->tmp_n32);
     nir::k_to_float<<<grid_for(h->m), nir::kBlock, 0, h->stream>>>(h->m, h->tmp_m, h->tmp_m32);
     NIR_LAUNCHED();
-    double best = 1e300;
-    int arg = auto_cta_cap(h);
-    for (int cap : {256, 512, 1024, 2048}) {
-        double t;
-        if (prec == NIR_PREC_FP64) t = time_layout<double, double>(h, cap);
-        else if (prec == NIR_PREC_MIXED) t = time_layout<float, double>(h, cap);
-        else t = time_layout<float, float>(h, cap);
-        if (t <= best * 1.02) {  // near-ties go to the larger capacity
-            arg = cap;
-            best = std::min(best, t);
+    LayChoice c;
+    for (int t = 0; t < 2; ++t) {
+        Orient& o = t ? h->At : h->A;
+        float best = 1e30f;
+        int lay = nir::kLayWarp, cap = auto_cap(h->nnz, o.rows);
+        auto consider = [&](int l, int k) {
+            float ms;
+            if (prec == NIR_PREC_FP64) ms = time_candidate<double, double>(h, o, l, k);
+            else if (prec == NIR_PREC_MIXED) ms = time_candidate<float, double>(h, o, l, k);
+            else ms = time_candidate<float, float>(h, o, l, k);
+            if (ms <= best * 1.02f) {  // near-ties go to the later candidate (larger blocks)
+                best = std::min(best, ms);
+                lay = l;
+                cap = k;
+            }
+        };
+        for (int k : {32, 64, 128, 256}) consider(nir::kLayWarp, k);
+        consider(nir::kLayCta, kCtaCap);
+        if (t) {
+            c.lay_at = lay;
+            c.cap_at = cap;
+        } else {
+            c.lay_a = lay;
+            c.cap_a = cap;
         }
     }
-    cached = arg;
+    h->tuned[prec] = c;
+    h->tuned_ok[prec] = true;
     std::lock_guard<std::mutex> g(g_tune_mu);
-    g_tuned.emplace_back(key, arg);
-    return arg;
+    g_tuned.emplace_back(key, c);
+    return c;
 }
 
 int solve_fast(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), void* ctx, double* x_out, double* y_out,
@@ -1351,8 +1426,7 @@ int solve_fast(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), void* 
     const double t0 = now_sec();
     const int n = h->n, m = h->m;
     const bool pdlp = p.algorithm == NIR_ALGO_PDLP;
-    const int cap = pick_cap(h, p);
-    use_cta(h, cap);
+    use_layouts(h, pick_layouts(h, p));
     ensure_partials(h);
     // value / iterate precision of each phase: FP64 (double, double); MIXED
     // (float, double) then the FP64 polish; FP32 (float, float)
@@ -1848,15 +1922,23 @@ namespace {
 
 // Launches k_spmv_cta for the run length of the layout with a persistent
 // grid of the resident CTAs.
+template <typename TA, typename TV, typename TX, int E>
+void launch_spmv_cta_e(nir_pdhg* h, const Orient::Cta& c, const int* rp, const TV* val, const TX* x, TA* y) {
+    auto* kern = nir::k_spmv_cta<TA, TV, TX, E>;
+    const int grid = lay_grid<E, TA>(h, kern, c.nblk);
+    kern<<<grid, nir::kBlock, 0, h->stream>>>(c.blk, c.nblk, rp, c.ci, val, x, y);
+    NIR_LAUNCHED();
+}
+
 template <typename TA, typename TV, typename TX>
 void launch_spmv_cta(nir_pdhg* h, const Orient::Cta& c, const int* rp, const TV* val, const TX* x, TA* y) {
-    with_run_len(c.cap, [&](auto e) {
-        constexpr int E = decltype(e)::value;
-        auto* kern = nir::k_spmv_cta<TA, TV, TX, E>;
-        const int grid = cta_grid(h, kern, c.nblk);
-        kern<<<grid, nir::kBlock, 0, h->stream>>>(c.blk, c.nblk, rp, c.ci, val, x, y);
-        NIR_LAUNCHED();
-    });
+    switch (c.cap) {
+        case 256: launch_spmv_cta_e<TA, TV, TX, 1>(h, c, rp, val, x, y); break;
+        case 512: launch_spmv_cta_e<TA, TV, TX, 2>(h, c, rp, val, x, y); break;
+        case 1024: launch_spmv_cta_e<TA, TV, TX, 4>(h, c, rp, val, x, y); break;
+        case 2048: launch_spmv_cta_e<TA, TV, TX, 8>(h, c, rp, val, x, y); break;
+        default: throw std::invalid_argument("CTA block capacity must be 256, 512, 1024 or 2048");
+    }
 }
 
 // One launch of a measured SpMV kind (nir_pdhg_time_kernel) on the
@@ -2048,31 +2130,32 @@ namespace {
 // a copy of the solver state marked running, on the layout and scaled
 // values of the last solve; they overwrite the iterates, which a finished
 // solve no longer needs (its result is in out_x / out_y).
-template <typename TV, typename TX, int E>
-void time_iteration_e(nir_pdhg* h, int reps, double* primal_us, double* dual_us, double* pair_us) {
+template <typename TV, typename TX, int LP, int LD>
+void time_iteration_l(nir_pdhg* h, int reps, double* primal_us, double* dual_us, double* pair_us) {
     cudaStream_t s = h->stream;
     const PartLayout L = part_layout(h);
-    const Orient::Cta& LA = h->A.cur();
-    const Orient::Cta& LT = h->At.cur();
     if (!h->st_time) h->st_time = h->alloc<nir::DevState>(1);
     nir::DevState st;
     d2h(h, &st, h->st, sizeof(st));
     st.done = 0;
     st.phase = 0;
     h2d(h, h->st_time, &st, sizeof(st));
-    const int gp = cta_grid(h, nir::k_primal<TV, TX, E, false>, LT.nblk);
-    const int gd = cta_grid(h, nir::k_dual<TV, TX, E, false>, LA.nblk);
-    nir::IterArgs ap{LT.blk, LT.nblk, h->At.rp, LT.ci, L.P, h->st_time, 1, 1, 0, 1.0};
-    nir::IterArgs ad{LA.blk, LA.nblk, h->A.rp, LA.ci, L.D, h->st_time, 1, 1, 0, 1.0};
+    const int gp = lay_grid<LP, TX>(h, nir::k_primal<LP, TV, TX, false>, lay_nblk(h->At));
+    const int gd = lay_grid<LD, TX>(h, nir::k_dual<LD, TV, TX, false>, lay_nblk(h->A));
+    const size_t sp = lay_smem<LP, TX>(), sd = lay_smem<LD, TX>();
+    nir::IterArgs ap{lay_of(h->At), L.P, h->st_time, 1, 1, 0, 1.0};
+    nir::IterArgs ad{lay_of(h->A), L.D, h->st_time, 1, 1, 0, 1.0};
+    const TV* valAt = vals_of<TV>(h->At);
+    const TV* valA = vals_of<TV>(h->A);
     auto primal = [&]() {
-        nir::k_primal<TV, TX, E, false><<<gp, nir::kBlock, 0, s>>>(
-            ap, vals<TV>(LT), Vec<TX>::y(h), Vec<TX>::x(h), Vec<TX>::xb(h), Vec<TX>::xp(h), Vec<TX>::c(h),
-            Vec<TX>::l(h), Vec<TX>::u(h), Vec<TX>::x0(h));
+        nir::k_primal<LP, TV, TX, false><<<gp, nir::kBlock, sp, s>>>(
+            ap, valAt, Vec<TX>::y(h), Vec<TX>::x(h), Vec<TX>::xb(h), Vec<TX>::xp(h), Vec<TX>::c(h), Vec<TX>::l(h),
+            Vec<TX>::u(h), Vec<TX>::x0(h));
     };
     auto dual = [&]() {
-        nir::k_dual<TV, TX, E, false><<<gd, nir::kBlock, 0, s>>>(ad, vals<TV>(LA), Vec<TX>::xb(h), Vec<TX>::y(h),
-                                                                 Vec<TX>::yp(h), Vec<TX>::rl(h), Vec<TX>::ru(h),
-                                                                 Vec<TX>::y0(h));
+        nir::k_dual<LD, TV, TX, false><<<gd, nir::kBlock, sd, s>>>(ad, valA, Vec<TX>::xb(h), Vec<TX>::y(h),
+                                                                   Vec<TX>::yp(h), Vec<TX>::rl(h), Vec<TX>::ru(h),
+                                                                   Vec<TX>::y0(h));
     };
     cudaEvent_t a, b;
     NIR_CUDA(cudaEventCreate(&a));
@@ -2113,13 +2196,14 @@ int nir_pdhg_time_iteration(nir_pdhg* h, int precision, int reps, double* primal
     if (h->inner) h = h->inner.get();  // PDHG / PDLP solves ran on the equivalent LP
     try {
         NIR_CUDA(cudaSetDevice(h->device));
-        if (h->A.it < 0) throw std::invalid_argument("no PDHG / PDLP solve has set up the iteration kernels yet");
+        if (h->A.lay < 0 || h->At.lay < 0)
+            throw std::invalid_argument("no PDHG / PDLP solve has set up the iteration kernels yet");
         if (h->last_x == h->x64) h->last_x = nullptr;  // a reference-loop result the kernels would overwrite
-        with_run_len(h->A.cur().cap, [&](auto e) {
-            constexpr int E = decltype(e)::value;
-            if (precision == NIR_PREC_FP64) time_iteration_e<double, double, E>(h, reps, primal_us, dual_us, pair_us);
-            else if (precision == NIR_PREC_MIXED) time_iteration_e<float, double, E>(h, reps, primal_us, dual_us, pair_us);
-            else time_iteration_e<float, float, E>(h, reps, primal_us, dual_us, pair_us);
+        with_lays(h, [&](auto lp, auto ld) {
+            constexpr int LP = decltype(lp)::value, LD = decltype(ld)::value;
+            if (precision == NIR_PREC_FP64) time_iteration_l<double, double, LP, LD>(h, reps, primal_us, dual_us, pair_us);
+            else if (precision == NIR_PREC_MIXED) time_iteration_l<float, double, LP, LD>(h, reps, primal_us, dual_us, pair_us);
+            else time_iteration_l<float, float, LP, LD>(h, reps, primal_us, dual_us, pair_us);
         });
         return 0;
     } catch (const std::invalid_argument& e) {
@@ -2162,10 +2246,10 @@ int nir_pdhg_get_layout(nir_pdhg* h, nir_pdhg_layout* out) {
     out->ncol = h->n;
     out->nnz = h->nnz;
     const nir_pdhg* src = h->inner ? h->inner.get() : h;  // PDHG / PDLP solves ran on the equivalent LP
-    const bool cta = src->A.it >= 0;
-    out->blocks_a = cta ? src->A.cur().nblk : h->A.nblk;
-    out->blocks_at = cta ? src->At.cur().nblk : h->At.nblk;
-    out->block_nnz = cta ? src->A.cur().cap : h->A.cap;
+    out->blocks_a = src->A.lay >= 0 ? lay_nblk(src->A) : 0;
+    out->blocks_at = src->At.lay >= 0 ? lay_nblk(src->At) : 0;
+    out->block_nnz = src->A.lay == nir::kLayCta ? kCtaCap : src->A.cap;
+    out->block_nnz_at = src->At.lay == nir::kLayCta ? kCtaCap : src->At.cap;
     out->device_bytes = h->device_bytes;
     return 0;
 }

@@ -13,19 +13,23 @@ struct nir_pdhg_batch {
     int* d_col_off = nullptr;
     int* d_row_inst = nullptr;
     int* d_col_inst = nullptr;
-    // CTA blocks per instance (no block crosses an instance) with their
-    // padded streams, one layout per capacity used, built once each
+    // the blocks of each orientation, instance by instance (no block crosses
+    // an instance), in the layout the autotuner picked for it, one set per
+    // layout choice used, built once each
     struct Orient2 {
-        int4* blk = nullptr;  // .w = instance
+        int lay = nir::kLayWarp;
+        int cap = 256;          // warp row-block capacity
+        void* blk = nullptr;    // int2 (warp) or int4 with the instance in .w (CTA)
         int nblk = 0;
-        int* lo = nullptr;    // first block of each instance (count + 1)
-        int* ci = nullptr;    // padded column indices
-        double* v64 = nullptr;
+        int* inst = nullptr;    // warp layout: instance of each block
+        int* lo = nullptr;      // first block of each instance (count + 1)
+        int* ci = nullptr;      // CTA layout: padded column indices (warp: the CSR's)
+        double* v64 = nullptr;  // CTA layout: padded scaled values (warp: the CSR's)
         float* v32 = nullptr;
     };
     struct Layout {
-        int cap = 0;
-        Orient2 a, at;        // A (rows) and A' (columns)
+        LayChoice choice;
+        Orient2 a, at;          // A (rows) and A' (columns)
         double* part = nullptr;
     };
     std::deque<Layout> layouts;
@@ -46,42 +50,62 @@ struct nir_pdhg_batch {
 
 namespace {
 
-// CTA blocks of one orientation, built instance by instance so that no
-// block crosses an instance, and the padded stream of its column indices
-// (values are padded after each preconditioning, batch_pad_values).
-void batch_blocks(nir_pdhg_batch* B, const Orient& o, const std::vector<int>& off, int cap,
+// The blocks of one orientation in layout `lay`, built instance by
+// instance so that no block crosses an instance; the CTA layout also gets
+// the padded stream of its column indices (values are padded after each
+// preconditioning, batch_pad_values).
+void batch_blocks(nir_pdhg_batch* B, Orient& o, const std::vector<int>& off, int lay, int cap,
                   nir_pdhg_batch::Orient2* out) {
     nir_pdhg* h = B->h;
     std::vector<int> lo;
-    const std::vector<int4> all = nir::build_batch_cta_blocks(o.h_rp, off, cap, &lo);
-    out->nblk = int(all.size()) - 1;
-    out->blk = h->alloc<int4>(all.size());
-    h2d(h, out->blk, all.data(), all.size() * sizeof(int4));
+    out->lay = lay;
+    out->cap = cap;
+    if (lay == nir::kLayWarp) {
+        std::vector<int> owner;
+        const std::vector<int2> all = nir::build_batch_row_blocks(o.h_rp, off, cap, &owner, &lo);
+        out->nblk = int(owner.size());
+        int2* blk = h->alloc<int2>(all.size());
+        h2d(h, blk, all.data(), all.size() * sizeof(int2));
+        out->blk = blk;
+        out->inst = h->alloc<int>(std::max<size_t>(owner.size(), 1));
+        if (!owner.empty()) h2d(h, out->inst, owner.data(), owner.size() * sizeof(int));
+        out->ci = o.ci;
+        out->v64 = o.v64;
+        out->v32 = o.v32;
+    } else {
+        const std::vector<int4> all = nir::build_batch_cta_blocks(o.h_rp, off, cap, &lo);
+        out->nblk = int(all.size()) - 1;
+        int4* blk = h->alloc<int4>(all.size());
+        h2d(h, blk, all.data(), all.size() * sizeof(int4));
+        out->blk = blk;
+        const size_t q = size_t(all.back().z);
+        out->ci = h->allocz<int>(q, 8);
+        out->v64 = h->allocz<double>(q, 8);
+        out->v32 = h->allocz<float>(q, 8);
+        if (out->nblk > 0 && o.nnz > 0) {
+            const unsigned g = unsigned(std::max(1, std::min(out->nblk, 4 * h->sms)));
+            nir::k_pad_stream<double><<<g, nir::kBlock, 0, h->stream>>>(blk, out->nblk, o.ci, o.v_orig, out->ci,
+                                                                        out->v64);
+            NIR_LAUNCHED();
+        }
+    }
     out->lo = h->alloc<int>(lo.size());
     h2d(h, out->lo, lo.data(), lo.size() * sizeof(int));
-    const size_t q = size_t(all.back().z);
-    out->ci = h->allocz<int>(q, 8);
-    out->v64 = h->allocz<double>(q, 8);
-    out->v32 = h->allocz<float>(q, 8);
-    if (out->nblk > 0 && o.nnz > 0) {
-        const unsigned g = unsigned(std::max(1, std::min(out->nblk, 4 * h->sms)));
-        nir::k_pad_stream<double><<<g, nir::kBlock, 0, h->stream>>>(out->blk, out->nblk, o.ci, o.v_orig, out->ci,
-                                                                    out->v64);
-        NIR_LAUNCHED();
-    }
     NIR_CUDA(cudaStreamSynchronize(h->stream));
 }
 
-// The scaled values (written by precondition) into the padded streams.
+// The scaled values (written by precondition) into the padded streams of
+// the orientations that use the CTA layout.
 void batch_pad_values(nir_pdhg_batch* B) {
     nir_pdhg* h = B->h;
     for (int t = 0; t < 2; ++t) {
         const nir_pdhg_batch::Orient2& L = t ? B->cur->at : B->cur->a;
         const Orient& o = t ? h->At : h->A;
-        if (L.nblk <= 0 || o.nnz <= 0) continue;
+        if (L.lay != nir::kLayCta || L.nblk <= 0 || o.nnz <= 0) continue;
+        const int4* blk = static_cast<const int4*>(L.blk);
         const unsigned g = unsigned(std::max(1, std::min(L.nblk, 4 * h->sms)));
-        nir::k_pad_stream<double><<<g, nir::kBlock, 0, h->stream>>>(L.blk, L.nblk, o.ci, o.v64, nullptr, L.v64);
-        nir::k_pad_stream<float><<<g, nir::kBlock, 0, h->stream>>>(L.blk, L.nblk, o.ci, o.v32, nullptr, L.v32);
+        nir::k_pad_stream<double><<<g, nir::kBlock, 0, h->stream>>>(blk, L.nblk, o.ci, o.v64, nullptr, L.v64);
+        nir::k_pad_stream<float><<<g, nir::kBlock, 0, h->stream>>>(blk, L.nblk, o.ci, o.v32, nullptr, L.v32);
         NIR_LAUNCHED();
     }
 }
@@ -101,12 +125,25 @@ nir::BatchArgs bargs(nir_pdhg_batch* B, bool transpose, double* part, int i, int
     nir_pdhg* h = B->h;
     const Orient& o = transpose ? h->At : h->A;
     const nir_pdhg_batch::Orient2& L = transpose ? B->cur->at : B->cur->a;
-    return nir::BatchArgs{L.blk, L.nblk, o.rp, L.ci, part, B->insts, i, halpern, phase, rho};
+    return nir::BatchArgs{nir::Lay{L.blk, L.nblk, L.cap, o.rp, L.ci}, L.inst, part, B->insts, i, halpern, phase, rho};
 }
 
-// One launch chunk of the batch; TV = value type, TX = iterate type.
-template <typename TV, typename TX, int E>
-void launch_batch_chunk_e(nir_pdhg_batch* B, const SolveCfg& cfg, int phase) {
+// Calls f(LP, LD) with the batch layouts of A' and A.
+template <class F>
+void with_batch_lays(const nir_pdhg_batch* B, F&& f) {
+    using W = std::integral_constant<int, nir::kLayWarp>;
+    using Cc = std::integral_constant<int, nir::kLayCta>;
+    const bool pc = B->cur->at.lay == nir::kLayCta, dc = B->cur->a.lay == nir::kLayCta;
+    if (pc && dc) f(Cc{}, Cc{});
+    else if (pc) f(Cc{}, W{});
+    else if (dc) f(W{}, Cc{});
+    else f(W{}, W{});
+}
+
+// One launch chunk of the batch; TV = value type, TX = iterate type, LP /
+// LD = layouts of A' / A.
+template <typename TV, typename TX, int LP, int LD>
+void launch_batch_chunk_l(nir_pdhg_batch* B, const SolveCfg& cfg, int phase) {
     nir_pdhg* h = B->h;
     cudaStream_t s = h->stream;
     const int K = cfg.K;
@@ -116,16 +153,18 @@ void launch_batch_chunk_e(nir_pdhg_batch* B, const SolveCfg& cfg, int phase) {
     double* D = P + 2 * size_t(std::max(LT.nblk, 1));
     double* KR = D + 2 * size_t(std::max(LA.nblk, 1));
     double* KC = KR + 4 * size_t(std::max(LA.nblk, 1));
-    const int gp1 = cta_grid(h, nir::k_bprimal<TV, TX, E, true>, LT.nblk);
-    const int gp0 = cta_grid(h, nir::k_bprimal<TV, TX, E, false>, LT.nblk);
-    const int gd1 = cta_grid(h, nir::k_bdual<TV, TX, E, true>, LA.nblk);
-    const int gd0 = cta_grid(h, nir::k_bdual<TV, TX, E, false>, LA.nblk);
-    const int gkr = cta_grid(h, nir::k_bkkt_rows<TX, E>, LA.nblk);
-    const int gkc = cta_grid(h, nir::k_bkkt_cols<TX, E>, LT.nblk);
+    const size_t sp = lay_smem<LP, TX>(), sd = lay_smem<LD, TX>();
+    const int gp1 = lay_grid<LP, TX>(h, nir::k_bprimal<LP, TV, TX, true>, LT.nblk);
+    const int gp0 = lay_grid<LP, TX>(h, nir::k_bprimal<LP, TV, TX, false>, LT.nblk);
+    const int gd1 = lay_grid<LD, TX>(h, nir::k_bdual<LD, TV, TX, true>, LA.nblk);
+    const int gd0 = lay_grid<LD, TX>(h, nir::k_bdual<LD, TV, TX, false>, LA.nblk);
+    const int gkr = lay_grid<LD, double>(h, nir::k_bkkt_rows<LD, TX>, LA.nblk);
+    const int gkc = lay_grid<LP, double>(h, nir::k_bkkt_cols<LP, TX>, LT.nblk);
     int i_first = 0;
     if (cfg.persistent && K > 1) {
         // iterations 0..K-2 in one cooperative launch; the check pair below
-        const int gc = cta_grid(h, nir::k_bchunk<TV, TX, E>, std::max(LA.nblk, LT.nblk));
+        const int gc = std::min(lay_grid<LP, TX>(h, nir::k_bchunk<LP, LD, TV, TX>, LT.nblk),
+                                lay_grid<LD, TX>(h, nir::k_bchunk<LP, LD, TV, TX>, LA.nblk));
         nir::BatchArgs ap = bargs(B, true, P, 0, cfg.halpern, phase, cfg.p.reflection);
         nir::BatchArgs ad = bargs(B, false, D, 0, cfg.halpern, phase, cfg.p.reflection);
         nir::ChunkPtrs<TV, TX> v{bvals<TV>(LT),  bvals<TV>(LA),  Vec<TX>::x(h),  Vec<TX>::xb(h), Vec<TX>::xp(h),
@@ -136,8 +175,8 @@ void launch_batch_chunk_e(nir_pdhg_batch* B, const SolveCfg& cfg, int phase) {
         nir::DevState* insts = B->insts;
         int i0 = 0, iters = K - 1, count = B->count;
         void* args[] = {&ap, &ad, &v, &i0, &iters, &gs, &insts, &count};
-        NIR_CUDA(cudaLaunchCooperativeKernel((const void*)nir::k_bchunk<TV, TX, E>, dim3(gc), dim3(nir::kBlock), args,
-                                             0, s));
+        NIR_CUDA(cudaLaunchCooperativeKernel((const void*)nir::k_bchunk<LP, LD, TV, TX>, dim3(gc), dim3(nir::kBlock),
+                                             args, std::max(sp, sd), s));
         h->launches += 1;
         i_first = K - 1;
     }
@@ -146,31 +185,31 @@ void launch_batch_chunk_e(nir_pdhg_batch* B, const SolveCfg& cfg, int phase) {
         nir::BatchArgs ap = bargs(B, true, P, i, cfg.halpern, phase, cfg.p.reflection);
         nir::BatchArgs ad = bargs(B, false, D, i, cfg.halpern, phase, cfg.p.reflection);
         if (check)
-            nir::k_bprimal<TV, TX, E, true><<<gp1, nir::kBlock, 0, s>>>(
+            nir::k_bprimal<LP, TV, TX, true><<<gp1, nir::kBlock, sp, s>>>(
                 ap, bvals<TV>(LT), Vec<TX>::y(h), Vec<TX>::x(h), Vec<TX>::xb(h), Vec<TX>::xp(h), Vec<TX>::c(h),
                 Vec<TX>::l(h), Vec<TX>::u(h), Vec<TX>::x0(h));
         else
-            nir::k_bprimal<TV, TX, E, false><<<gp0, nir::kBlock, 0, s>>>(
+            nir::k_bprimal<LP, TV, TX, false><<<gp0, nir::kBlock, sp, s>>>(
                 ap, bvals<TV>(LT), Vec<TX>::y(h), Vec<TX>::x(h), Vec<TX>::xb(h), Vec<TX>::xp(h), Vec<TX>::c(h),
                 Vec<TX>::l(h), Vec<TX>::u(h), Vec<TX>::x0(h));
         NIR_LAUNCHED();
         if (check)
-            nir::k_bdual<TV, TX, E, true><<<gd1, nir::kBlock, 0, s>>>(ad, bvals<TV>(LA), Vec<TX>::xb(h), Vec<TX>::y(h),
-                                                                      Vec<TX>::yp(h), Vec<TX>::rl(h), Vec<TX>::ru(h),
-                                                                      Vec<TX>::y0(h));
+            nir::k_bdual<LD, TV, TX, true><<<gd1, nir::kBlock, sd, s>>>(ad, bvals<TV>(LA), Vec<TX>::xb(h),
+                                                                        Vec<TX>::y(h), Vec<TX>::yp(h), Vec<TX>::rl(h),
+                                                                        Vec<TX>::ru(h), Vec<TX>::y0(h));
         else
-            nir::k_bdual<TV, TX, E, false><<<gd0, nir::kBlock, 0, s>>>(ad, bvals<TV>(LA), Vec<TX>::xb(h),
-                                                                       Vec<TX>::y(h), Vec<TX>::yp(h), Vec<TX>::rl(h),
-                                                                       Vec<TX>::ru(h), Vec<TX>::y0(h));
+            nir::k_bdual<LD, TV, TX, false><<<gd0, nir::kBlock, sd, s>>>(ad, bvals<TV>(LA), Vec<TX>::xb(h),
+                                                                         Vec<TX>::y(h), Vec<TX>::yp(h), Vec<TX>::rl(h),
+                                                                         Vec<TX>::ru(h), Vec<TX>::y0(h));
         NIR_LAUNCHED();
         h->launches += 2;
     }
     nir::BatchArgs kr = bargs(B, false, KR, 0, 0, phase, 0.0);
-    nir::k_bkkt_rows<TX, E><<<gkr, nir::kBlock, 0, s>>>(kr, LA.v64, Vec<TX>::xp(h), Vec<TX>::yp(h), h->dr, h->rl,
-                                                        h->ru);
+    nir::k_bkkt_rows<LD, TX><<<gkr, nir::kBlock, lay_smem<LD, double>(), s>>>(kr, LA.v64, Vec<TX>::xp(h),
+                                                                             Vec<TX>::yp(h), h->dr, h->rl, h->ru);
     nir::BatchArgs kc = bargs(B, true, KC, 0, 0, phase, 0.0);
-    nir::k_bkkt_cols<TX, E><<<gkc, nir::kBlock, 0, s>>>(kc, LT.v64, Vec<TX>::xp(h), Vec<TX>::yp(h), h->dc, h->c,
-                                                        h->l, h->u);
+    nir::k_bkkt_cols<LP, TX><<<gkc, nir::kBlock, lay_smem<LP, double>(), s>>>(kc, LT.v64, Vec<TX>::xp(h),
+                                                                             Vec<TX>::yp(h), h->dc, h->c, h->l, h->u);
     NIR_LAUNCHED();
     nir::CtlArgs ca{};
     ca.K = K;
@@ -200,22 +239,25 @@ void launch_batch_chunk_e(nir_pdhg_batch* B, const SolveCfg& cfg, int phase) {
 
 template <typename TV, typename TX>
 void launch_batch_chunk(nir_pdhg_batch* B, const SolveCfg& cfg, int phase) {
-    with_run_len(B->cur->cap, [&](auto e) { launch_batch_chunk_e<TV, TX, decltype(e)::value>(B, cfg, phase); });
+    with_batch_lays(B, [&](auto lp, auto ld) {
+        launch_batch_chunk_l<TV, TX, decltype(lp)::value, decltype(ld)::value>(B, cfg, phase);
+    });
 }
 
 template <typename TV, typename TX>
 void warm_batch_cfgs(nir_pdhg_batch* B) {
     nir_pdhg* h = B->h;
-    with_run_len(B->cur->cap, [&](auto e) {
-        constexpr int E = decltype(e)::value;
+    with_batch_lays(B, [&](auto lp, auto ld) {
+        constexpr int LP = decltype(lp)::value, LD = decltype(ld)::value;
         const int na = B->cur->a.nblk, nt = B->cur->at.nblk;
-        cta_grid(h, nir::k_bprimal<TV, TX, E, true>, nt);
-        cta_grid(h, nir::k_bprimal<TV, TX, E, false>, nt);
-        cta_grid(h, nir::k_bdual<TV, TX, E, true>, na);
-        cta_grid(h, nir::k_bdual<TV, TX, E, false>, na);
-        cta_grid(h, nir::k_bkkt_rows<TX, E>, na);
-        cta_grid(h, nir::k_bkkt_cols<TX, E>, nt);
-        cta_grid(h, nir::k_bchunk<TV, TX, E>, std::max(na, nt));
+        lay_grid<LP, TX>(h, nir::k_bprimal<LP, TV, TX, true>, nt);
+        lay_grid<LP, TX>(h, nir::k_bprimal<LP, TV, TX, false>, nt);
+        lay_grid<LD, TX>(h, nir::k_bdual<LD, TV, TX, true>, na);
+        lay_grid<LD, TX>(h, nir::k_bdual<LD, TV, TX, false>, na);
+        lay_grid<LD, double>(h, nir::k_bkkt_rows<LD, TX>, na);
+        lay_grid<LP, double>(h, nir::k_bkkt_cols<LP, TX>, nt);
+        lay_grid<LP, TX>(h, nir::k_bchunk<LP, LD, TV, TX>, nt);
+        lay_grid<LD, TX>(h, nir::k_bchunk<LP, LD, TV, TX>, na);
     });
 }
 
@@ -304,17 +346,21 @@ int batch_solve_impl(nir_pdhg_batch* B, const nir_pdhg_params& p, int (*poll)(vo
     if (p.algorithm != NIR_ALGO_PDLP) throw std::invalid_argument("the batch runs NIR_ALGO_PDLP only");
     if (p.check_every < 1 || p.reflection < 0.0 || p.reflection > 1.0 || !(p.tol >= 0.0))
         throw std::invalid_argument("invalid parameters");
-    const int cap = pick_cap(h, p);  // timed on the block-diagonal matrix
-    if (!B->cur || B->cur->cap != cap) {
+    // layouts timed on the block-diagonal matrix, then built per instance
+    const LayChoice lc = pick_layouts(h, p);
+    auto same = [](const LayChoice& a, const LayChoice& b) {
+        return a.lay_a == b.lay_a && a.cap_a == b.cap_a && a.lay_at == b.lay_at && a.cap_at == b.cap_at;
+    };
+    if (!B->cur || !same(B->cur->choice, lc)) {
         B->cur = nullptr;
         for (auto& l : B->layouts)
-            if (l.cap == cap) B->cur = &l;
+            if (same(l.choice, lc)) B->cur = &l;
         if (!B->cur) {
             B->layouts.emplace_back();
             nir_pdhg_batch::Layout& l = B->layouts.back();
-            l.cap = cap;
-            batch_blocks(B, h->A, B->row_off, cap, &l.a);
-            batch_blocks(B, h->At, B->col_off, cap, &l.at);
+            l.choice = lc;
+            batch_blocks(B, h->A, B->row_off, lc.lay_a, lc.lay_a == nir::kLayCta ? kCtaCap : lc.cap_a, &l.a);
+            batch_blocks(B, h->At, B->col_off, lc.lay_at, lc.lay_at == nir::kLayCta ? kCtaCap : lc.cap_at, &l.at);
             l.part = h->alloc<double>(6 * size_t(std::max(l.a.nblk, 1)) + 6 * size_t(std::max(l.at.nblk, 1)));
             B->cur = &l;
         }
@@ -411,7 +457,8 @@ int batch_solve_impl(nir_pdhg_batch* B, const nir_pdhg_params& p, int (*poll)(vo
         const int per = 2 * cfg.K + 7;
         if (p.use_graphs && !cfg.persistent) {
             KeyHash k;
-            k.add(chunk_key(h, cfg, phase, prec)).add(B->cur->a.blk).add(B->cur->at.blk).add(B->cur->part).add(B->insts);
+            k.add(chunk_key(h, cfg, phase, prec)).add(B->cur->a.blk).add(B->cur->at.blk).add(B->cur->a.lay);
+            k.add(B->cur->at.lay).add(B->cur->a.cap).add(B->cur->at.cap).add(B->cur->part).add(B->insts);
             ChunkGraph& g = B->graphs[phase];
             if (!(g.ge && g.valid && g.key == k.h)) {
                 // capture into the handle's slot, then keep it with the batch

@@ -248,7 +248,7 @@ KktReport kkt_of_point(nir_pdhg* h, const nir_pdhg_params& p, const std::vector<
                        const std::vector<double>& y) {
     cudaStream_t s = h->stream;
     const int n = h->n, m = h->m;
-    if (h->A.it < 0) use_cta(h, auto_cta_cap(h));
+    if (h->A.lay < 0 || h->At.lay < 0) use_layouts(h, default_layouts(h));
     precondition(h, p, false);  // unit scales: the scaled copies equal the original LP
     pad_scaled(h);
     ensure_partials(h);

@@ -2,11 +2,11 @@
 //
 // The instances are laid out block-diagonally in one handle: instance i
 // owns rows [row_off[i], row_off[i+1]) and columns [col_off[i],
-// col_off[i+1]), and its CTA blocks (which never cross an instance) are
-// contiguous.  Every instance keeps its own DevState on the device:
+// col_off[i+1]), and its blocks (which never cross an instance) are
+// contiguous, in either layout of k_iter.cuh.  Every instance keeps its own DevState on the device:
 // step sizes, primal weight, Halpern counter, restart anchor, precision
 // phase and convergence flag.  The iteration kernels look up the instance
-// of each CTA block, skip converged instances, and in a check launch
+// of each block, skip converged instances, and in a check launch
 // leave one partial sum per quantity and block; the controller then runs
 // one CTA per instance, reducing that instance's block range in a fixed
 // order (deterministic) and applying the same update as the single-LP
@@ -19,10 +19,8 @@
 namespace nir {
 
 struct BatchArgs {
-    const int4* blk;      // CTA-block descriptors; .w = the block's instance
-    int nblk;
-    const int* rp;
-    const int* ci;        // padded column indices
+    Lay lay;              // blocks never cross an instance
+    const int* blk_inst;  // kLayWarp: instance of each warp row block (kLayCta: the descriptor's 4th field)
     double* part;         // per-block partials: part[q * nblk + block]
     const DevState* inst;
     int i_in_chunk;
@@ -33,11 +31,23 @@ struct BatchArgs {
 
 __device__ __forceinline__ bool inst_active(const DevState& s, int phase) { return !s.done && s.phase == phase; }
 
-// Reduces each per-thread quantity over the CTA into the block's partial
-// slot and clears it for the next block.
+// Warp layout: reduces each per-lane quantity over the warp into the
+// block's partial slot and clears it for the next block.
 template <class Epi>
-__device__ __forceinline__ void flush_block_partials(Epi& epi, double* __restrict__ part, int nblk, int b,
-                                                     double* s_red) {
+__device__ __forceinline__ void flush_warp_partials(Epi& epi, double* __restrict__ part, int nblk, int b) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int q = 0; q < Epi::NQ; ++q) {
+        const double v = (Epi::kLastIsMax && q == Epi::NQ - 1) ? warp_max(epi.q[q]) : warp_sum(epi.q[q]);
+        if (lane == 0) part[q * nblk + b] = v;
+        epi.q[q] = 0.0;
+    }
+}
+
+// CTA layout: the same over the CTA.
+template <class Epi>
+__device__ __forceinline__ void flush_cta_partials(Epi& epi, double* __restrict__ part, int nblk, int b,
+                                                   double* s_red) {
 #pragma unroll
     for (int q = 0; q < Epi::NQ; ++q) {
         const double v = (Epi::kLastIsMax && q == Epi::NQ - 1) ? block_max(epi.q[q], s_red) : block_sum(epi.q[q], s_red);
@@ -46,31 +56,80 @@ __device__ __forceinline__ void flush_block_partials(Epi& epi, double* __restric
     }
 }
 
-// cta_spmv over the batch: per block, the instance decides whether the
-// block runs and with which scalars (SetFn(epi, DevState&)).  The decision
-// is the same for every thread of the CTA.
-template <typename TA, typename TV, typename TX, int E, class Epi, bool COH = false, class SetFn>
-__device__ __forceinline__ void cta_spmv_batch(const BatchArgs& a, const TV* __restrict__ val,
-                                               const TX* __restrict__ x, Epi& epi, SetFn set, CtaShared<TA>* sm,
-                                               double* s_red) {
-    int k = 0;
-    for (int b = blockIdx.x; b < a.nblk; b += gridDim.x) {
-        const int4 d0 = __ldg(a.blk + b), d1 = __ldg(a.blk + b + 1);
-        const DevState& s = a.inst[d0.w];
-        if (!inst_active(s, a.phase)) continue;
-        set(epi, s);
-        cta_block<TA, TV, TX, E, Epi, COH>(d0, d1, a.rp, a.ci, val, x, epi, sm[k & 1]);
-        ++k;
-        if (Epi::NQ > 0) flush_block_partials(epi, a.part, a.nblk, b, s_red);
+// The layout's SpMV over the batch: per block, the instance decides whether
+// the block runs and with which scalars (SetFn(epi, DevState&)).  In the CTA
+// layout the decision is the same for every thread of the CTA.
+template <int LAY, typename TA, typename TV, typename TX, class Epi, bool COH = false, class SetFn>
+__device__ __forceinline__ void lay_spmv_batch(const BatchArgs& a, const TV* __restrict__ val,
+                                               const TX* __restrict__ x, Epi& epi, SetFn set, double* s_red) {
+    const Lay& L = a.lay;
+    if constexpr (LAY == kLayWarp) {
+        extern __shared__ __align__(16) unsigned char nir_smem[];
+        const int w = threadIdx.x >> 5;
+        TA* s_prod = reinterpret_cast<TA*>(nir_smem) + w * kWarpCapMax;
+        const int2* blk = static_cast<const int2*>(L.blk);
+        const int G = gridDim.x * kWarps;
+        int b = blockIdx.x * kWarps + w;
+        if (b >= L.nblk) return;
+        int2 d0 = __ldg(blk + b), d1 = __ldg(blk + b + 1);
+        int inst = __ldg(a.blk_inst + b);
+        bool act = inst_active(a.inst[inst], a.phase);
+        int c[kWarpU];
+        TV v[kWarpU];
+        stream_load<TV>(d0, d1, act ? L.cap : -1, L.ci, val, c, v);
+        for (;;) {
+            const int bn = b + G;
+            const bool has_next = bn < L.nblk;
+            int2 n0 = make_int2(0, 0), n1 = make_int2(0, 0);
+            int inst_n = 0;
+            bool act_n = false;
+            if (has_next) {
+                n0 = __ldg(blk + bn);
+                n1 = __ldg(blk + bn + 1);
+                inst_n = __ldg(a.blk_inst + bn);
+                act_n = inst_active(a.inst[inst_n], a.phase);
+            }
+            int cn[kWarpU];
+            TV vn[kWarpU];
+            stream_load<TV>(n0, n1, act_n ? L.cap : -1, L.ci, val, cn, vn);
+            if (act) {
+                set(epi, a.inst[inst]);
+                warp_process<TA, TV, TX, Epi, COH>(d0, d1, L.cap, L.rp, L.ci, val, x, epi, s_prod, c, v);
+                if (Epi::NQ > 0) flush_warp_partials(epi, a.part, L.nblk, b);
+            }
+            if (!has_next) break;
+#pragma unroll
+            for (int q = 0; q < kWarpU; ++q) {
+                c[q] = cn[q];
+                v[q] = vn[q];
+            }
+            d0 = n0;
+            d1 = n1;
+            inst = inst_n;
+            act = act_n;
+            b = bn;
+        }
+    } else {
+        __shared__ CtaShared<TA> sm[2];
+        const int4* blk = static_cast<const int4*>(L.blk);
+        int k = 0;
+        for (int b = blockIdx.x; b < L.nblk; b += gridDim.x) {
+            const int4 d0 = __ldg(blk + b), d1 = __ldg(blk + b + 1);
+            const DevState& s = a.inst[d0.w];
+            if (!inst_active(s, a.phase)) continue;
+            set(epi, s);
+            cta_block<TA, TV, TX, LAY, Epi, COH>(d0, d1, L.rp, L.ci, val, x, epi, sm[k & 1]);
+            ++k;
+            if (Epi::NQ > 0) flush_cta_partials(epi, a.part, L.nblk, b, s_red);
+        }
     }
 }
 
-template <typename TV, typename TX, int E, bool CHECK>
-__global__ void __launch_bounds__(kBlock, cta_min_blocks<TX, E>())
+template <int LAY, typename TV, typename TX, bool CHECK>
+__global__ void __launch_bounds__(kBlock, (lay_min_blocks<LAY, TX>()))
     k_bprimal(BatchArgs a, const TV* __restrict__ val, const TX* __restrict__ y, TX* __restrict__ x,
               TX* __restrict__ xbar, TX* __restrict__ xplus, const TX* __restrict__ c, const TX* __restrict__ lo,
               const TX* __restrict__ up, const TX* __restrict__ x0) {
-    __shared__ CtaShared<TX> sm[2];
     __shared__ double s_red[kWarps];
     PrimalEpi<TX, CHECK> epi;
     epi.x = x;
@@ -81,16 +140,15 @@ __global__ void __launch_bounds__(kBlock, cta_min_blocks<TX, E>())
     epi.up = up;
     epi.x0 = x0;
     epi.halpern = a.halpern;
-    cta_spmv_batch<TX, TV, TX, E>(a, val, y, epi, [&](PrimalEpi<TX, CHECK>& e, const DevState& s) {
+    lay_spmv_batch<LAY, TX, TV, TX>(a, val, y, epi, [&](PrimalEpi<TX, CHECK>& e, const DevState& s) {
         e.s = step_scalars<TX>(&s, a.i_in_chunk, a.halpern, a.rho);
-    }, sm, s_red);
+    }, s_red);
 }
 
-template <typename TV, typename TX, int E, bool CHECK>
-__global__ void __launch_bounds__(kBlock, cta_min_blocks<TX, E>())
+template <int LAY, typename TV, typename TX, bool CHECK>
+__global__ void __launch_bounds__(kBlock, (lay_min_blocks<LAY, TX>()))
     k_bdual(BatchArgs a, const TV* __restrict__ val, const TX* __restrict__ xbar, TX* __restrict__ y,
             TX* __restrict__ yplus, const TX* __restrict__ rl, const TX* __restrict__ ru, const TX* __restrict__ y0) {
-    __shared__ CtaShared<TX> sm[2];
     __shared__ double s_red[kWarps];
     DualEpi<TX, CHECK> epi;
     epi.y = y;
@@ -99,32 +157,30 @@ __global__ void __launch_bounds__(kBlock, cta_min_blocks<TX, E>())
     epi.ru = ru;
     epi.y0 = y0;
     epi.halpern = a.halpern;
-    cta_spmv_batch<TX, TV, TX, E>(a, val, xbar, epi, [&](DualEpi<TX, CHECK>& e, const DevState& s) {
+    lay_spmv_batch<LAY, TX, TV, TX>(a, val, xbar, epi, [&](DualEpi<TX, CHECK>& e, const DevState& s) {
         e.s = step_scalars<TX>(&s, a.i_in_chunk, a.halpern, a.rho);
-    }, sm, s_red);
+    }, s_red);
 }
 
-template <typename TX, int E>
-__global__ void __launch_bounds__(kBlock, cta_min_blocks<double, E>())
+template <int LAY, typename TX>
+__global__ void __launch_bounds__(kBlock)
     k_bkkt_rows(BatchArgs a, const double* __restrict__ val, const TX* __restrict__ xplus,
                 const TX* __restrict__ yplus, const double* __restrict__ dr, const double* __restrict__ rl,
                 const double* __restrict__ ru) {
-    __shared__ CtaShared<double> sm[2];
     __shared__ double s_red[kWarps];
     KktRowEpi<TX> epi;
     epi.dr = dr;
     epi.rl = rl;
     epi.ru = ru;
     epi.yplus = yplus;
-    cta_spmv_batch<double, double, TX, E>(a, val, xplus, epi, [](KktRowEpi<TX>&, const DevState&) {}, sm, s_red);
+    lay_spmv_batch<LAY, double, double, TX>(a, val, xplus, epi, [](KktRowEpi<TX>&, const DevState&) {}, s_red);
 }
 
-template <typename TX, int E>
-__global__ void __launch_bounds__(kBlock, cta_min_blocks<double, E>())
+template <int LAY, typename TX>
+__global__ void __launch_bounds__(kBlock)
     k_bkkt_cols(BatchArgs a, const double* __restrict__ val, const TX* __restrict__ xplus,
                 const TX* __restrict__ yplus, const double* __restrict__ dc, const double* __restrict__ c,
                 const double* __restrict__ l, const double* __restrict__ u) {
-    __shared__ CtaShared<double> sm[2];
     __shared__ double s_red[kWarps];
     KktColEpi<TX> epi;
     epi.dc = dc;
@@ -132,7 +188,7 @@ __global__ void __launch_bounds__(kBlock, cta_min_blocks<double, E>())
     epi.l = l;
     epi.u = u;
     epi.xplus = xplus;
-    cta_spmv_batch<double, double, TX, E>(a, val, yplus, epi, [](KktColEpi<TX>&, const DevState&) {}, sm, s_red);
+    lay_spmv_batch<LAY, double, double, TX>(a, val, yplus, epi, [](KktColEpi<TX>&, const DevState&) {}, s_red);
 }
 
 struct BatchCtlArgs {

@@ -8,13 +8,13 @@
 // are tested.
 //
 // One cooperative launch runs the non-check iterations of a chunk: the
-// primal phase over all CTA blocks of A', a grid barrier, the dual phase
-// over A, a grid barrier, and so on.  The block code and the per-row
-// summation order are those of k_primal / k_dual, so the iterates are
-// bit-identical to the two-kernel path; the gathers go through L2
-// (cta_gather<true>) because the gathered vectors change inside the launch.
-// Every CTA keeps the same blocks in every iteration, so a row's own x / y
-// entries are read back only by the CTA that wrote them.
+// primal phase over all blocks of A', a grid barrier, the dual phase over A,
+// a grid barrier, and so on.  The block code and the per-row summation
+// order are those of k_primal / k_dual, so the iterates are bit-identical
+// to the two-kernel path; the gathers go through L2 because the gathered
+// vectors change inside the launch.  Every warp (warp layout) or CTA (CTA
+// layout) keeps the same blocks in every iteration, so a row's own x / y
+// entries are read back only by the one that wrote them.
 //
 // The barrier is a counter and a generation word in global memory.  A
 // cooperative launch makes every CTA co-resident, so it always completes;
@@ -75,19 +75,22 @@ struct ChunkPtrs {
     const TX *c, *l, *u, *x0, *rl, *ru, *y0;
 };
 
-template <typename TV, typename TX, int E>
-__global__ void __launch_bounds__(kBlock, cta_min_blocks<TX, E>())
+// LP / LD: layouts of A' (primal phase) and A (dual phase).  A kernel that
+// mixes the layouts needs both kinds of shared memory; its dynamic part is
+// the warp layout's.
+template <int LP, int LD, typename TV, typename TX>
+__global__ void __launch_bounds__(kBlock, (lay_min_blocks<LP, TX>() < lay_min_blocks<LD, TX>() ? lay_min_blocks<LP, TX>()
+                                                                                                : lay_min_blocks<LD, TX>()))
     k_chunk(IterArgs ap, IterArgs ad, ChunkPtrs<TV, TX> v, int i0, int iters, GridSync gs, DevState* st) {
-    __shared__ CtaShared<TX> sm[2];
     __shared__ double s_red[kWarps];
     // no kernel changes the state during a chunk: every CTA decides alike
     if (ap.st->done || ap.st->phase != ap.phase) return;
     for (int i = i0; i < i0 + iters; ++i) {
         ap.i_in_chunk = i;
         ad.i_in_chunk = i;
-        primal_phase<TV, TX, E, false, true>(ap, v.valAt, v.y, v.x, v.xb, v.xp, v.c, v.l, v.u, v.x0, sm, s_red);
+        primal_phase<LP, TV, TX, false, true>(ap, v.valAt, v.y, v.x, v.xb, v.xp, v.c, v.l, v.u, v.x0, s_red);
         if (!grid_sync(gs)) break;
-        dual_phase<TV, TX, E, false, true>(ad, v.valA, v.xb, v.y, v.yp, v.rl, v.ru, v.y0, sm, s_red);
+        dual_phase<LD, TV, TX, false, true>(ad, v.valA, v.xb, v.y, v.yp, v.rl, v.ru, v.y0, s_red);
         if (!grid_sync(gs)) break;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0 && *(volatile int*)gs.err) {
@@ -96,16 +99,16 @@ __global__ void __launch_bounds__(kBlock, cta_min_blocks<TX, E>())
     }
 }
 
-// The batched chunk: the same loop over the batch's CTA blocks
-// (k_batch.cuh), each block running only while its instance is active.
-// No kernel changes an instance's state inside the launch, so every CTA
-// skips the same blocks.  On a barrier that gave up, every instance still
-// running ends with NIR_STATUS_INTERNAL_ERROR.
-template <typename TV, typename TX, int E>
-__global__ void __launch_bounds__(kBlock, cta_min_blocks<TX, E>())
+// The batched chunk: the same loop over the batch's blocks (k_batch.cuh),
+// each block running only while its instance is active.  No kernel changes
+// an instance's state inside the launch, so every CTA skips the same
+// blocks.  On a barrier that gave up, every instance still running ends
+// with NIR_STATUS_INTERNAL_ERROR.
+template <int LP, int LD, typename TV, typename TX>
+__global__ void __launch_bounds__(kBlock, (lay_min_blocks<LP, TX>() < lay_min_blocks<LD, TX>() ? lay_min_blocks<LP, TX>()
+                                                                                                : lay_min_blocks<LD, TX>()))
     k_bchunk(BatchArgs ap, BatchArgs ad, ChunkPtrs<TV, TX> v, int i0, int iters, GridSync gs, DevState* insts,
              int count) {
-    __shared__ CtaShared<TX> sm[2];
     __shared__ double s_red[kWarps];
     for (int i = i0; i < i0 + iters; ++i) {
         ap.i_in_chunk = i;
@@ -119,10 +122,10 @@ __global__ void __launch_bounds__(kBlock, cta_min_blocks<TX, E>())
         pe.up = v.u;
         pe.x0 = v.x0;
         pe.halpern = ap.halpern;
-        cta_spmv_batch<TX, TV, TX, E, PrimalEpi<TX, false>, true>(
+        lay_spmv_batch<LP, TX, TV, TX, PrimalEpi<TX, false>, true>(
             ap, v.valAt, v.y, pe,
             [&](PrimalEpi<TX, false>& e, const DevState& s) { e.s = step_scalars<TX>(&s, ap.i_in_chunk, ap.halpern, ap.rho); },
-            sm, s_red);
+            s_red);
         if (!grid_sync(gs)) break;
         DualEpi<TX, false> de;
         de.y = v.y;
@@ -131,10 +134,10 @@ __global__ void __launch_bounds__(kBlock, cta_min_blocks<TX, E>())
         de.ru = v.ru;
         de.y0 = v.y0;
         de.halpern = ad.halpern;
-        cta_spmv_batch<TX, TV, TX, E, DualEpi<TX, false>, true>(
+        lay_spmv_batch<LD, TX, TV, TX, DualEpi<TX, false>, true>(
             ad, v.valA, v.xb, de,
             [&](DualEpi<TX, false>& e, const DevState& s) { e.s = step_scalars<TX>(&s, ad.i_in_chunk, ad.halpern, ad.rho); },
-            sm, s_red);
+            s_red);
         if (!grid_sync(gs)) break;
     }
     if (blockIdx.x == 0 && *(volatile int*)gs.err) {

@@ -78,7 +78,8 @@ class KernelTime(C.Structure):
 
 class Layout(C.Structure):
     _fields_ = [("nrow", C.c_int32), ("ncol", C.c_int32), ("nnz", C.c_int64), ("blocks_a", C.c_int32),
-                ("blocks_at", C.c_int32), ("block_nnz", C.c_int32), ("device_bytes", C.c_int64)]
+                ("blocks_at", C.c_int32), ("block_nnz", C.c_int32), ("device_bytes", C.c_int64),
+                ("block_nnz_at", C.c_int32), ("pad_", C.c_int32)]
 
 
 POLL_FN = C.CFUNCTYPE(C.c_int, C.c_void_p)
