@@ -43,15 +43,23 @@ def test_groups_proportions_patterns_and_tolerance():
         [(0, 1.0), (2, -3.0)],                           # 2: another pattern
         [(0, 3.0), (2, -9.0), (5, 1.5 * (1 + 1e-7))],    # 3: 3 x column 0, eps within 1e-6
         [(0, 1.0), (2, -3.0), (5, 0.6)],                 # 4: same pattern, not parallel
-        [(1, 4.0)],                                      # 5: representative of its own
-        [(1, 8.0)],                                      # 6: 2 x column 5
+        [(1, 4.0), (4, 1.0)],                            # 5: representative of its own
+        [(1, 8.0), (4, 2.0)],                            # 6: 2 x column 5
         [],                                              # 7: empty: never grouped
         [],                                              # 8
+        [(3, 1.0)],                                      # 9: single entries: never grouped
+        [(3, 5.0)],                                      # 10
     ]
     rep, lam, groups = pdhg.parallel_groups(_lp_from_columns(cols, 6))
     assert groups == 2
-    assert rep.tolist() == [-1, 0, -1, 0, -1, -1, 5, -1, -1]
+    assert rep.tolist() == [-1, 0, -1, 0, -1, -1, 5, -1, -1, -1, -1]
     assert lam[1] == -2.0 and lam[3] == pytest.approx(3.0, rel=1e-12) and lam[6] == 2.0
+
+
+def test_power_law_lp_has_no_groups():
+    # its coincidental pairs are single-entry columns of one row
+    _, _, groups = pdhg.parallel_groups(L.generate(L.ZIPF, 1, m=20000, n=50000, target_nnz=500000))
+    assert groups == 0
 
 
 def test_rejects_a_malformed_lp():
