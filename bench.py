@@ -309,22 +309,48 @@ def run_ours(args, rank, world, local):
                     rel_kkt=i64.rel_kkt, objective=i64.objective)
     kt[pdhg.PREC_FP64] = eng.time_iteration(pdhg.PREC_FP64, reps=100)
     lay64 = eng.layout()
-    # plain SpMV with a cold L2 (the SpMV GB/s of the metric): the CTA-block
-    # kernel in each precision and the row-less gather ceilings
-    spmv = {}
-    for tr, side in ((False, "A"), (True, "At")):
-        for kname, kind, vw, xw, cap in (("cta_f32", pdhg.K_CTA32, 4, 4, lay_first.block_nnz),
-                                         ("cta_f32val_f64x", pdhg.K_CTA_MIXED, 4, 8, lay_first.block_nnz),
-                                         ("cta_f64", pdhg.K_CTA64, 8, 8, lay64.block_nnz),
-                                         ("ceiling_gather_f32", pdhg.K_CEIL_GATHER32, 4, 4, 0),
-                                         ("ceiling_gather_f64", pdhg.K_CEIL_GATHER64, 8, 8, 0),
-                                         ("ceiling_stream_f64", pdhg.K_CEIL_STREAM64, 8, 8, 0)):
-            us = eng.time_kernel(tr, kind, cap, reps=20, flush_l2=True)
-            by = spmv_bytes_w(lp, tr, vw, xw)
-            spmv[f"{side}_{kname}"] = {"us": us, "GBs": by / (us * 1e-6) / 1e9, "bytes": by, "block_nnz": cap}
+    # plain SpMV with a cold L2 (the SpMV GB/s of the metric): both layout
+    # families in each precision and the row-less gather ceilings
+    spmv = spmv_figures(eng, lp, lay_first, reps=20)
     eng.close()
     return dict(lp=lp, ms=ms, infos=infos, launches=launches, e2e=e2e, kt=kt, lay=lay_first, lay64=lay64,
                 clocks=clk.summary(), spmv=spmv, fp64=fp64)
+
+
+def spmv_figures(eng, lp, lay=None, reps=20):
+    """Cold-L2 CUDA-event times of the plain SpMV kernels of both layout
+    families (warp row blocks at the capacity the solve chose for that
+    orientation, else 256 and 128; CTA blocks of 256 x 4 nonzeros) in each
+    precision, and of the row-less ceilings over the same stream, with the
+    algorithmic GB/s of each.  `best_f32` / `best_f64` per orientation is the
+    faster family."""
+    from nirnaya_b200 import pdhg
+
+    out = {}
+    for tr, side in ((False, "A"), (True, "At")):
+        chosen = None if lay is None else (lay.block_nnz_at if tr else lay.block_nnz)
+        warp_caps = [chosen] if chosen is not None and chosen <= 256 else [256, 128]
+        rows = []
+        for cap in warp_caps:
+            rows += [("warp_f32", pdhg.K_WARP32, 4, 4, cap), ("warp_f64", pdhg.K_WARP64, 8, 8, cap)]
+        rows += [("cta_f32", pdhg.K_CTA32, 4, 4, 1024), ("cta_f32val_f64x", pdhg.K_CTA_MIXED, 4, 8, 1024),
+                 ("cta_f64", pdhg.K_CTA64, 8, 8, 1024),
+                 ("ceiling_gather_f32", pdhg.K_CEIL_GATHER32, 4, 4, 0),
+                 ("ceiling_gather_f64", pdhg.K_CEIL_GATHER64, 8, 8, 0),
+                 ("ceiling_stream_f64", pdhg.K_CEIL_STREAM64, 8, 8, 0)]
+        for kname, kind, vw, xw, cap in rows:
+            us = eng.time_kernel(tr, kind, cap, reps=reps, flush_l2=True)
+            by = spmv_bytes_w(lp, tr, vw, xw)
+            key = f"{side}_{kname}"
+            fig = {"us": us, "GBs": by / (us * 1e-6) / 1e9, "bytes": by, "block_nnz": cap}
+            if key not in out or us < out[key]["us"]:
+                out[key] = fig
+        for prec in ("f32", "f64"):
+            fam = min(("warp", "cta"), key=lambda f: out[f"{side}_{f}_{prec}"]["us"])
+            out[f"{side}_best_{prec}"] = {**out[f"{side}_{fam}_{prec}"], "family": fam,
+                                         "chosen_by_solve": None if chosen is None else
+                                         ("cta" if chosen > 256 else "warp")}
+    return out
 
 
 def cpu_baseline(lp, label, seconds=15.0, threads=None):
@@ -630,18 +656,7 @@ def run_blocks(args, local):
                np.concatenate([lp.rowup for lp in lps]))
     del Ab
     with pdhg.Engine(big, local) as eng:
-        sp_fig = {}
-        for tr, side in ((False, "A"), (True, "At")):
-            for kname, kind, vw, xw in (("cta_f32", pdhg.K_CTA32, 4, 4), ("cta_f32val_f64x", pdhg.K_CTA_MIXED, 4, 8),
-                                        ("cta_f64", pdhg.K_CTA64, 8, 8),
-                                        ("ceiling_gather_f32", pdhg.K_CEIL_GATHER32, 4, 4)):
-                best = None
-                for cap in ((1024, 2048) if kind < pdhg.K_CEIL_GATHER64 else (0,)):
-                    us = eng.time_kernel(tr, kind, cap, reps=10, flush_l2=True)
-                    if best is None or us < best[0]:
-                        best = (us, cap)
-                by = spmv_bytes_w(big, tr, vw, xw)
-                sp_fig[f"{side}_{kname}"] = {"us": best[0], "GBs": by / (best[0] * 1e-6) / 1e9, "block_nnz": best[1]}
+        sp_fig = spmv_figures(eng, big, None, reps=10)
         out["batch"]["spmv_cold"] = sp_fig
     del big
     # c4
@@ -1031,8 +1046,23 @@ def main():
     ap.add_argument("--host-path", action="store_true",
                     help="the CLI's host steps around PDHG (read, presolve, scale, verify, write_sol) "
                          "against the reference's")
+    ap.add_argument("--spmv-case", action="store_true",
+                    help="cold-L2 times of the plain SpMV kernels of both layout families and of the row-less "
+                         "gather ceilings on the workload's matrix (one JSON line), then exit")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
+    if args.spmv_case:
+        from nirnaya_b200 import lp as L
+        from nirnaya_b200 import pdhg
+
+        lp = L.generate(wl["kind"], wl["seed"], **wl["kw"])
+        with pdhg.Engine(lp, 0) as eng:
+            fig = spmv_figures(eng, lp, None, reps=10)
+        peak, peak_kind = peaks()
+        print(json.dumps({"workload": wl["label"], "nnz": lp.nnz, "hbm_peak_GBs": peak, "peak_kind": peak_kind,
+                          "timing": "CUDA events on the engine's stream, L2 flushed (512 MB write) before each "
+                                    "of 10 launches after one warm-up", "kernels": fig}))
+        return
     if args.host_path:
         host_path_bench(args)
         return

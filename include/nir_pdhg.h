@@ -89,8 +89,9 @@ typedef struct nir_pdhg_params {
     double primal_weight_smoothing; /* theta of the log-space weight update      (0.5)   */
     double step_factor;           /* eta = step_factor / ||A||_2 estimate        (0.998) */
     int32_t power_iters;          /* power-iteration rounds for ||A||_2          (64)    */
-    int32_t polish_stall_checks;  /* MIXED: FP64 polish after this many checks
-                                     without a 0.8x improvement of the best KKT   (40)   */
+    int32_t polish_stall_checks;  /* MIXED: FP64 polish after this many checks, and
+                                     half of the checks so far, without a 0.8x
+                                     improvement of the best KKT                  (40)   */
     double polish_switch_kkt;     /* MIXED: ... or as soon as KKT <= this        (0)     */
     int32_t spmv_block_nnz;       /* SpMV layout of both orientations: 32, 64, 128 or 256 =
                                      warp row blocks of that many nonzeros, 1024 = CTA
@@ -210,7 +211,10 @@ int nir_pdhg_time_spmv(nir_pdhg* h, int transpose, int kernel, int reps, int flu
  *   6-9  (timing only) the row-less ceilings: the stream of indices and
  *        values with the gathers of x (6 FP64, 7 FP32) or without them
  *        (8 FP64, 9 FP32), with no row structure at all
- * block_nnz: CTA-block capacity for 3-5 (256, 512, 1024 or 2048; 0 = 2048).
+ * block_nnz: CTA-block capacity for 3-5 (256, 512, 1024 or 2048; 0 = 1024,
+ * the capacity of the iteration kernels); nir_pdhg_time_kernel also takes
+ * the warp row-block capacity for 1-2 (32, 64, 128 or 256; 0 = the current
+ * blocks).
  * No counterpart in the reference: measurement of the SpMV kernels that
  * replace CscMatrix::spmv / spmv_transpose (src/core/csc_matrix.hpp:99-120). */
 int nir_pdhg_spmv_kernel(nir_pdhg* h, int transpose, int kernel, int block_nnz, const double* x, double* y);

@@ -2024,7 +2024,7 @@ int nir_pdhg_spmv_kernel(nir_pdhg* h, int transpose, int kernel, int block_nnz, 
         NIR_CUDA(cudaMemcpyAsync(din, x, nin * sizeof(double), cudaMemcpyHostToDevice, s));
         nir::k_to_float<<<std::max(grid_for(nin), 1u), nir::kBlock, 0, s>>>(nin, din, fin);
         NIR_LAUNCHED();
-        launch_kernel_kind(h, o, kernel, block_nnz > 0 ? block_nnz : 2048, din, fin, dout, fout);
+        launch_kernel_kind(h, o, kernel, block_nnz >= 256 ? block_nnz : kCtaCap, din, fin, dout, fout);
         if (kernel == 2 || kernel == 4) {
             nir::k_to_double<<<std::max(grid_for(nout), 1u), nir::kBlock, 0, s>>>(nout, fout, dout);
             NIR_LAUNCHED();
@@ -2052,9 +2052,15 @@ int nir_pdhg_time_kernel(nir_pdhg* h, int transpose, int kernel, int block_nnz, 
         cudaStream_t s = h->stream;
         Orient& o = transpose ? h->At : h->A;
         const int nin = o.cols;
-        if (!o.blk) set_blocks(h, o, auto_cap(h->nnz, o.rows));
+        // warp kinds: row blocks of capacity block_nnz (32..256), else the
+        // current ones (or the automatic capacity); CTA kinds: blocks of
+        // block_nnz (256..2048), else those of the iteration kernels (1024)
+        if (kernel == 1 || kernel == 2) {
+            if (block_nnz >= 32 && block_nnz <= nir::kWarpCapMax) set_blocks(h, o, block_nnz);
+            else if (!o.blk) set_blocks(h, o, auto_cap(h->nnz, o.rows));
+        }
         ensure_v32_orig(h, o);
-        const int cap = block_nnz > 0 ? block_nnz : 2048;
+        const int cap = block_nnz >= 256 ? block_nnz : kCtaCap;
         if (kernel >= 3 && kernel <= 5) cta_orig_values(h, o, cta_layout(h, o, cap));
         double* din = transpose ? h->tmp_m : h->tmp_n;
         double* dout = transpose ? h->tmp_n : h->tmp_m;

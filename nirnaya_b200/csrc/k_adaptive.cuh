@@ -598,7 +598,13 @@ __device__ void control_update(const CtlArgs& a, DevState* st, const CtlSums& su
         } else {
             st->stall += 1;
         }
-        if (st->stall >= a.polish_stall || kkt <= a.polish_switch) {
+        // a plateau counts as a stall only once it has lasted polish_stall
+        // checks and half of the checks so far: PDLP's own plateaus grow
+        // with its restart lengths (an artificial restart at 0.36 of the
+        // iterations so far), and a hand-over inside one of them only
+        // slows the solve down
+        const long long window = max((long long)a.polish_stall, (it / max(a.K, 1)) / 2);
+        if (st->stall >= window || kkt <= a.polish_switch) {
             st->switch_request = 1;
             st->phase = 1;
             return;
