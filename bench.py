@@ -536,6 +536,41 @@ def learned_figures(n_train, n_test, n_pdhg, pdhg_iters, epochs):
         tpl.append(time.perf_counter() - t1)
         itpl.append(ip.iterations)
         stpl.append(ip.status)
+    # what a warm start must achieve: PDLP iterations from the instance's own
+    # accurate solution (tol 1e-9) perturbed per entry by a relative Gaussian
+    # error, from the training mean, and from the network's prediction, with
+    # the relative distance of each start from that solution
+    ok = train.status == pdhg.OPTIMAL
+    xbar = train.x[ok].astype(np.float64).mean(0)
+    ybar = train.y[ok].astype(np.float64).mean(0)
+    sens = {"instances": len(sub_), "iterations": {}, "rel_dist_x": {}, "rel_dist_y": {}}
+    rows_ = []
+    for sd in sub_:
+        f_, g_ = fam.factors(sd)
+        rowlo, cost = fam.vectors(f_, g_)
+        eng.update_vectors(cost=cost, rowlo=rowlo)
+        _, _, ci = eng.solve(p)
+        xs, ys, si = eng.solve(pdhg.default_params(tol=1e-9, max_iters=1000000))
+        xp, yp, wp = model.predict(f_, g_)
+        rng = np.random.default_rng(sd)
+        starts = {"cold": None, "network": (xp, yp, wp), "training_mean": (xbar, ybar, wp)}
+        for eps in (1e-3, 1e-2, 1e-1):
+            starts[f"own_solution_rel_err_{eps:g}"] = (xs * (1 + eps * rng.standard_normal(xs.size)),
+                                                        ys * (1 + eps * rng.standard_normal(ys.size)), si.primal_weight)
+        rec = {}
+        for k, st_ in starts.items():
+            if st_ is None:
+                rec[k] = (ci.iterations, 0.0, 0.0)
+                continue
+            x0 = np.clip(st_[0], fam.base.collo, fam.base.colup)
+            _, _, wi = eng.solve(p, x_init=x0, y_init=st_[1], omega_init=st_[2])
+            rec[k] = (wi.iterations, float(np.linalg.norm(x0 - xs) / max(np.linalg.norm(xs), 1e-300)),
+                      float(np.linalg.norm(st_[1] - ys) / max(np.linalg.norm(ys), 1e-300)))
+        rows_.append(rec)
+    for k in rows_[0] if rows_ else []:
+        sens["iterations"][k] = float(np.mean([r[k][0] for r in rows_]))
+        sens["rel_dist_x"][k] = float(np.mean([r[k][1] for r in rows_]))
+        sens["rel_dist_y"][k] = float(np.mean([r[k][2] for r in rows_]))
     eng.close()
     model.close()
     warm_s = summ["warm_seconds_mean"]
@@ -557,6 +592,7 @@ def learned_figures(n_train, n_test, n_pdhg, pdhg_iters, epochs):
                     "row_loss_first_last": [float(fit["row_loss"][0]), float(fit["row_loss"][-1])],
                     "col_samples": fit["col_samples"], "row_samples": fit["row_samples"],
                     "train_solutions_optimal": int((train.status == pdhg.OPTIMAL).sum())},
+        "warm_start_sensitivity": sens,
         "note": None if pdhg_reached else "plain PDHG hit its iteration cap on some instances: its time is a lower bound",
         "train_step_us": us_step, "train_step_flops": flops_step,
     }

@@ -2132,7 +2132,8 @@ namespace {
 // Steady-state timing of the fused iteration kernels of one precision on
 // the handle's current state: `reps` back-to-back launches of k_primal
 // alone, of k_dual alone, and of reps (k_primal, k_dual) pairs, each batch
-// bracketed by CUDA events on the handle's stream.  The kernels run against
+// captured in a CUDA graph as the solve's chunks are, and its launch
+// bracketed by CUDA events on the handle's stream (a warm-up launch first).  The kernels run against
 // a copy of the solver state marked running, on the layout and scaled
 // values of the last solve; they overwrite the iterates, which a finished
 // solve no longer needs (its result is in out_x / out_y).
@@ -2167,18 +2168,36 @@ void time_iteration_l(nir_pdhg* h, int reps, double* primal_us, double* dual_us,
     NIR_CUDA(cudaEventCreate(&a));
     NIR_CUDA(cudaEventCreate(&b));
     auto timed = [&](int which) {
-        for (int w = 0; w < 2; ++w) {  // the first batch warms up
-            NIR_CUDA(cudaEventRecord(a, s));
-            for (int r = 0; r < reps; ++r) {
-                if (which != 1) primal();
-                if (which != 0) dual();
-            }
-            NIR_LAUNCHED();
-            NIR_CUDA(cudaEventRecord(b, s));
-            NIR_CUDA(cudaEventSynchronize(b));
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t ge = nullptr;
+        NIR_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        for (int r = 0; r < reps; ++r) {
+            if (which != 1) primal();
+            if (which != 0) dual();
+        }
+        const cudaError_t launched = cudaGetLastError();
+        const cudaError_t ended = cudaStreamEndCapture(s, &g);
+        if (launched != cudaSuccess || ended != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            NIR_CUDA(launched != cudaSuccess ? launched : ended);
         }
         float ms = 0.0f;
-        NIR_CUDA(cudaEventElapsedTime(&ms, a, b));
+        try {
+            NIR_CUDA(cudaGraphInstantiate(&ge, g, 0));
+            for (int w = 0; w < 2; ++w) {  // the first launch warms up
+                NIR_CUDA(cudaEventRecord(a, s));
+                NIR_CUDA(cudaGraphLaunch(ge, s));
+                NIR_CUDA(cudaEventRecord(b, s));
+                NIR_CUDA(cudaEventSynchronize(b));
+            }
+            NIR_CUDA(cudaEventElapsedTime(&ms, a, b));
+        } catch (...) {
+            if (ge) cudaGraphExecDestroy(ge);
+            cudaGraphDestroy(g);
+            throw;
+        }
+        cudaGraphExecDestroy(ge);
+        cudaGraphDestroy(g);
         return 1000.0 * ms / reps;
     };
     *primal_us = timed(0);

@@ -599,12 +599,14 @@ __device__ void control_update(const CtlArgs& a, DevState* st, const CtlSums& su
             st->stall += 1;
         }
         // a plateau counts as a stall only once it has lasted polish_stall
-        // checks and half of the checks so far: PDLP's own plateaus grow
-        // with its restart lengths (an artificial restart at 0.36 of the
-        // iterations so far), and a hand-over inside one of them only
-        // slows the solve down
+        // checks and half of the checks so far, and only within a factor
+        // 100 of the tolerance: PDLP's own plateaus grow with its restart
+        // lengths (an artificial restart at 0.36 of the iterations so far)
+        // and sit at any KKT level, while the rounding of the FP32 matrix
+        // values (2^-24 relative) shows only near the tolerance; a
+        // hand-over earlier only slows the solve down
         const long long window = max((long long)a.polish_stall, (it / max(a.K, 1)) / 2);
-        if (st->stall >= window || kkt <= a.polish_switch) {
+        if ((st->stall >= window && kkt <= 100.0 * a.tol) || kkt <= a.polish_switch) {
             st->switch_request = 1;
             st->phase = 1;
             return;
