@@ -333,9 +333,10 @@ def spmv_figures(eng, lp, lay=None, reps=20):
         rows = []
         for cap in warp_caps:
             rows += [("warp_f32", pdhg.K_WARP32, 4, 4, cap), ("warp_f64", pdhg.K_WARP64, 8, 8, cap)]
-        rows += [("cta_f32", pdhg.K_CTA32, 4, 4, 1024), ("cta_f32val_f64x", pdhg.K_CTA_MIXED, 4, 8, 1024),
-                 ("cta_f64", pdhg.K_CTA64, 8, 8, 1024),
-                 ("ceiling_gather_f32", pdhg.K_CEIL_GATHER32, 4, 4, 0),
+        for cap in ((1024,) if lay is not None else (1024, 2048)):
+            rows += [("cta_f32", pdhg.K_CTA32, 4, 4, cap), ("cta_f32val_f64x", pdhg.K_CTA_MIXED, 4, 8, cap),
+                     ("cta_f64", pdhg.K_CTA64, 8, 8, cap)]
+        rows += [("ceiling_gather_f32", pdhg.K_CEIL_GATHER32, 4, 4, 0),
                  ("ceiling_gather_f64", pdhg.K_CEIL_GATHER64, 8, 8, 0),
                  ("ceiling_stream_f64", pdhg.K_CEIL_STREAM64, 8, 8, 0)]
         for kname, kind, vw, xw, cap in rows:
@@ -671,6 +672,21 @@ def run_blocks(args, local):
             b.record()
             torch.cuda.synchronize()
             times.append(a.elapsed_time(b) / 1000.0)
+        # the same batch with each chunk's non-check iterations in one
+        # cooperative persistent launch (grid barriers between half-iterations)
+        pp_ = pdhg.default_params(tol=1e-6, max_iters=args.max_iters, persistent=1)
+        eng.solve(pp_)
+        ptimes = []
+        for _ in range(2):
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            pres, _ = eng.solve(pp_)
+            b.record()
+            torch.cuda.synchronize()
+            ptimes.append(a.elapsed_time(b) / 1000.0)
     st = [r[2].status for r in res]
     its = [r[2].iterations for r in res]
     alg = sum(r[2].iterations * (12.0 * lp.nnz + 8 * 9 * lp.ncol + 8 * 8 * lp.nrow) for lp, r in zip(lps, res))
@@ -681,6 +697,10 @@ def run_blocks(args, local):
                     "iterations_max": int(max(its)), "iterations_median": float(np.median(its)),
                     "rel_kkt_max": float(max(r[2].rel_kkt for r in res)),
                     "loop_algorithmic_GBs": alg / tts / 1e9,
+                    "persistent_time_to_tol_s": float(np.mean(ptimes)),
+                    "persistent_same_iterations": [r[2].iterations for r in pres] == its,
+                    "launch_mode": "graph-launched kernels per half-iteration (the default); "
+                                   "persistent_time_to_tol_s: the cooperative persistent chunk kernel",
                     "note": "algorithmic bytes of the iterations each instance ran, counted at FP32 values with "
                             "FP64 vectors, over the device time of the whole solve"}
     # the batch matrix as one block-diagonal LP: cold plain SpMV GB/s
@@ -1245,7 +1265,8 @@ def run_arm(args, wl, rank, world, local):
         dom_name, dom = "none", {"achieved_GBs": None, "algorithmic_bytes_per_launch": None, "launch_us": None}
     achieved = dom["achieved_GBs"]
     wl = WORKLOADS[args.workload]
-    traffic = committed_traffic(f"{dom_name}:{wl['label']}")
+    dom_family = "cta" if (r["lay"].block_nnz_at if "primal" in dom_name else r["lay"].block_nnz) > 256 else "warp"
+    traffic = committed_traffic(f"{dom_name}[{dom_family}]:{wl['label']}")
     cpu = cpu_baseline(lp, wl["label"], seconds=args.cpu_seconds)
     fp64 = r["fp64"]
     if cpu and fp64 and fp64["iterations"]:
@@ -1290,7 +1311,9 @@ def run_arm(args, wl, rank, world, local):
         "gpu_launches": r["launches"],
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                     "kernel": f"{dom_name} (fused CTA-block SpMV + update), dominant by time in the solve",
+                     "kernel": f"{dom_name} (fused SpMV + update over "
+                               f"{'CTA blocks' if dom_family == 'cta' else 'warp row blocks'}), "
+                               "dominant by time in the solve",
                      "algorithmic_bytes_per_launch": dom["algorithmic_bytes_per_launch"],
                      "launch_us": dom["launch_us"],
                      "timing": "steady state: 100 back-to-back launches on the solved state, CUDA events on "
