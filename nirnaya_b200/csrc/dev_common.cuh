@@ -56,6 +56,7 @@ struct DevState {
     int ref_stopped;
     int pad_;
     long long probe_hit;   // reference loop: first probed iteration with rel KKT <= tol (-1: none yet)
+    double bnorm, cnorm;   // ||b||, ||c|| of the original LP: the relative KKT's denominators
 };
 
 // Deterministic block-wide sum / max over kBlock threads: a fixed shuffle

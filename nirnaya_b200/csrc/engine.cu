@@ -184,6 +184,17 @@ struct nir_pdhg {
     std::vector<double> h_c, h_l, h_u, h_rl, h_ru;
     // scaling and scaled vectors
     double *dr = nullptr, *dc = nullptr;
+    // what dr, dc and the scaled matrix copies hold: they depend on the
+    // matrix and the scaling parameters only, so solves that change only
+    // the vectors (nir_pdhg_update_vectors) reuse them and ||A||_2
+    struct ScaleState {
+        bool valid = false;
+        bool enabled = false;
+        int ruiz = -1, pc = -1;
+        bool norm_valid = false;
+        int power_iters = -1;
+        double norm = 0.0;
+    } scaled;
     double *c64 = nullptr, *l64 = nullptr, *u64 = nullptr, *rl64 = nullptr, *ru64 = nullptr;
     float *c32 = nullptr, *l32 = nullptr, *u32 = nullptr, *rl32 = nullptr, *ru32 = nullptr;
     // iterates
@@ -871,8 +882,6 @@ void launch_fast_chunk_l(nir_pdhg* h, const SolveCfg& cfg, int phase, ChunkTimer
     ca.nD = gd1;
     ca.nKR = gkr;
     ca.nKC = gkc;
-    ca.bnorm = cfg.bnorm;
-    ca.cnorm = cfg.cnorm;
     ca.offset = h->offset;
     ca.tol = cfg.p.tol;
     ca.feas_tol = cfg.p.feas_tol;
@@ -944,7 +953,7 @@ struct KeyHash {
 // 2 = FP64 values and iterates.
 unsigned long long chunk_key(const nir_pdhg* h, const SolveCfg& c, int phase, int prec) {
     KeyHash k;
-    k.add(phase).add(prec).add(c.K).add(c.halpern).add(c.restarts).add(c.mixed).add(c.bnorm).add(c.cnorm);
+    k.add(phase).add(prec).add(c.K).add(c.halpern).add(c.restarts).add(c.mixed);
     k.add(c.p.reflection).add(c.p.restart_sufficient).add(c.p.restart_necessary).add(c.p.restart_artificial);
     k.add(c.p.primal_weight_smoothing).add(c.p.polish_stall_checks).add(c.p.polish_switch_kkt).add(c.p.tol);
     k.add(c.p.feas_tol).add(c.p.restart_anchor).add(c.p.primal_weight_decades).add(c.p.polish_fresh).add(h->offset).add(h->part).add(h->hist);
@@ -1214,6 +1223,17 @@ int solve_reference(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), v
 void precondition(nir_pdhg* h, const nir_pdhg_params& p, bool enable) {
     cudaStream_t s = h->stream;
     const int n = h->n, m = h->m;
+    auto& sc = h->scaled;
+    if (sc.valid && sc.enabled == enable && (!enable || (sc.ruiz == p.ruiz_iters && sc.pc == p.pock_chambolle))) {
+        // the matrix scaling of the last solve holds: scale the vectors only
+        nir::k_scale_vectors<<<std::max(grid_for(std::max(n, m)), 1u), nir::kBlock, 0, s>>>(
+            n, m, h->c, h->l, h->u, h->rl, h->ru, h->dc, h->dr, h->c64, h->l64, h->u64, h->rl64, h->ru64, h->c32,
+            h->l32, h->u32, h->rl32, h->ru32);
+        NIR_LAUNCHED();
+        h->launches += 1;
+        return;
+    }
+    sc = nir_pdhg::ScaleState{};
     nir::k_fill<<<grid_for(m), nir::kBlock, 0, s>>>(m, 1.0, h->dr);
     nir::k_fill<<<grid_for(n), nir::kBlock, 0, s>>>(n, 1.0, h->dc);
     NIR_LAUNCHED();
@@ -1244,10 +1264,17 @@ void precondition(nir_pdhg* h, const nir_pdhg_params& p, bool enable) {
         h->u32, h->rl32, h->ru32);
     NIR_LAUNCHED();
     h->launches += 7;
+    sc.valid = true;
+    sc.enabled = enable;
+    sc.ruiz = p.ruiz_iters;
+    sc.pc = p.pock_chambolle;
 }
 
-// ||A_scaled||_2 by power iteration on A'A (FP64, deterministic).
+// ||A_scaled||_2 by power iteration on A'A (FP64, deterministic), kept
+// with the scaling it was computed for.
 double power_norm(nir_pdhg* h, int rounds) {
+    auto& sc = h->scaled;
+    if (sc.valid && sc.norm_valid && sc.power_iters == rounds) return sc.norm;
     cudaStream_t s = h->stream;
     const int n = h->n, m = h->m;
     const PartLayout L = part_layout(h);
@@ -1269,7 +1296,13 @@ double power_norm(nir_pdhg* h, int rounds) {
     nir::DevState st;
     NIR_CUDA(cudaMemcpyAsync(&st, h->st, sizeof(st), cudaMemcpyDeviceToHost, s));
     NIR_CUDA(cudaStreamSynchronize(s));
-    return std::sqrt(st.ref_norm_est);  // ||A'A u|| ~ sigma_max^2 for unit u
+    const double norm = std::sqrt(st.ref_norm_est);  // ||A'A u|| ~ sigma_max^2 for unit u
+    if (sc.valid) {
+        sc.norm_valid = true;
+        sc.power_iters = rounds;
+        sc.norm = norm;
+    }
+    return norm;
 }
 
 double norm2(const std::vector<double>& v) {
@@ -1464,6 +1497,8 @@ int solve_fast(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), void* 
     nir::DevState st0{};
     st0.max_iters = p.max_iters;
     st0.best_kkt = INFINITY;
+    st0.bnorm = cfg.bnorm;
+    st0.cnorm = cfg.cnorm;
     double eta, omega;
     if (pdlp) {
         const double sig = power_norm(h, std::max(1, p.power_iters));

@@ -500,7 +500,7 @@ struct CtlArgs {
     const double* partKR;  // KKT row partials, 4 x nKR
     const double* partKC;  // KKT column partials, 4 x nKC
     int nP, nD, nKR, nKC;  // grids of the kernels that wrote them
-    double bnorm, cnorm, offset;
+    double offset;
     double tol, feas_tol;
     int K;
     int restarts_on;       // PDLP
@@ -677,7 +677,7 @@ __global__ void __launch_bounds__(kBlock) k_control(CtlArgs a, DevState* st) {
     const double xviol2 = block_sum_array(a.partKC + 3 * a.nKC, a.nKC, sh);
     if (threadIdx.x != 0) return;
     const CtlSums sums{dx2, dxa2, dy2, dya2, pres2, dobj_r, ywrong2, maxrel, dres2, dobj_c, pobj_c, xviol2};
-    control_update(a, st, sums, a.bnorm, a.cnorm, a.offset, a.hist);
+    control_update(a, st, sums, st->bnorm, st->cnorm, a.offset, a.hist);
 }
 
 // KKT probe of the reference loop (after a chunk's KKT kernels): records

@@ -275,6 +275,8 @@ class Evaluation:
             "warm_iterations_mean": float(self.warm_iterations.mean()),
             "cold_seconds_mean": float(self.cold_seconds.mean()),
             "warm_seconds_mean": float(used_s.mean() + self.predict_seconds / len(acc)),
+            "warm_solve_seconds_mean": float(self.warm_seconds.mean()),
+            "predict_seconds_mean": float(self.predict_seconds / len(acc)),
             "iteration_ratio": float(self.cold_iterations.mean() / max(self.warm_iterations.mean(), 1.0)),
             "time_ratio": float(self.cold_seconds.mean() / (used_s.mean() + self.predict_seconds / len(acc))),
             "max_rel_objective_gap": float(np.max(np.abs(self.warm_objective - self.cold_objective)
