@@ -149,11 +149,19 @@ class WarmStart:
         dem = b.row_index < fam.nd
         self.dem_w = np.bincount(self.cols[dem], weights=b.value[dem], minlength=fam.n)  # sum of demand coefficients
         self.row_abs = np.bincount(b.row_index, weights=np.abs(b.value), minlength=fam.m)
+        # the two per-instance aggregations of the features as fixed sparse
+        # operators (built once): demand perturbation per column and cost
+        # perturbation per row
+        import scipy.sparse as sp
+
+        self._dem_t = sp.csr_matrix((b.value[dem], (self.cols[dem], b.row_index[dem])), shape=(fam.n, fam.nd))
+        self._abs_a = sp.csr_matrix((np.abs(b.value), (b.row_index, self.cols)), shape=(fam.m, fam.n))
         self.fitted = False
 
     # ---- statistics of the training solutions
     def _stats(self, sol: Solutions):
         fam = self.fam
+        self._colF = self._rowF = None
         ok = sol.status == P.OPTIMAL
         X = sol.x[ok].astype(np.float64)
         Y = sol.y[ok].astype(np.float64)
@@ -173,43 +181,56 @@ class WarmStart:
         self.log_omega = float(np.mean(np.log(np.maximum(sol.omega[ok], 1e-30))))
 
     # ---- features of one instance
+    def _col_base(self) -> np.ndarray:
+        """The instance-independent column features (built once per fit)."""
+        if getattr(self, "_colF", None) is None:
+            fam = self.fam
+            F = np.zeros((fam.n, COL_FEATURES), np.float32)
+            F[:, 3] = self.xbar / self.u
+            F[:, 4] = self.p_up
+            F[:, 5] = self.p_zero
+            F[:, 7] = self.u / 10.0
+            F[:, 8] = fam.cost0 / self.cscale
+            F[:, 9] = 1.0
+            self._colF = F
+        return self._colF
+
+    def _row_base(self) -> np.ndarray:
+        """The instance-independent row features (built once per fit)."""
+        if getattr(self, "_rowF", None) is None:
+            fam = self.fam
+            F = np.zeros((fam.m, ROW_FEATURES), np.float32)
+            F[: fam.nd, 0] = 1.0
+            F[:, 2] = self.ybar / self.ysd
+            F[:, 3] = self.p_tight
+            F[:, 7] = 1.0
+            self._rowF = F
+        return self._rowF
+
     def col_features(self, f, g) -> np.ndarray:
-        fam, b = self.fam, self.fam.base
+        fam = self.fam
         c = fam.cost0 * g
-        F = np.zeros((fam.n, COL_FEATURES), np.float32)
-        dem = b.row_index < fam.nd
-        fd = np.zeros(fam.m)
-        fd[: fam.nd] = f - 1.0
-        dpert = np.bincount(self.cols[dem], weights=b.value[dem] * fd[b.row_index[dem]], minlength=fam.n)
+        F = self._col_base().copy()
+        dpert = self._dem_t @ (f - 1.0)
         F[:, 0] = (g - 1.0) / 0.1
         F[:, 1] = c / self.cscale
         F[:, 2] = (c - self.atybar) / self.cscale
-        F[:, 3] = self.xbar / self.u
-        F[:, 4] = self.p_up
-        F[:, 5] = self.p_zero
         F[:, 6] = dpert / np.maximum(self.dem_w, 1e-12) / 0.2
-        F[:, 7] = self.u / 10.0
-        F[:, 8] = fam.cost0 / self.cscale
-        F[:, 9] = 1.0
         return F
 
     def row_features(self, f, g) -> np.ndarray:
         fam, b = self.fam, self.fam.base
-        F = np.zeros((fam.m, ROW_FEATURES), np.float32)
+        F = self._row_base().copy()
         nd = fam.nd
         rowlo = fam.rowlo0.copy()
         rowlo[:nd] *= f
-        gpert = np.bincount(b.row_index, weights=np.abs(b.value) * (g - 1.0)[self.cols], minlength=fam.m)
-        F[:nd, 0] = 1.0
+        gpert = self._abs_a @ (g - 1.0)
         F[:nd, 1] = (f - 1.0) / 0.2
-        F[:, 2] = self.ybar / self.ysd
-        F[:, 3] = self.p_tight
         slack_lo = np.where(np.isfinite(rowlo), self.axbar - rowlo, 0.0)
         slack_up = np.where(np.isfinite(b.rowup), b.rowup - self.axbar, 0.0)
         F[:, 4] = slack_lo / self.bscale
         F[:, 5] = slack_up / self.bscale
         F[:, 6] = gpert / np.maximum(self.row_abs, 1e-12) / 0.1
-        F[:, 7] = 1.0
         return F
 
     def fit(self, sol: Solutions, epochs=20, batch=1024, cols_per_instance=4096, rows_per_instance=2048,
