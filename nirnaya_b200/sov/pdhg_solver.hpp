@@ -26,6 +26,9 @@
 //     undone exactly before the engine runs and the solution is mapped
 //     back: the engine preconditions by itself, and power-of-two
 //     equilibration ahead of it slows the restarted PDHG's duality gap;
+//   * when only that row margin is missing at the cap, the solve goes on
+//     once in FP64 on the GPU from the point it reached (the retry that
+//     Solver's presolve-less fallback would otherwise make from scratch);
 //   * optionally, a crossover turns the engine's point into a vertex: a
 //     basis is read off the point and the program's own simplex
 //     (sov::LpSolver) is warm-started from it (nir::dropin::crossover
@@ -33,7 +36,8 @@
 // Environment knobs (no Options field is added, so options.hpp stays as
 // it is): NIR_PDHG_ALGO = pdlp | pdhg | reference, NIR_PDHG_PRECISION =
 // mixed | fp64 | fp32, NIR_PDHG_TOL, NIR_PDHG_MAX_ITERS, NIR_PDHG_DEVICE,
-// NIR_PDHG_KEEP_SCALING=1 (solve the scaled model as given),
+// NIR_PDHG_KEEP_SCALING=1 (solve the scaled model as given), NIR_PDHG_RETRY=0
+// (no FP64 retry on the GPU when only the row margin is missing at the cap),
 // NIR_PDHG_CROSSOVER = 1 (after every solve) | auto (when the engine stops
 // short of Optimal), NIR_PDHG_CROSSOVER_TOL (relative distance at which a
 // value sits at its bound, default 1e-6), NIR_PDHG_CROSSOVER_METHOD =
@@ -239,10 +243,40 @@ public:
         res.y.assign(model.nrow, 0.0);
         nir_pdhg_info info;
         const int device = env_int("NIR_PDHG_DEVICE", 0);
-        const int st = nir_pdhg_solve_lp(&lp, device, &p, &poll_deadline, const_cast<Deadline*>(&deadline),
-                                         res.x.data(), res.y.data(), &info);
+        int st = nir_pdhg_solve_lp(&lp, device, &p, &poll_deadline, const_cast<Deadline*>(&deadline), res.x.data(),
+                                   res.y.data(), &info);
         if (st == NIR_STATUS_INPUT_ERROR || st == NIR_STATUS_INTERNAL_ERROR)
             throw std::runtime_error(std::string("B200 PDHG engine: ") + nir_pdhg_last_error());
+        // The FP64 retry on the GPU.  When the solve met the relative KKT but
+        // not the row margin at its cap (the case in which Solver's dd check
+        // can fail and its fallback re-runs everything presolve-less,
+        // include/sov/solver.hpp:283-296), it goes on once in FP64 from the
+        // point it reached, with its primal weight and a second cap.  The
+        // retry's point replaces the first only if it meets the KKT
+        // tolerance.  NIR_PDHG_RETRY=0 turns it off.
+        if (st == NIR_STATUS_ITERATION_LIMIT && p.feas_tol > 0.0 && info.rel_kkt <= p.tol &&
+            p.algorithm != NIR_ALGO_REFERENCE && env_int("NIR_PDHG_RETRY", 1) != 0 && !deadline.expired()) {
+            nir_pdhg_params q = p;
+            q.precision = NIR_PREC_FP64;
+            const std::vector<double> x0 = res.x, y0 = res.y;
+            q.x_init = x0.data();
+            q.y_init = y0.data();
+            q.omega_init = info.primal_weight;
+            nir_pdhg_info info2;
+            const int st2 = nir_pdhg_solve_lp(&lp, device, &q, &poll_deadline, const_cast<Deadline*>(&deadline),
+                                              res.x.data(), res.y.data(), &info2);
+            if (st2 == NIR_STATUS_INPUT_ERROR || st2 == NIR_STATUS_INTERNAL_ERROR)
+                throw std::runtime_error(std::string("B200 PDHG engine: ") + nir_pdhg_last_error());
+            if (st2 == NIR_STATUS_OPTIMAL || info2.rel_kkt <= p.tol) {
+                info2.iterations += info.iterations;
+                info = info2;
+                st = st2;
+            } else {
+                res.x = x0;
+                res.y = y0;
+                info.iterations += info2.iterations;
+            }
+        }
         res.status = static_cast<Status>(st);
         // The engine iterates until the relative KKT is below tol and, as a
         // margin for Solver's double-double check, every row's relative

@@ -355,6 +355,16 @@ def test_dropin_pdhg_undoes_scale_model_exactly(tmp_path):
     assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr
 
 
+def test_dropin_pdhg_retries_in_fp64_when_only_the_row_margin_is_missing(tmp_path):
+    """A solve that meets the relative KKT but not the row margin at its cap
+    goes on once in FP64 on the GPU from the point it reached (the retry
+    Solver's presolve-less fallback would otherwise make from scratch,
+    include/sov/solver.hpp:283-296); checked with a scripted stand-in for the
+    engine entry point (tests/native/pdhg_dropin_retry_harness.cpp)."""
+    r = _harness(tmp_path, "pdhg_dropin_retry_harness.cpp")
+    assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr
+
+
 def test_dropin_crossover_reaches_the_simplex_optimum(tmp_path):
     """NIR_PDHG_CROSSOVER: from an approximate optimum (the simplex's,
     perturbed by 1e-8, 1e-6 and 1e-3 relative), a real PDHG iterate (the
