@@ -35,6 +35,8 @@ struct nir_pdhg_batch {
     std::deque<Layout> layouts;
     Layout* cur = nullptr;
     nir::DevState* insts = nullptr;
+    // the running instances and their block prefixes (k_bcompact)
+    int *d_act_inst = nullptr, *d_act_off_a = nullptr, *d_act_off_at = nullptr, *d_act_n = nullptr;
     double *d_bnorm = nullptr, *d_cnorm = nullptr, *d_offset = nullptr, *d_norm = nullptr;
     ChunkGraph graphs[2];
     bool solved = false;  // h->out_x holds the points the last batch solve returned
@@ -125,7 +127,28 @@ nir::BatchArgs bargs(nir_pdhg_batch* B, bool transpose, double* part, int i, int
     nir_pdhg* h = B->h;
     const Orient& o = transpose ? h->At : h->A;
     const nir_pdhg_batch::Orient2& L = transpose ? B->cur->at : B->cur->a;
-    return nir::BatchArgs{nir::Lay{L.blk, L.nblk, L.cap, o.rp, L.ci}, L.inst, part, B->insts, i, halpern, phase, rho};
+    return nir::BatchArgs{nir::Lay{L.blk, L.nblk, L.cap, o.rp, L.ci},
+                          L.inst,
+                          part,
+                          B->insts,
+                          i,
+                          halpern,
+                          phase,
+                          rho,
+                          L.lo,
+                          B->d_act_inst,
+                          transpose ? B->d_act_off_at : B->d_act_off_a,
+                          B->d_act_n};
+}
+
+// Lists the running instances and their block prefixes for the layouts in
+// use (after the states are set, and after every check).
+void launch_bcompact(nir_pdhg_batch* B) {
+    nir_pdhg* h = B->h;
+    nir::k_bcompact<<<1, nir::kBlock, 0, h->stream>>>(B->count, B->insts, B->cur->a.lo, B->cur->at.lo, B->d_act_inst,
+                                                      B->d_act_off_a, B->d_act_off_at, B->d_act_n);
+    NIR_LAUNCHED();
+    h->launches += 1;
 }
 
 // Calls f(LP, LD) with the batch layouts of A' and A.
@@ -232,6 +255,7 @@ void launch_batch_chunk_l(nir_pdhg_batch* B, const SolveCfg& cfg, int phase) {
     nir::k_bapply_restart<TX><<<grid_for(std::max(h->n, h->m)), nir::kBlock, 0, s>>>(
         h->n, h->m, B->d_col_inst, B->d_row_inst, B->insts, phase, Vec<TX>::x(h), Vec<TX>::x0(h), Vec<TX>::xp(h),
         Vec<TX>::y(h), Vec<TX>::y0(h), Vec<TX>::yp(h));
+    launch_bcompact(B);  // the next chunk visits the blocks of the instances still running
     nir::k_bsnap<<<1, nir::kBlock, 0, s>>>(B->count, B->insts, h->snap.ring, h->snap.d_seq);
     NIR_LAUNCHED();
     h->launches += 7;
@@ -330,6 +354,10 @@ void batch_create_impl(nir_pdhg_batch* B, const nir_lp_view* lps, int count, int
     h2d(h, B->d_row_off, B->row_off.data(), (count + 1) * sizeof(int));
     h2d(h, B->d_col_off, B->col_off.data(), (count + 1) * sizeof(int));
     B->insts = h->alloc<nir::DevState>(count);
+    B->d_act_inst = h->alloc<int>(count);
+    B->d_act_off_a = h->alloc<int>(size_t(count) + 1);
+    B->d_act_off_at = h->alloc<int>(size_t(count) + 1);
+    B->d_act_n = h->alloc<int>(1);
     B->d_bnorm = h->alloc<double>(count);
     B->d_cnorm = h->alloc<double>(count);
     B->d_offset = h->alloc<double>(count);
@@ -433,6 +461,7 @@ int batch_solve_impl(nir_pdhg_batch* B, const nir_pdhg_params& p, int (*poll)(vo
         bn[i] = std::sqrt(bo.hi + bo.lo);
     }
     h2d(h, B->insts, st0.data(), I * sizeof(nir::DevState));
+    launch_bcompact(B);
     h2d(h, B->d_bnorm, bn.data(), I * sizeof(double));
     h2d(h, B->d_cnorm, cn.data(), I * sizeof(double));
     h2d(h, B->d_offset, B->offsets.data(), I * sizeof(double));

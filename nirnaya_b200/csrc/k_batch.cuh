@@ -27,9 +27,84 @@ struct BatchArgs {
     int halpern;
     int phase;
     double rho;
+    // the blocks the kernels visit: those of the instances still running,
+    // listed by k_bcompact after every check (blocks of instance i are
+    // [blk_lo[i], blk_lo[i+1]) in this orientation)
+    const int* blk_lo;
+    const int* act_inst;  // running instances, ascending
+    const int* act_off;   // their first visited block in this orientation's list (act_n + 1 entries)
+    const int* act_n;
 };
 
 __device__ __forceinline__ bool inst_active(const DevState& s, int phase) { return !s.done && s.phase == phase; }
+
+// Block of the v-th visited position (v < act_off[nact]) and its instance:
+// the running instance whose range holds v (binary search over the running
+// instances), then the offset within its blocks.
+__device__ __forceinline__ int visited_block(const BatchArgs& a, int v, int nact, int& inst) {
+    int lo = 0, hi = nact - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(a.act_off + mid) <= v) lo = mid;
+        else hi = mid - 1;
+    }
+    inst = __ldg(a.act_inst + lo);
+    return __ldg(a.blk_lo + inst) + (v - __ldg(a.act_off + lo));
+}
+
+// Lists the running instances (not done, in either phase) and the prefix of
+// their block counts in both orientations.  One CTA; a fixed scan order.
+__global__ void __launch_bounds__(kBlock) k_bcompact(int count, const DevState* __restrict__ insts,
+                                                     const int* __restrict__ a_lo, const int* __restrict__ at_lo,
+                                                     int* __restrict__ act_inst, int* __restrict__ act_off_a,
+                                                     int* __restrict__ act_off_at, int* __restrict__ act_n) {
+    __shared__ int sh[3][kWarps];
+    __shared__ int carry[3];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (threadIdx.x == 0) carry[0] = carry[1] = carry[2] = 0;
+    __syncthreads();
+    for (int base = 0; base < count; base += kBlock) {
+        const int i = base + threadIdx.x;
+        const bool run = i < count && !insts[i].done;
+        int v[3] = {run ? 1 : 0, run ? a_lo[i + 1] - a_lo[i] : 0, run ? at_lo[i + 1] - at_lo[i] : 0};
+        int incl[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            int x = v[q];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            incl[q] = x;
+            if (lane == 31) sh[q][w] = x;
+        }
+        __syncthreads();
+        int pre[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            int before = carry[q];
+            for (int k = 0; k < w; ++k) before += sh[q][k];
+            pre[q] = before + incl[q] - v[q];
+        }
+        if (run) {
+            act_inst[pre[0]] = i;
+            act_off_a[pre[0]] = pre[1];
+            act_off_at[pre[0]] = pre[2];
+        }
+        __syncthreads();
+        if (threadIdx.x == kBlock - 1) {
+#pragma unroll
+            for (int q = 0; q < 3; ++q) carry[q] = pre[q] + v[q];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        act_off_a[carry[0]] = carry[1];
+        act_off_at[carry[0]] = carry[2];
+        *act_n = carry[0];
+    }
+}
 
 // Warp layout: reduces each per-lane quantity over the warp into the
 // block's partial slot and clears it for the next block.
@@ -69,24 +144,27 @@ __device__ __forceinline__ void lay_spmv_batch(const BatchArgs& a, const TV* __r
         TA* s_prod = reinterpret_cast<TA*>(nir_smem) + w * kWarpCapMax;
         const int2* blk = static_cast<const int2*>(L.blk);
         const int G = gridDim.x * kWarps;
-        int b = blockIdx.x * kWarps + w;
-        if (b >= L.nblk) return;
+        const int nact = __ldg(a.act_n);
+        const int total = nact > 0 ? __ldg(a.act_off + nact) : 0;
+        int pos = blockIdx.x * kWarps + w;
+        if (pos >= total) return;
+        int inst = 0;
+        int b = visited_block(a, pos, nact, inst);
         int2 d0 = __ldg(blk + b), d1 = __ldg(blk + b + 1);
-        int inst = __ldg(a.blk_inst + b);
         bool act = inst_active(a.inst[inst], a.phase);
         int c[kWarpU];
         TV v[kWarpU];
         stream_load<TV>(d0, d1, act ? L.cap : -1, L.ci, val, c, v);
         for (;;) {
-            const int bn = b + G;
-            const bool has_next = bn < L.nblk;
+            const int pn = pos + G;
+            const bool has_next = pn < total;
             int2 n0 = make_int2(0, 0), n1 = make_int2(0, 0);
-            int inst_n = 0;
+            int inst_n = 0, bn = 0;
             bool act_n = false;
             if (has_next) {
+                bn = visited_block(a, pn, nact, inst_n);
                 n0 = __ldg(blk + bn);
                 n1 = __ldg(blk + bn + 1);
-                inst_n = __ldg(a.blk_inst + bn);
                 act_n = inst_active(a.inst[inst_n], a.phase);
             }
             int cn[kWarpU];
@@ -108,14 +186,19 @@ __device__ __forceinline__ void lay_spmv_batch(const BatchArgs& a, const TV* __r
             inst = inst_n;
             act = act_n;
             b = bn;
+            pos = pn;
         }
     } else {
         __shared__ CtaShared<TA> sm[2];
         const int4* blk = static_cast<const int4*>(L.blk);
         int k = 0;
-        for (int b = blockIdx.x; b < L.nblk; b += gridDim.x) {
+        const int nact = __ldg(a.act_n);
+        const int total = nact > 0 ? __ldg(a.act_off + nact) : 0;
+        for (int pos = blockIdx.x; pos < total; pos += gridDim.x) {
+            int inst = 0;
+            const int b = visited_block(a, pos, nact, inst);
             const int4 d0 = __ldg(blk + b), d1 = __ldg(blk + b + 1);
-            const DevState& s = a.inst[d0.w];
+            const DevState& s = a.inst[inst];
             if (!inst_active(s, a.phase)) continue;
             set(epi, s);
             cta_block<TA, TV, TX, LAY, Epi, COH>(d0, d1, L.rp, L.ci, val, x, epi, sm[k & 1]);
