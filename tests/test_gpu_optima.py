@@ -111,3 +111,18 @@ def test_batch_of_multiperiod_members_matches_their_optima():
     assert total.status == pdhg.OPTIMAL
     for lp, (x, y, info), opt in zip(lps, res, opts):
         _check(lp, x, y, info, opt)
+
+
+def test_power_law_lp_at_full_size_is_confirmed_by_the_oracle():
+    # C2, the headline workload (200,000 x 500,000, 5M nonzeros): no external
+    # optimum finishes at this size, so the engine's report is checked
+    # instead: the relative KKT error it claims is the oracle's double-double
+    # one on the returned point, and its objective is the dd c'x bit for bit
+    lp = L.generate(L.ZIPF, 1)
+    with pdhg.Engine(lp) as eng:
+        x, y, info = eng.solve(pdhg.default_params(tol=TOL))
+    assert info.status == pdhg.OPTIMAL, (pdhg.STATUS_NAMES.get(info.status), info.rel_kkt)
+    k = ffi.rel_kkt(lp, x, y)
+    assert k.rel_kkt <= 1.05 * TOL, k.rel_kkt
+    assert info.rel_kkt == pytest.approx(k.rel_kkt, rel=0.05)
+    assert info.objective == ffi.eval_objective(lp, x)
