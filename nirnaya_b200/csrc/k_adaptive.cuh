@@ -137,11 +137,11 @@ __device__ __forceinline__ void warp_process(int2 d0, int2 d1, int cap, const in
     typename Epi::Pre pre{};
     if (nnzb > cap) {
         // one long row in rounds of 32*U nonzeros; the first round's stream
-        // is already in (c, v).  With 4-byte values each round's stream is
-        // requested before the previous round's gathers are consumed; with
-        // 8-byte values the extra live registers cost more occupancy than
-        // the overlap gains, so the rounds stay sequential.  Per lane the
-        // products are summed in the same order either way.
+        // is already in (c, v).  Each round's stream is requested before the
+        // previous round's gathers are consumed (with 8-byte values this
+        // takes the kernels to 128 registers, still 2 CTAs per SM, and made
+        // the C2 A x 1.3 % and the C4 A' y 3.6 % faster).  Per lane the
+        // products are summed in the same order as without the overlap.
         if (lane == 0) pre = epi.prefetch(r0);
         TA s = TA(0);
         int cc[U];
@@ -151,7 +151,6 @@ __device__ __forceinline__ void warp_process(int2 d0, int2 d1, int cap, const in
             cc[q] = c[q];
             vv[q] = v[q];
         }
-        constexpr bool kPipe = sizeof(TV) == 4;
         for (int base = p0 + lane; base < p1; base += 32 * U) {
             TX xv[U];
 #pragma unroll
@@ -159,24 +158,14 @@ __device__ __forceinline__ void warp_process(int2 d0, int2 d1, int cap, const in
             const int nb = base + 32 * U;
             int cn[U];
             TV vn[U];
-            if (kPipe) {
 #pragma unroll
-                for (int q = 0; q < U; ++q) {
-                    const int k = nb + 32 * q;
-                    cn[q] = (k < p1) ? stream_ld(ci + k) : 0;
-                    vn[q] = (k < p1) ? stream_ld(val + k) : TV(0);
-                }
+            for (int q = 0; q < U; ++q) {
+                const int k = nb + 32 * q;
+                cn[q] = (k < p1) ? stream_ld(ci + k) : 0;
+                vn[q] = (k < p1) ? stream_ld(val + k) : TV(0);
             }
 #pragma unroll
             for (int q = 0; q < U; ++q) s += TA(vv[q]) * TA(xv[q]);
-            if (!kPipe) {
-#pragma unroll
-                for (int q = 0; q < U; ++q) {
-                    const int k = nb + 32 * q;
-                    cn[q] = (k < p1) ? stream_ld(ci + k) : 0;
-                    vn[q] = (k < p1) ? stream_ld(val + k) : TV(0);
-                }
-            }
 #pragma unroll
             for (int q = 0; q < U; ++q) {
                 cc[q] = cn[q];
