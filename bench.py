@@ -173,21 +173,19 @@ def primal_bytes(lp, w, vw=None):
     unfused: the CSR SpMV of A' (n rows; vw-byte values, 4-byte indices and
     row pointers, y read once, A'y written once) plus the primal update
     (x, c, l, u, A'y read, x and x-bar written), w = 4 (FP32) or 8 (FP64)
-    the iterate width, vw the value width.  The SpMVs gather copies of the
-    iterates in the value type, so y is read and x-bar written with vw bytes
-    (FP32 values with FP64 iterates: FP32 copies)."""
+    the vector width, vw the value width (w unless the values are FP32 with
+    FP64 vectors)."""
     n, m, nnz = lp.ncol, lp.nrow, lp.nnz
     vw = w if vw is None else vw
-    return (4 + vw) * nnz + 4 * (n + 1) + vw * m + w * n + 6 * w * n + vw * n
+    return (4 + vw) * nnz + 4 * (n + 1) + w * m + w * n + 7 * w * n
 
 
 def dual_bytes(lp, w, vw=None):
-    """Same for the fused A x-bar + dual-update launch: SpMV of A (m rows,
-    x-bar gathered with vw bytes) plus the dual update (y, A x-bar, row
-    bounds read, y written; with vw < w also y's vw-byte copy written)."""
+    """Same for the fused A x-bar + dual-update launch: SpMV of A (m rows)
+    plus the dual update (y, A x-bar, row bounds read, y written)."""
     n, m, nnz = lp.ncol, lp.nrow, lp.nnz
     vw = w if vw is None else vw
-    return (4 + vw) * nnz + 4 * (m + 1) + vw * n + w * m + 5 * w * m + (vw * m if vw != w else 0)
+    return (4 + vw) * nnz + 4 * (m + 1) + w * n + w * m + 5 * w * m
 
 
 def spmv_bytes_w(lp, transpose, vword, xword):

@@ -659,18 +659,6 @@ struct Vec<double> {
     static const double* ru(nir_pdhg* h) { return h->ru64; }
 };
 
-// The copies of the iterates the SpMVs gather, in the value type TV: the
-// iterates themselves when TV == TX; with FP32 values and FP64 iterates
-// (the first phase of the mixed precision) FP32 copies, written by the
-// epilogues: x-bar only in FP32, y in FP64 and in FP32 (yg).
-template <typename TV, typename TX>
-struct Gat {
-    static TV* xb(nir_pdhg* h) { return Vec<TV>::xb(h); }
-    static TV* y(nir_pdhg* h) { return Vec<TV>::y(h); }
-    // the FP32 copy of y the dual epilogue and the restart write (or y itself)
-    static TV* yg(nir_pdhg* h) { return Vec<TV>::y(h); }
-};
-
 // The layout an orientation's iteration and KKT kernels use (o.lay) as the
 // kernels see it, and its scaled values: the CSR's own arrays for the warp
 // layout, the padded stream for the CTA layout.
@@ -840,10 +828,9 @@ void launch_fast_chunk_l(nir_pdhg* h, const SolveCfg& cfg, int phase, ChunkTimer
                                 lay_grid<LD, TX>(h, nir::k_chunk<LP, LD, TV, TX>, nba));
         nir::IterArgs ap{lt, L.P, h->st, 0, cfg.halpern, phase, cfg.p.reflection};
         nir::IterArgs ad{la, L.D, h->st, 0, cfg.halpern, phase, cfg.p.reflection};
-        nir::ChunkPtrs<TV, TX> v{valAt,           valA,           Vec<TX>::x(h),  Gat<TV, TX>::xb(h),
-                                 Vec<TX>::xp(h),  Vec<TX>::y(h),  Gat<TV, TX>::yg(h), Vec<TX>::yp(h),
-                                 Vec<TX>::c(h),   Vec<TX>::l(h),  Vec<TX>::u(h),  Vec<TX>::x0(h),
-                                 Vec<TX>::rl(h),  Vec<TX>::ru(h), Vec<TX>::y0(h)};
+        nir::ChunkPtrs<TV, TX> v{valAt,          valA,           Vec<TX>::x(h),  Vec<TX>::xb(h), Vec<TX>::xp(h),
+                                 Vec<TX>::y(h),  Vec<TX>::yp(h), Vec<TX>::c(h),  Vec<TX>::l(h),  Vec<TX>::u(h),
+                                 Vec<TX>::x0(h), Vec<TX>::rl(h), Vec<TX>::ru(h), Vec<TX>::y0(h)};
         // ~1 s of SM clock per wait; 0.1 s and one CTA too many in the test
         nir::GridSync gs{h->gs_count, h->gs_gen, h->gs_err, unsigned(gc) + (cfg.barrier_test ? 1u : 0u),
                          cfg.barrier_test ? 200000000LL : 2000000000LL};
@@ -863,22 +850,22 @@ void launch_fast_chunk_l(nir_pdhg* h, const SolveCfg& cfg, int phase, ChunkTimer
         if (timed) NIR_CUDA(cudaEventRecord(tm->e[0], s));
         if (check)
             nir::k_primal<LP, TV, TX, true><<<gp1, nir::kBlock, sp, s>>>(
-                ap, valAt, Gat<TV, TX>::y(h), Vec<TX>::x(h), Gat<TV, TX>::xb(h), Vec<TX>::xp(h), Vec<TX>::c(h),
-                Vec<TX>::l(h), Vec<TX>::u(h), Vec<TX>::x0(h));
+                ap, valAt, Vec<TX>::y(h), Vec<TX>::x(h), Vec<TX>::xb(h), Vec<TX>::xp(h), Vec<TX>::c(h), Vec<TX>::l(h),
+                Vec<TX>::u(h), Vec<TX>::x0(h));
         else
             nir::k_primal<LP, TV, TX, false><<<gp0, nir::kBlock, sp, s>>>(
-                ap, valAt, Gat<TV, TX>::y(h), Vec<TX>::x(h), Gat<TV, TX>::xb(h), Vec<TX>::xp(h), Vec<TX>::c(h),
-                Vec<TX>::l(h), Vec<TX>::u(h), Vec<TX>::x0(h));
+                ap, valAt, Vec<TX>::y(h), Vec<TX>::x(h), Vec<TX>::xb(h), Vec<TX>::xp(h), Vec<TX>::c(h), Vec<TX>::l(h),
+                Vec<TX>::u(h), Vec<TX>::x0(h));
         NIR_LAUNCHED();
         if (timed) NIR_CUDA(cudaEventRecord(tm->e[1], s));
         if (check)
-            nir::k_dual<LD, TV, TX, true><<<gd1, nir::kBlock, sd, s>>>(ad, valA, Gat<TV, TX>::xb(h), Vec<TX>::y(h),
+            nir::k_dual<LD, TV, TX, true><<<gd1, nir::kBlock, sd, s>>>(ad, valA, Vec<TX>::xb(h), Vec<TX>::y(h),
                                                                        Vec<TX>::yp(h), Vec<TX>::rl(h), Vec<TX>::ru(h),
-                                                                       Vec<TX>::y0(h), Gat<TV, TX>::yg(h));
+                                                                       Vec<TX>::y0(h));
         else
-            nir::k_dual<LD, TV, TX, false><<<gd0, nir::kBlock, sd, s>>>(ad, valA, Gat<TV, TX>::xb(h), Vec<TX>::y(h),
+            nir::k_dual<LD, TV, TX, false><<<gd0, nir::kBlock, sd, s>>>(ad, valA, Vec<TX>::xb(h), Vec<TX>::y(h),
                                                                         Vec<TX>::yp(h), Vec<TX>::rl(h), Vec<TX>::ru(h),
-                                                                        Vec<TX>::y0(h), Gat<TV, TX>::yg(h));
+                                                                        Vec<TX>::y0(h));
         NIR_LAUNCHED();
         if (timed) NIR_CUDA(cudaEventRecord(tm->e[2], s));
         h->launches += 2;
@@ -914,10 +901,9 @@ void launch_fast_chunk_l(nir_pdhg* h, const SolveCfg& cfg, int phase, ChunkTimer
     nir::k_control<<<1, nir::kBlock, 0, s>>>(ca, h->st);
     NIR_LAUNCHED();
     const int nm = std::max(h->n, h->m);
-    nir::k_apply_restart<TX, TV><<<grid_for(nm), nir::kBlock, 0, s>>>(h->n, h->m, h->st, phase, Vec<TX>::x(h),
-                                                                       Vec<TX>::x0(h), Vec<TX>::xp(h), Vec<TX>::y(h),
-                                                                       Vec<TX>::y0(h), Vec<TX>::yp(h),
-                                                                       Gat<TV, TX>::yg(h));
+    nir::k_apply_restart<TX><<<grid_for(nm), nir::kBlock, 0, s>>>(h->n, h->m, h->st, phase, Vec<TX>::x(h),
+                                                                   Vec<TX>::x0(h), Vec<TX>::xp(h), Vec<TX>::y(h),
+                                                                   Vec<TX>::y0(h), Vec<TX>::yp(h));
     NIR_LAUNCHED();
     nir::k_snap<<<1, 32, 0, s>>>(h->st, h->snap.ring, h->snap.d_seq);
     NIR_LAUNCHED();
@@ -2205,13 +2191,13 @@ void time_iteration_l(nir_pdhg* h, int reps, double* primal_us, double* dual_us,
     const TV* valA = vals_of<TV>(h->A);
     auto primal = [&]() {
         nir::k_primal<LP, TV, TX, false><<<gp, nir::kBlock, sp, s>>>(
-            ap, valAt, Gat<TV, TX>::y(h), Vec<TX>::x(h), Gat<TV, TX>::xb(h), Vec<TX>::xp(h), Vec<TX>::c(h),
-            Vec<TX>::l(h), Vec<TX>::u(h), Vec<TX>::x0(h));
+            ap, valAt, Vec<TX>::y(h), Vec<TX>::x(h), Vec<TX>::xb(h), Vec<TX>::xp(h), Vec<TX>::c(h), Vec<TX>::l(h),
+            Vec<TX>::u(h), Vec<TX>::x0(h));
     };
     auto dual = [&]() {
-        nir::k_dual<LD, TV, TX, false><<<gd, nir::kBlock, sd, s>>>(ad, valA, Gat<TV, TX>::xb(h), Vec<TX>::y(h),
+        nir::k_dual<LD, TV, TX, false><<<gd, nir::kBlock, sd, s>>>(ad, valA, Vec<TX>::xb(h), Vec<TX>::y(h),
                                                                    Vec<TX>::yp(h), Vec<TX>::rl(h), Vec<TX>::ru(h),
-                                                                   Vec<TX>::y0(h), Gat<TV, TX>::yg(h));
+                                                                   Vec<TX>::y0(h));
     };
     cudaEvent_t a, b;
     NIR_CUDA(cudaEventCreate(&a));

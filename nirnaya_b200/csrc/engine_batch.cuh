@@ -190,10 +190,9 @@ void launch_batch_chunk_l(nir_pdhg_batch* B, const SolveCfg& cfg, int phase) {
                                 lay_grid<LD, TX>(h, nir::k_bchunk<LP, LD, TV, TX>, LA.nblk));
         nir::BatchArgs ap = bargs(B, true, P, 0, cfg.halpern, phase, cfg.p.reflection);
         nir::BatchArgs ad = bargs(B, false, D, 0, cfg.halpern, phase, cfg.p.reflection);
-        nir::ChunkPtrs<TV, TX> v{bvals<TV>(LT),  bvals<TV>(LA),  Vec<TX>::x(h),      Gat<TV, TX>::xb(h),
-                                 Vec<TX>::xp(h), Vec<TX>::y(h),  Gat<TV, TX>::yg(h), Vec<TX>::yp(h),
-                                 Vec<TX>::c(h),  Vec<TX>::l(h),  Vec<TX>::u(h),      Vec<TX>::x0(h),
-                                 Vec<TX>::rl(h), Vec<TX>::ru(h), Vec<TX>::y0(h)};
+        nir::ChunkPtrs<TV, TX> v{bvals<TV>(LT),  bvals<TV>(LA),  Vec<TX>::x(h),  Vec<TX>::xb(h), Vec<TX>::xp(h),
+                                 Vec<TX>::y(h),  Vec<TX>::yp(h), Vec<TX>::c(h),  Vec<TX>::l(h),  Vec<TX>::u(h),
+                                 Vec<TX>::x0(h), Vec<TX>::rl(h), Vec<TX>::ru(h), Vec<TX>::y0(h)};
         nir::GridSync gs{h->gs_count, h->gs_gen, h->gs_err, unsigned(gc) + (cfg.barrier_test ? 1u : 0u),
                          cfg.barrier_test ? 200000000LL : 2000000000LL};
         nir::DevState* insts = B->insts;
@@ -210,21 +209,21 @@ void launch_batch_chunk_l(nir_pdhg_batch* B, const SolveCfg& cfg, int phase) {
         nir::BatchArgs ad = bargs(B, false, D, i, cfg.halpern, phase, cfg.p.reflection);
         if (check)
             nir::k_bprimal<LP, TV, TX, true><<<gp1, nir::kBlock, sp, s>>>(
-                ap, bvals<TV>(LT), Gat<TV, TX>::y(h), Vec<TX>::x(h), Gat<TV, TX>::xb(h), Vec<TX>::xp(h),
-                Vec<TX>::c(h), Vec<TX>::l(h), Vec<TX>::u(h), Vec<TX>::x0(h));
+                ap, bvals<TV>(LT), Vec<TX>::y(h), Vec<TX>::x(h), Vec<TX>::xb(h), Vec<TX>::xp(h), Vec<TX>::c(h),
+                Vec<TX>::l(h), Vec<TX>::u(h), Vec<TX>::x0(h));
         else
             nir::k_bprimal<LP, TV, TX, false><<<gp0, nir::kBlock, sp, s>>>(
-                ap, bvals<TV>(LT), Gat<TV, TX>::y(h), Vec<TX>::x(h), Gat<TV, TX>::xb(h), Vec<TX>::xp(h),
-                Vec<TX>::c(h), Vec<TX>::l(h), Vec<TX>::u(h), Vec<TX>::x0(h));
+                ap, bvals<TV>(LT), Vec<TX>::y(h), Vec<TX>::x(h), Vec<TX>::xb(h), Vec<TX>::xp(h), Vec<TX>::c(h),
+                Vec<TX>::l(h), Vec<TX>::u(h), Vec<TX>::x0(h));
         NIR_LAUNCHED();
         if (check)
-            nir::k_bdual<LD, TV, TX, true><<<gd1, nir::kBlock, sd, s>>>(
-                ad, bvals<TV>(LA), Gat<TV, TX>::xb(h), Vec<TX>::y(h), Vec<TX>::yp(h), Vec<TX>::rl(h), Vec<TX>::ru(h),
-                Vec<TX>::y0(h), Gat<TV, TX>::yg(h));
+            nir::k_bdual<LD, TV, TX, true><<<gd1, nir::kBlock, sd, s>>>(ad, bvals<TV>(LA), Vec<TX>::xb(h),
+                                                                        Vec<TX>::y(h), Vec<TX>::yp(h), Vec<TX>::rl(h),
+                                                                        Vec<TX>::ru(h), Vec<TX>::y0(h));
         else
-            nir::k_bdual<LD, TV, TX, false><<<gd0, nir::kBlock, sd, s>>>(
-                ad, bvals<TV>(LA), Gat<TV, TX>::xb(h), Vec<TX>::y(h), Vec<TX>::yp(h), Vec<TX>::rl(h), Vec<TX>::ru(h),
-                Vec<TX>::y0(h), Gat<TV, TX>::yg(h));
+            nir::k_bdual<LD, TV, TX, false><<<gd0, nir::kBlock, sd, s>>>(ad, bvals<TV>(LA), Vec<TX>::xb(h),
+                                                                         Vec<TX>::y(h), Vec<TX>::yp(h), Vec<TX>::rl(h),
+                                                                         Vec<TX>::ru(h), Vec<TX>::y0(h));
         NIR_LAUNCHED();
         h->launches += 2;
     }
@@ -253,9 +252,9 @@ void launch_batch_chunk_l(nir_pdhg_batch* B, const SolveCfg& cfg, int phase) {
     ca.hist = nullptr;
     nir::BatchCtlArgs cb{P, D, KR, KC, LT.nblk, LA.nblk, LT.lo, LA.lo, B->d_bnorm, B->d_cnorm, B->d_offset};
     nir::k_bcontrol<<<B->count, nir::kBlock, 0, s>>>(ca, cb, B->insts);
-    nir::k_bapply_restart<TX, TV><<<grid_for(std::max(h->n, h->m)), nir::kBlock, 0, s>>>(
+    nir::k_bapply_restart<TX><<<grid_for(std::max(h->n, h->m)), nir::kBlock, 0, s>>>(
         h->n, h->m, B->d_col_inst, B->d_row_inst, B->insts, phase, Vec<TX>::x(h), Vec<TX>::x0(h), Vec<TX>::xp(h),
-        Vec<TX>::y(h), Vec<TX>::y0(h), Vec<TX>::yp(h), Gat<TV, TX>::yg(h));
+        Vec<TX>::y(h), Vec<TX>::y0(h), Vec<TX>::yp(h));
     launch_bcompact(B);  // the next chunk visits the blocks of the instances still running
     nir::k_bsnap<<<1, nir::kBlock, 0, s>>>(B->count, B->insts, h->snap.ring, h->snap.d_seq);
     NIR_LAUNCHED();

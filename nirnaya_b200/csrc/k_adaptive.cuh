@@ -22,8 +22,6 @@
 // extended by the Halpern/reflection step of the restarted method.
 #pragma once
 
-#include <type_traits>
-
 #include "dev_common.cuh"
 #include "row_blocks.hpp"
 
@@ -318,11 +316,7 @@ __device__ __forceinline__ StepScalars<T> step_scalars(const DevState* st, int i
     return s;
 }
 
-// The primal step of one column.  T is the iterate type; G the type of the
-// gathered copies (x-bar, which the dual SpMV gathers): T, or FP32 in the
-// first phase of the mixed precision, whose SpMVs gather FP32 copies of
-// FP64 iterates.
-template <typename T, bool CHECK, typename G = T>
+template <typename T, bool CHECK>
 struct PrimalEpi {
     static constexpr int NQ = CHECK ? 2 : 0;
     static constexpr bool kLastIsMax = false;
@@ -331,7 +325,7 @@ struct PrimalEpi {
     };
     double q[2] = {0.0, 0.0};
     T* __restrict__ x;
-    G* __restrict__ xbar;
+    T* __restrict__ xbar;
     T* __restrict__ xplus;
     const T* __restrict__ c;
     const T* __restrict__ lo;
@@ -351,7 +345,7 @@ struct PrimalEpi {
     __device__ void row(int j, T aty, const Pre& p) {
         const T xj = p.x;
         const T xp = clamp_box(xj - s.tau * (p.c - aty), p.lo, p.up);
-        xbar[j] = G(T(2) * xp - xj);
+        xbar[j] = T(2) * xp - xj;
         T xn = xp;
         if (halpern) xn = s.w * ((T(1) + s.rho) * xp - s.rho * xj) + s.onemw * p.x0;
         x[j] = xn;
@@ -365,9 +359,7 @@ struct PrimalEpi {
     }
 };
 
-// The dual step of one row; with G != T it also writes the G copy of y
-// that the primal SpMV gathers.
-template <typename T, bool CHECK, typename G = T>
+template <typename T, bool CHECK>
 struct DualEpi {
     static constexpr int NQ = CHECK ? 2 : 0;
     static constexpr bool kLastIsMax = false;
@@ -377,7 +369,6 @@ struct DualEpi {
     double q[2] = {0.0, 0.0};
     T* __restrict__ y;
     T* __restrict__ yplus;
-    G* __restrict__ yg = nullptr;
     const T* __restrict__ rl;
     const T* __restrict__ ru;
     const T* __restrict__ y0;
@@ -398,7 +389,6 @@ struct DualEpi {
         T yn = yp;
         if (halpern) yn = s.w * ((T(1) + s.rho) * yp - s.rho * yi) + s.onemw * p.y0;
         y[i] = yn;
-        if constexpr (!std::is_same<G, T>::value) yg[i] = G(yn);
         if (CHECK) {
             yplus[i] = yp;
             const double d = double(yi) - double(yp);
@@ -709,12 +699,11 @@ __global__ void __launch_bounds__(kBlock) k_ref_probe(const double* __restrict__
     if (st->probe_hit < 0 && k.kkt <= tol) st->probe_hit = st->iter;
 }
 
-// Restart: the anchor and the iterate become (x+, y+); with G != T also the
-// G copy of y that the primal SpMV gathers.
-template <typename T, typename G = T>
+// Restart: the anchor and the iterate become (x+, y+).
+template <typename T>
 __global__ void k_apply_restart(int n, int m, const DevState* __restrict__ st, int phase, T* __restrict__ x,
                                 T* __restrict__ x0, const T* __restrict__ xplus, T* __restrict__ y,
-                                T* __restrict__ y0, const T* __restrict__ yplus, G* __restrict__ yg) {
+                                T* __restrict__ y0, const T* __restrict__ yplus) {
     if (!st->apply_restart || st->done || st->phase != phase) return;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t < n) {
@@ -726,7 +715,6 @@ __global__ void k_apply_restart(int n, int m, const DevState* __restrict__ st, i
         const T v = yplus[t];
         y[t] = v;
         y0[t] = v;
-        if constexpr (!std::is_same<G, T>::value) yg[t] = G(v);
     }
 }
 

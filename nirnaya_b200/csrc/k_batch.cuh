@@ -210,11 +210,11 @@ __device__ __forceinline__ void lay_spmv_batch(const BatchArgs& a, const TV* __r
 
 template <int LAY, typename TV, typename TX, bool CHECK>
 __global__ void __launch_bounds__(kBlock, (lay_min_blocks<LAY, TX>()))
-    k_bprimal(BatchArgs a, const TV* __restrict__ val, const TV* __restrict__ y, TX* __restrict__ x,
-              TV* __restrict__ xbar, TX* __restrict__ xplus, const TX* __restrict__ c, const TX* __restrict__ lo,
+    k_bprimal(BatchArgs a, const TV* __restrict__ val, const TX* __restrict__ y, TX* __restrict__ x,
+              TX* __restrict__ xbar, TX* __restrict__ xplus, const TX* __restrict__ c, const TX* __restrict__ lo,
               const TX* __restrict__ up, const TX* __restrict__ x0) {
     __shared__ double s_red[kWarps];
-    PrimalEpi<TX, CHECK, TV> epi;
+    PrimalEpi<TX, CHECK> epi;
     epi.x = x;
     epi.xbar = xbar;
     epi.xplus = xplus;
@@ -223,26 +223,24 @@ __global__ void __launch_bounds__(kBlock, (lay_min_blocks<LAY, TX>()))
     epi.up = up;
     epi.x0 = x0;
     epi.halpern = a.halpern;
-    lay_spmv_batch<LAY, TX, TV, TV>(a, val, y, epi, [&](PrimalEpi<TX, CHECK, TV>& e, const DevState& s) {
+    lay_spmv_batch<LAY, TX, TV, TX>(a, val, y, epi, [&](PrimalEpi<TX, CHECK>& e, const DevState& s) {
         e.s = step_scalars<TX>(&s, a.i_in_chunk, a.halpern, a.rho);
     }, s_red);
 }
 
 template <int LAY, typename TV, typename TX, bool CHECK>
 __global__ void __launch_bounds__(kBlock, (lay_min_blocks<LAY, TX>()))
-    k_bdual(BatchArgs a, const TV* __restrict__ val, const TV* __restrict__ xbar, TX* __restrict__ y,
-            TX* __restrict__ yplus, const TX* __restrict__ rl, const TX* __restrict__ ru, const TX* __restrict__ y0,
-            TV* __restrict__ yg) {
+    k_bdual(BatchArgs a, const TV* __restrict__ val, const TX* __restrict__ xbar, TX* __restrict__ y,
+            TX* __restrict__ yplus, const TX* __restrict__ rl, const TX* __restrict__ ru, const TX* __restrict__ y0) {
     __shared__ double s_red[kWarps];
-    DualEpi<TX, CHECK, TV> epi;
+    DualEpi<TX, CHECK> epi;
     epi.y = y;
     epi.yplus = yplus;
-    epi.yg = yg;
     epi.rl = rl;
     epi.ru = ru;
     epi.y0 = y0;
     epi.halpern = a.halpern;
-    lay_spmv_batch<LAY, TX, TV, TV>(a, val, xbar, epi, [&](DualEpi<TX, CHECK, TV>& e, const DevState& s) {
+    lay_spmv_batch<LAY, TX, TV, TX>(a, val, xbar, epi, [&](DualEpi<TX, CHECK>& e, const DevState& s) {
         e.s = step_scalars<TX>(&s, a.i_in_chunk, a.halpern, a.rho);
     }, s_red);
 }
@@ -325,13 +323,11 @@ __global__ void __launch_bounds__(kBlock) k_bcontrol(CtlArgs a, BatchCtlArgs b, 
     control_update(a, st, s, b.bnorm[i], b.cnorm[i], b.offset[i], nullptr);
 }
 
-// Restart of the instances whose controller asked for one; with G != T
-// also the G copy of y that the primal SpMV gathers.
-template <typename T, typename G = T>
+template <typename T>
 __global__ void k_bapply_restart(int n, int m, const int* __restrict__ col_inst, const int* __restrict__ row_inst,
                                  const DevState* __restrict__ insts, int phase, T* __restrict__ x, T* __restrict__ x0,
                                  const T* __restrict__ xplus, T* __restrict__ y, T* __restrict__ y0,
-                                 const T* __restrict__ yplus, G* __restrict__ yg) {
+                                 const T* __restrict__ yplus) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t < n) {
         const DevState& s = insts[col_inst[t]];
@@ -347,7 +343,6 @@ __global__ void k_bapply_restart(int n, int m, const int* __restrict__ col_inst,
             const T v = yplus[t];
             y[t] = v;
             y0[t] = v;
-            if constexpr (!std::is_same<G, T>::value) yg[t] = G(v);
         }
     }
 }

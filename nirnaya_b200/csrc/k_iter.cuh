@@ -70,16 +70,12 @@ struct IterArgs {
     double rho;
 };
 
-// The SpMVs gather copies of the iterates in the value type TV: the
-// iterates themselves when TV == TX, FP32 copies of FP64 iterates in the
-// first phase of the mixed precision (y for A' y, written by the dual
-// epilogue; x-bar for A x-bar, written only in TV).
 template <int LAY, typename TV, typename TX, bool CHECK, bool COH>
-__device__ __forceinline__ void primal_phase(const IterArgs& a, const TV* __restrict__ val, const TV* __restrict__ y,
-                                             TX* __restrict__ x, TV* __restrict__ xbar, TX* __restrict__ xplus,
+__device__ __forceinline__ void primal_phase(const IterArgs& a, const TV* __restrict__ val, const TX* __restrict__ y,
+                                             TX* __restrict__ x, TX* __restrict__ xbar, TX* __restrict__ xplus,
                                              const TX* __restrict__ c, const TX* __restrict__ lo,
                                              const TX* __restrict__ up, const TX* __restrict__ x0, double* s_red) {
-    PrimalEpi<TX, CHECK, TV> epi;
+    PrimalEpi<TX, CHECK> epi;
     epi.x = x;
     epi.xbar = xbar;
     epi.xplus = xplus;
@@ -89,32 +85,30 @@ __device__ __forceinline__ void primal_phase(const IterArgs& a, const TV* __rest
     epi.x0 = x0;
     epi.s = step_scalars<TX>(a.st, a.i_in_chunk, a.halpern, a.rho);
     epi.halpern = a.halpern;
-    lay_spmv<LAY, TX, TV, TV, PrimalEpi<TX, CHECK, TV>, COH>(a.lay, val, y, epi);
+    lay_spmv<LAY, TX, TV, TX, PrimalEpi<TX, CHECK>, COH>(a.lay, val, y, epi);
     if (CHECK) write_partials(epi, a.part, s_red);
 }
 
 template <int LAY, typename TV, typename TX, bool CHECK, bool COH>
-__device__ __forceinline__ void dual_phase(const IterArgs& a, const TV* __restrict__ val, const TV* __restrict__ xbar,
+__device__ __forceinline__ void dual_phase(const IterArgs& a, const TV* __restrict__ val, const TX* __restrict__ xbar,
                                            TX* __restrict__ y, TX* __restrict__ yplus, const TX* __restrict__ rl,
-                                           const TX* __restrict__ ru, const TX* __restrict__ y0, TV* __restrict__ yg,
-                                           double* s_red) {
-    DualEpi<TX, CHECK, TV> epi;
+                                           const TX* __restrict__ ru, const TX* __restrict__ y0, double* s_red) {
+    DualEpi<TX, CHECK> epi;
     epi.y = y;
     epi.yplus = yplus;
-    epi.yg = yg;
     epi.rl = rl;
     epi.ru = ru;
     epi.y0 = y0;
     epi.s = step_scalars<TX>(a.st, a.i_in_chunk, a.halpern, a.rho);
     epi.halpern = a.halpern;
-    lay_spmv<LAY, TX, TV, TV, DualEpi<TX, CHECK, TV>, COH>(a.lay, val, xbar, epi);
+    lay_spmv<LAY, TX, TV, TX, DualEpi<TX, CHECK>, COH>(a.lay, val, xbar, epi);
     if (CHECK) write_partials(epi, a.part, s_red);
 }
 
 template <int LAY, typename TV, typename TX, bool CHECK>
 __global__ void __launch_bounds__(kBlock, (lay_min_blocks<LAY, TX>()))
-    k_primal(IterArgs a, const TV* __restrict__ val, const TV* __restrict__ y, TX* __restrict__ x,
-             TV* __restrict__ xbar, TX* __restrict__ xplus, const TX* __restrict__ c, const TX* __restrict__ lo,
+    k_primal(IterArgs a, const TV* __restrict__ val, const TX* __restrict__ y, TX* __restrict__ x,
+             TX* __restrict__ xbar, TX* __restrict__ xplus, const TX* __restrict__ c, const TX* __restrict__ lo,
              const TX* __restrict__ up, const TX* __restrict__ x0) {
     __shared__ double s_red[kWarps];
     if (a.st->done || a.st->phase != a.phase) return;
@@ -123,12 +117,11 @@ __global__ void __launch_bounds__(kBlock, (lay_min_blocks<LAY, TX>()))
 
 template <int LAY, typename TV, typename TX, bool CHECK>
 __global__ void __launch_bounds__(kBlock, (lay_min_blocks<LAY, TX>()))
-    k_dual(IterArgs a, const TV* __restrict__ val, const TV* __restrict__ xbar, TX* __restrict__ y,
-           TX* __restrict__ yplus, const TX* __restrict__ rl, const TX* __restrict__ ru, const TX* __restrict__ y0,
-           TV* __restrict__ yg) {
+    k_dual(IterArgs a, const TV* __restrict__ val, const TX* __restrict__ xbar, TX* __restrict__ y,
+           TX* __restrict__ yplus, const TX* __restrict__ rl, const TX* __restrict__ ru, const TX* __restrict__ y0) {
     __shared__ double s_red[kWarps];
     if (a.st->done || a.st->phase != a.phase) return;
-    dual_phase<LAY, TV, TX, CHECK, false>(a, val, xbar, y, yplus, rl, ru, y0, yg, s_red);
+    dual_phase<LAY, TV, TX, CHECK, false>(a, val, xbar, y, yplus, rl, ru, y0, s_red);
 }
 
 // ---------------------------------------------------------------- KKT (FP64)

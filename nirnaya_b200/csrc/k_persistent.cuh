@@ -71,11 +71,7 @@ __device__ __forceinline__ bool grid_sync(const GridSync& g) {
 template <typename TV, typename TX>
 struct ChunkPtrs {
     const TV *valAt, *valA;
-    TX* x;
-    TV* xb;  // x-bar, in the gathered type
-    TX *xp, *y;
-    TV* yg;  // the gathered copy of y (y itself when TV == TX)
-    TX* yp;
+    TX *x, *xb, *xp, *y, *yp;
     const TX *c, *l, *u, *x0, *rl, *ru, *y0;
 };
 
@@ -92,9 +88,9 @@ __global__ void __launch_bounds__(kBlock, (lay_min_blocks<LP, TX>() < lay_min_bl
     for (int i = i0; i < i0 + iters; ++i) {
         ap.i_in_chunk = i;
         ad.i_in_chunk = i;
-        primal_phase<LP, TV, TX, false, true>(ap, v.valAt, v.yg, v.x, v.xb, v.xp, v.c, v.l, v.u, v.x0, s_red);
+        primal_phase<LP, TV, TX, false, true>(ap, v.valAt, v.y, v.x, v.xb, v.xp, v.c, v.l, v.u, v.x0, s_red);
         if (!grid_sync(gs)) break;
-        dual_phase<LD, TV, TX, false, true>(ad, v.valA, v.xb, v.y, v.yp, v.rl, v.ru, v.y0, v.yg, s_red);
+        dual_phase<LD, TV, TX, false, true>(ad, v.valA, v.xb, v.y, v.yp, v.rl, v.ru, v.y0, s_red);
         if (!grid_sync(gs)) break;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0 && *(volatile int*)gs.err) {
@@ -117,7 +113,7 @@ __global__ void __launch_bounds__(kBlock, (lay_min_blocks<LP, TX>() < lay_min_bl
     for (int i = i0; i < i0 + iters; ++i) {
         ap.i_in_chunk = i;
         ad.i_in_chunk = i;
-        PrimalEpi<TX, false, TV> pe;
+        PrimalEpi<TX, false> pe;
         pe.x = v.x;
         pe.xbar = v.xb;
         pe.xplus = v.xp;
@@ -126,22 +122,21 @@ __global__ void __launch_bounds__(kBlock, (lay_min_blocks<LP, TX>() < lay_min_bl
         pe.up = v.u;
         pe.x0 = v.x0;
         pe.halpern = ap.halpern;
-        lay_spmv_batch<LP, TX, TV, TV, PrimalEpi<TX, false, TV>, true>(
-            ap, v.valAt, v.yg, pe,
-            [&](PrimalEpi<TX, false, TV>& e, const DevState& s) { e.s = step_scalars<TX>(&s, ap.i_in_chunk, ap.halpern, ap.rho); },
+        lay_spmv_batch<LP, TX, TV, TX, PrimalEpi<TX, false>, true>(
+            ap, v.valAt, v.y, pe,
+            [&](PrimalEpi<TX, false>& e, const DevState& s) { e.s = step_scalars<TX>(&s, ap.i_in_chunk, ap.halpern, ap.rho); },
             s_red);
         if (!grid_sync(gs)) break;
-        DualEpi<TX, false, TV> de;
+        DualEpi<TX, false> de;
         de.y = v.y;
         de.yplus = v.yp;
-        de.yg = v.yg;
         de.rl = v.rl;
         de.ru = v.ru;
         de.y0 = v.y0;
         de.halpern = ad.halpern;
-        lay_spmv_batch<LD, TX, TV, TV, DualEpi<TX, false, TV>, true>(
+        lay_spmv_batch<LD, TX, TV, TX, DualEpi<TX, false>, true>(
             ad, v.valA, v.xb, de,
-            [&](DualEpi<TX, false, TV>& e, const DevState& s) { e.s = step_scalars<TX>(&s, ad.i_in_chunk, ad.halpern, ad.rho); },
+            [&](DualEpi<TX, false>& e, const DevState& s) { e.s = step_scalars<TX>(&s, ad.i_in_chunk, ad.halpern, ad.rho); },
             s_red);
         if (!grid_sync(gs)) break;
     }
