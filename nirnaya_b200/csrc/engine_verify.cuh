@@ -67,7 +67,7 @@ void verify_impl(nir_pdhg* h, int count, const int* d_row_off, const int* d_col_
     const unsigned grid = unsigned((threads + nir::vfy::kVfyBlock - 1) / nir::vfy::kVfyBlock);
     nir::vfy::k_vfy_rows<<<grid, nir::vfy::kVfyBlock, 0, s>>>(count, h->m, d_row_off, d_col_off, d_row_inst, h->A.rp,
                                                               h->A.ci, h->A.v_orig, d_x, h->rl, h->ru, h->c, v.offset,
-                                                              v.fb, v.rv, v.rs, v.obj);
+                                                              v.fb, h->d_row_orig, v.rv, v.rs, v.obj);
     NIR_LAUNCHED();
     nir::vfy::k_vfy_report<<<count, nir::vfy::kVfyBlock, 0, s>>>(d_row_off, d_col_off, v.rv, v.rs, v.fb, b, g, v.obj,
                                                                  v.claimed, tol, v.rep);

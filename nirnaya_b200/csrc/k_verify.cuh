@@ -319,13 +319,17 @@ __global__ void __launch_bounds__(kVfyBlock) k_vfy_cols(const int* __restrict__ 
 // sequential double-double sum).  Threads [count, count + m): row
 // t - count, its record's value and side (0 lower, 1 upper).  Rows of an
 // instance with a non-finite column are skipped (the host check stops
-// before the rows there).  row_inst null: one instance.
+// before the rows there).  row_inst null: one instance.  row_orig (null:
+// the identity) is the caller's index of each row, where its record goes:
+// a handle holds its rows in its own order, and the report's reduction
+// runs in the caller's.
 __global__ void __launch_bounds__(kVfyBlock) k_vfy_rows(
     int count, long long m, const int* __restrict__ row_off, const int* __restrict__ col_off,
     const int* __restrict__ row_inst, const int* __restrict__ rp, const int* __restrict__ ci,
     const double* __restrict__ val, const double* __restrict__ x, const double* __restrict__ rl,
     const double* __restrict__ ru, const double* __restrict__ c, const double* __restrict__ offset,
-    const long long* __restrict__ fb, double* __restrict__ rv, int8_t* __restrict__ rs, double* __restrict__ obj) {
+    const long long* __restrict__ fb, const int* __restrict__ row_orig, double* __restrict__ rv,
+    int8_t* __restrict__ rs, double* __restrict__ obj) {
     const long long t = blockIdx.x * (long long)kVfyBlock + threadIdx.x;
     if (t < count) {
         const int k = int(t);
@@ -336,14 +340,15 @@ __global__ void __launch_bounds__(kVfyBlock) k_vfy_rows(
     const long long r = t - count;
     if (r >= m) return;
     const int k = row_inst ? row_inst[r] : 0;
+    const long long ro = row_orig ? (long long)row_orig[r] : r;
     if (fb[k] < (long long)(col_off[k + 1] - col_off[k])) {
-        rv[r] = 0.0;
-        rs[r] = 0;
+        rv[ro] = 0.0;
+        rs[ro] = 0;
         return;
     }
-    const Rec R = row_check(r - row_off[k], rp[r], rp[r + 1], ci, val, x, rl[r], ru[r]);
-    rv[r] = R.v;
-    rs[r] = R.pos >= 0 ? int8_t(R.pos & 1) : int8_t(0);
+    const Rec R = row_check(ro - row_off[k], rp[r], rp[r + 1], ci, val, x, rl[r], ru[r]);
+    rv[ro] = R.v;
+    rs[ro] = R.pos >= 0 ? int8_t(R.pos & 1) : int8_t(0);
 }
 
 // One block per instance: the row record over the instance's rows, then
