@@ -416,9 +416,11 @@ void validate_lp(const nir_lp_view* lp) {
 // most often sit together, so that they stay in L1.  On the 200,000 x
 // 500,000 power-law LP this took the FP64 iteration from 74 to 59 us and
 // the solve from 11.1 to 9.4 s, with the same iterations.  Every row keeps
-// its entries and their order, so each row's and column's sums are the
-// same, and the caller sees its own order: row-indexed inputs and outputs
-// are mapped at the C ABI.  NIR_PDHG_ROW_ORDER=0 keeps the caller's order,
+// its entries and their order and every column its entries' order, so the
+// reference loop's sequential sums are the same bits (the row-block SpMVs
+// sum a row by a tree that depends on the rows sharing its block, so they
+// agree to rounding), and the caller sees its own order: row-indexed
+// inputs and outputs are mapped at the C ABI.  NIR_PDHG_ROW_ORDER=0 keeps the caller's order,
 // =1 reorders whatever the lengths.
 std::vector<int> row_order(const nir_lp_view* lp) {
     const int m = lp->nrow;
