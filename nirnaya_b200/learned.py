@@ -315,6 +315,10 @@ def evaluate(fam: BlendFamily, model: WarmStart, seeds, params: P.Params | None 
     N = len(seeds)
     ev = Evaluation(np.zeros(N, np.int64), np.zeros(N, np.int64), np.zeros(N), np.zeros(N), 0.0,
                     np.zeros(N, bool), np.zeros(N), np.zeros(N))
+    if N:
+        # one untimed prediction: the networks' first call sizes their
+        # device buffers, a one-off cost of the handle, not of an instance
+        model.predict(*fam.factors(seeds[0]))
     try:
         for i, s in enumerate(seeds):
             f, g = fam.factors(s)
