@@ -620,6 +620,7 @@ def run_learned(args, world):
                    "train_instances": args.c4_train, "test_instances": args.c4_test, "network": fig["network"],
                    "tol": 1e-6, "parallelism": "single gpu"},
         "learned": fig["learned"],
+        "warm_start_sensitivity": fig["warm_start_sensitivity"],
         "baselines": {k: fig[k] for k in ("cold_mixed_pdlp_s", "cold_fp64_pdlp_s", "plain_fp64_pdhg_s",
                                           "plain_fp64_pdhg_iterations", "plain_fp64_pdhg_reached_tol",
                                           "baseline_subset", "ratio_plain_fp64_pdhg_over_learned_warm", "note")},
