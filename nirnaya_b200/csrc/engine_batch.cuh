@@ -21,7 +21,6 @@ struct nir_pdhg_batch {
         int cap = 256;          // warp row-block capacity
         void* blk = nullptr;    // int2 (warp) or int4 with the instance in .w (CTA)
         int nblk = 0;
-        int* inst = nullptr;    // warp layout: instance of each block
         int* lo = nullptr;      // first block of each instance (count + 1)
         int* ci = nullptr;      // CTA layout: padded column indices (warp: the CSR's)
         double* v64 = nullptr;  // CTA layout: padded scaled values (warp: the CSR's)
@@ -69,8 +68,6 @@ void batch_blocks(nir_pdhg_batch* B, Orient& o, const std::vector<int>& off, int
         int2* blk = h->alloc<int2>(all.size());
         h2d(h, blk, all.data(), all.size() * sizeof(int2));
         out->blk = blk;
-        out->inst = h->alloc<int>(std::max<size_t>(owner.size(), 1));
-        if (!owner.empty()) h2d(h, out->inst, owner.data(), owner.size() * sizeof(int));
         out->ci = o.ci;
         out->v64 = o.v64;
         out->v32 = o.v32;
@@ -128,7 +125,6 @@ nir::BatchArgs bargs(nir_pdhg_batch* B, bool transpose, double* part, int i, int
     const Orient& o = transpose ? h->At : h->A;
     const nir_pdhg_batch::Orient2& L = transpose ? B->cur->at : B->cur->a;
     return nir::BatchArgs{nir::Lay{L.blk, L.nblk, L.cap, o.rp, L.ci},
-                          L.inst,
                           part,
                           B->insts,
                           i,

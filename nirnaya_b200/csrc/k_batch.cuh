@@ -5,8 +5,8 @@
 // col_off[i+1]), and its blocks (which never cross an instance) are
 // contiguous, in either layout of k_iter.cuh.  Every instance keeps its own DevState on the device:
 // step sizes, primal weight, Halpern counter, restart anchor, precision
-// phase and convergence flag.  The iteration kernels look up the instance
-// of each block, skip converged instances, and in a check launch
+// phase and convergence flag.  The iteration kernels visit the blocks of
+// the instances still running (k_bcompact), and in a check launch
 // leave one partial sum per quantity and block; the controller then runs
 // one CTA per instance, reducing that instance's block range in a fixed
 // order (deterministic) and applying the same update as the single-LP
@@ -20,7 +20,6 @@ namespace nir {
 
 struct BatchArgs {
     Lay lay;              // blocks never cross an instance
-    const int* blk_inst;  // kLayWarp: instance of each warp row block (kLayCta: the descriptor's 4th field)
     double* part;         // per-block partials: part[q * nblk + block]
     const DevState* inst;
     int i_in_chunk;
