@@ -208,7 +208,7 @@ __device__ __forceinline__ void lay_spmv_batch(const BatchArgs& a, const TV* __r
 }
 
 template <int LAY, typename TV, typename TX, bool CHECK>
-__global__ void __launch_bounds__(kBlock, (lay_min_blocks<LAY, TX>()))
+__global__ void __launch_bounds__(kBlock, (lay_min_blocks<LAY, TV, TX, true>()))
     k_bprimal(BatchArgs a, const TV* __restrict__ val, const TX* __restrict__ y, TX* __restrict__ x,
               TX* __restrict__ xbar, TX* __restrict__ xplus, const TX* __restrict__ c, const TX* __restrict__ lo,
               const TX* __restrict__ up, const TX* __restrict__ x0) {
@@ -228,7 +228,7 @@ __global__ void __launch_bounds__(kBlock, (lay_min_blocks<LAY, TX>()))
 }
 
 template <int LAY, typename TV, typename TX, bool CHECK>
-__global__ void __launch_bounds__(kBlock, (lay_min_blocks<LAY, TX>()))
+__global__ void __launch_bounds__(kBlock, (lay_min_blocks<LAY, TV, TX, true>()))
     k_bdual(BatchArgs a, const TV* __restrict__ val, const TX* __restrict__ xbar, TX* __restrict__ y,
             TX* __restrict__ yplus, const TX* __restrict__ rl, const TX* __restrict__ ru, const TX* __restrict__ y0) {
     __shared__ double s_red[kWarps];

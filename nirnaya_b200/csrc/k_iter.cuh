@@ -31,9 +31,22 @@ namespace nir {
 constexpr int kLayWarp = 0;
 constexpr int kLayCta = 4;  // CTA blocks with a run of 4 nonzeros per thread
 
-template <int LAY, typename TX>
+// Resident CTAs per SM an iteration kernel is compiled for: by the
+// accumulator width in the warp layout, by the run length in the CTA
+// layout.  BATCH: the batched kernels, whose FP32-value / FP64-iterate warp
+// kernels get one CTA more (80 instead of 110-128 registers).  Their
+// instances are medium LPs with short rows, where the extra resident warps
+// pay: the 256-instance multiperiod batch solved in 2.99 s against 3.85 s.
+// The single-LP kernels keep 2: on the power-law LP the long rows' overlapped
+// rounds need the registers, and A x was 12 % slower with 3.
+template <int LAY, typename TV, typename TX, bool BATCH = false>
 constexpr int lay_min_blocks() {
-    return LAY == kLayWarp ? iter_min_blocks<TX>() : cta_min_blocks<TX, LAY>();
+    if constexpr (LAY == kLayWarp) {
+        if constexpr (BATCH && sizeof(TV) == 4 && sizeof(TX) == 8) return iter_min_blocks<TX>() + 1;
+        return iter_min_blocks<TX>();
+    } else {
+        return cta_min_blocks<TX, LAY>();
+    }
 }
 
 // One orientation's layout as the kernels see it.
@@ -106,7 +119,7 @@ __device__ __forceinline__ void dual_phase(const IterArgs& a, const TV* __restri
 }
 
 template <int LAY, typename TV, typename TX, bool CHECK>
-__global__ void __launch_bounds__(kBlock, (lay_min_blocks<LAY, TX>()))
+__global__ void __launch_bounds__(kBlock, (lay_min_blocks<LAY, TV, TX>()))
     k_primal(IterArgs a, const TV* __restrict__ val, const TX* __restrict__ y, TX* __restrict__ x,
              TX* __restrict__ xbar, TX* __restrict__ xplus, const TX* __restrict__ c, const TX* __restrict__ lo,
              const TX* __restrict__ up, const TX* __restrict__ x0) {
@@ -116,7 +129,7 @@ __global__ void __launch_bounds__(kBlock, (lay_min_blocks<LAY, TX>()))
 }
 
 template <int LAY, typename TV, typename TX, bool CHECK>
-__global__ void __launch_bounds__(kBlock, (lay_min_blocks<LAY, TX>()))
+__global__ void __launch_bounds__(kBlock, (lay_min_blocks<LAY, TV, TX>()))
     k_dual(IterArgs a, const TV* __restrict__ val, const TX* __restrict__ xbar, TX* __restrict__ y,
            TX* __restrict__ yplus, const TX* __restrict__ rl, const TX* __restrict__ ru, const TX* __restrict__ y0) {
     __shared__ double s_red[kWarps];

@@ -79,8 +79,8 @@ struct ChunkPtrs {
 // mixes the layouts needs both kinds of shared memory; its dynamic part is
 // the warp layout's.
 template <int LP, int LD, typename TV, typename TX>
-__global__ void __launch_bounds__(kBlock, (lay_min_blocks<LP, TX>() < lay_min_blocks<LD, TX>() ? lay_min_blocks<LP, TX>()
-                                                                                                : lay_min_blocks<LD, TX>()))
+__global__ void __launch_bounds__(kBlock, (lay_min_blocks<LP, TV, TX>() < lay_min_blocks<LD, TV, TX>() ? lay_min_blocks<LP, TV, TX>()
+                                                                                                : lay_min_blocks<LD, TV, TX>()))
     k_chunk(IterArgs ap, IterArgs ad, ChunkPtrs<TV, TX> v, int i0, int iters, GridSync gs, DevState* st) {
     __shared__ double s_red[kWarps];
     // no kernel changes the state during a chunk: every CTA decides alike
@@ -105,8 +105,8 @@ __global__ void __launch_bounds__(kBlock, (lay_min_blocks<LP, TX>() < lay_min_bl
 // blocks.  On a barrier that gave up, every instance still running ends
 // with NIR_STATUS_INTERNAL_ERROR.
 template <int LP, int LD, typename TV, typename TX>
-__global__ void __launch_bounds__(kBlock, (lay_min_blocks<LP, TX>() < lay_min_blocks<LD, TX>() ? lay_min_blocks<LP, TX>()
-                                                                                                : lay_min_blocks<LD, TX>()))
+__global__ void __launch_bounds__(kBlock, (lay_min_blocks<LP, TV, TX, true>() < lay_min_blocks<LD, TV, TX, true>() ? lay_min_blocks<LP, TV, TX, true>()
+                                                                                                : lay_min_blocks<LD, TV, TX, true>()))
     k_bchunk(BatchArgs ap, BatchArgs ad, ChunkPtrs<TV, TX> v, int i0, int iters, GridSync gs, DevState* insts,
              int count) {
     __shared__ double s_red[kWarps];
