@@ -395,6 +395,8 @@ struct nir_mlp {
     int* perm = nullptr;
     int64_t adam_t = 0;
     double us_per_step = 0.0, flops_per_step = 0.0;
+    float* stage = nullptr;  // FP32 staging of uploaded rows, grown on demand
+    size_t stage_len = 0;
     std::vector<void*> allocs;
 
     template <typename T>
@@ -574,13 +576,19 @@ void ensure_losses(nir_mlp* h, int n) {
     h->losses_len = n;
 }
 
+// Host FP32 rows -> device BF16, through a staging buffer that grows on
+// demand and is kept (no allocation per call once it is large enough).
 void upload_rows(nir_mlp* h, const float* x, int rows, bf16* dst, int cols) {
-    float* tmp = h->alloc<float>((size_t)rows * cols);
-    MLP_CUDA(cudaMemcpyAsync(tmp, x, (size_t)rows * cols * sizeof(float), cudaMemcpyHostToDevice, h->stream));
-    k_to_bf16<<<grid1d((size_t)rows * cols), 256, 0, h->stream>>>((size_t)rows * cols, tmp, dst);
+    const size_t len = (size_t)rows * cols;
+    if (len > h->stage_len) {
+        if (h->stage) h->release(h->stage);
+        h->stage = h->alloc<float>(len);
+        h->stage_len = len;
+    }
+    MLP_CUDA(cudaMemcpyAsync(h->stage, x, len * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    k_to_bf16<<<grid1d(len), 256, 0, h->stream>>>(len, h->stage, dst);
     MLP_LAUNCHED();
     MLP_CUDA(cudaStreamSynchronize(h->stream));
-    h->release(tmp);
 }
 
 int fail(const std::exception& e, bool input) {
@@ -828,7 +836,9 @@ int nir_mlp_predict(nir_mlp* h, const float* x, int32_t n, float* y) {
     }
     try {
         MLP_CUDA(cudaSetDevice(h->device));
-        const int chunk = std::min(n, 16384);
+        // one chunk for a whole family member's variables (70,000 at the
+        // 20,000 x 50,000 blending size): fewer uploads and synchronisations
+        const int chunk = std::min(n, 65536);
         ensure_rows(h, chunk);
         for (int r = 0; r < n; r += chunk) {
             const int k = std::min(chunk, n - r);  // a multiple of 8
