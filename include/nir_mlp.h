@@ -74,6 +74,11 @@ int nir_mlp_train(nir_mlp* h, int32_t epochs, int32_t batch, float* epoch_loss);
 /* Forward pass of n samples (n a multiple of 8): y (n x d_out). */
 int nir_mlp_predict(nir_mlp* h, const float* x, int32_t n, float* y);
 
+/* The same forward pass from FP32 samples already on this handle's device
+ * (x_dev: n x d_in, row-major, written before the call by work that has
+ * finished, e.g. nir_blend_features_build); y on the host. */
+int nir_mlp_predict_device(nir_mlp* h, const float* x_dev, int32_t n, float* y);
+
 /* Loss and gradients of one minibatch (n a multiple of 8, at most 4096)
  * without updating the weights: grads in the flat parameter layout. */
 int nir_mlp_gradients(nir_mlp* h, const float* x, const float* targets, int32_t n, float* loss, float* grads);
@@ -96,6 +101,59 @@ int nir_mlp_gemm_time(nir_mlp* h, int32_t M, int32_t N, int32_t K, int32_t reps,
  * step (2 * batch * sum of in_l * out_l, forward plus both backward
  * products). */
 int nir_mlp_step_stats(nir_mlp* h, double* us_per_step, double* flops_per_step);
+
+/* --- the blending family's per-variable features on the device ---
+ *
+ * The inputs of the warm-start networks (nirnaya_b200/learned.py,
+ * WarmStart.col_features / row_features) built on the GPU, so that a
+ * prediction uploads only the instance's factors (nd + n doubles) instead
+ * of 16 features per variable.  Instance (f, g): demand factors f (the first
+ * nd rows' lower bounds are rowlo0 * f) and cost factors g (cost = cost0 * g).
+ * Columns j (nf features each, the template's values elsewhere):
+ *   F[j][0] = (g_j - 1) / 0.1
+ *   F[j][1] = cost0_j g_j / cscale
+ *   F[j][2] = (cost0_j g_j - atybar_j) / cscale
+ *   F[j][6] = (sum_k D[j][k] (f_k - 1)) / max(dem_w_j, 1e-12) / 0.2,
+ *             D the n x nd CSR of the columns' demand-row coefficients
+ * Rows i:
+ *   F[i][1] = (f_i - 1) / 0.2                                   (i < nd)
+ *   F[i][4] = (axbar_i - lo_i) / bscale_i if lo_i is finite, else 0,
+ *             lo_i = rowlo0_i f_i (i < nd) or rowlo0_i
+ *   F[i][5] = (rowup_i - axbar_i) / bscale_i if rowup_i is finite, else 0
+ *   F[i][6] = (sum_j |A|[i][j] (g_j - 1)) / max(row_abs_i, 1e-12) / 0.1,
+ *             |A| the m x n CSR of the absolute values of A
+ * Computed in FP64 and rounded to FP32, each sum in its CSR order.  No
+ * counterpart in the reference (it has no learned component). */
+typedef struct nir_blend_feature_data {
+    int32_t n, m, nd, nf;          /* columns, rows, demand rows (the first nd), features (>= 7) */
+    const float* col_template;     /* n x nf, row-major                                         */
+    const float* row_template;     /* m x nf                                                    */
+    const double* cost0;           /* per column                                                */
+    const double* atybar;
+    const double* dem_w;
+    double cscale;
+    const int64_t* dem_rp;         /* n + 1 */
+    const int32_t* dem_ci;         /* demand-row index of each entry (< nd)                     */
+    const double* dem_val;
+    const double* rowlo0;          /* per row (+-inf where unbounded)                           */
+    const double* rowup;
+    const double* axbar;
+    const double* bscale;
+    const double* row_abs;
+    const int64_t* abs_rp;         /* m + 1 */
+    const int32_t* abs_ci;         /* column index of each entry (< n)                          */
+    const double* abs_val;
+} nir_blend_feature_data;
+
+typedef struct nir_blend_features nir_blend_features;
+
+/* Copies the family's data to `device`.  Returns 0 or an error code. */
+int nir_blend_features_create(const nir_blend_feature_data* d, int32_t device, nir_blend_features** out);
+/* Features of instance (f: nd, g: n) into device arrays the handle owns
+ * (valid until its next call); synchronous. */
+int nir_blend_features_build(nir_blend_features* h, const double* f, const double* g, const float** col_dev,
+                             const float** row_dev);
+void nir_blend_features_free(nir_blend_features* h);
 
 #ifdef __cplusplus
 }

@@ -854,6 +854,31 @@ int nir_mlp_predict(nir_mlp* h, const float* x, int32_t n, float* y) {
     return 0;
 }
 
+int nir_mlp_predict_device(nir_mlp* h, const float* x_dev, int32_t n, float* y) {
+    if (!h || !x_dev || !y || n < 8 || n % 8 != 0) {
+        g_err = "invalid arguments (n must be a positive multiple of 8)";
+        return 2;
+    }
+    try {
+        MLP_CUDA(cudaSetDevice(h->device));
+        const int chunk = std::min(n, 65536);
+        ensure_rows(h, chunk);
+        for (int r = 0; r < n; r += chunk) {
+            const int k = std::min(chunk, n - r);
+            const size_t len = (size_t)k * h->cfg.d_in;
+            k_to_bf16<<<grid1d(len), 256, 0, h->stream>>>(len, x_dev + (size_t)r * h->cfg.d_in, h->x);
+            MLP_LAUNCHED();
+            forward(h, k);
+            MLP_CUDA(cudaMemcpyAsync(y + (size_t)r * h->cfg.d_out, h->pred, (size_t)k * h->cfg.d_out * sizeof(float),
+                                     cudaMemcpyDeviceToHost, h->stream));
+            MLP_CUDA(cudaStreamSynchronize(h->stream));
+        }
+    } catch (const std::exception& e) {
+        return fail(e, false);
+    }
+    return 0;
+}
+
 int nir_mlp_gradients(nir_mlp* h, const float* x, const float* targets, int32_t n, float* loss, float* grads) {
     if (!h || !x || !targets || n < 8 || n % 8 != 0 || n > 4096) {
         g_err = "invalid arguments (n must be a multiple of 8 in [8, 4096])";
@@ -959,5 +984,174 @@ int nir_mlp_step_stats(nir_mlp* h, double* us_per_step, double* flops_per_step) 
     if (flops_per_step) *flops_per_step = h->flops_per_step;
     return 0;
 }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- blending-family features
+
+namespace {
+
+__global__ void k_blend_cols(int n, int nf, const float* __restrict__ tmpl, const double* __restrict__ g,
+                             const double* __restrict__ f, const double* __restrict__ cost0,
+                             const double* __restrict__ atybar, const double* __restrict__ dem_w, double cscale,
+                             const long long* __restrict__ rp, const int* __restrict__ ci,
+                             const double* __restrict__ val, float* __restrict__ out) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const float* t = tmpl + (size_t)j * nf;
+    float* o = out + (size_t)j * nf;
+    for (int k = 0; k < nf; ++k) o[k] = t[k];
+    const double gj = g[j];
+    const double c = cost0[j] * gj;
+    double dp = 0.0;
+    for (long long q = rp[j]; q < rp[j + 1]; ++q) dp += val[q] * (f[ci[q]] - 1.0);
+    o[0] = float((gj - 1.0) / 0.1);
+    o[1] = float(c / cscale);
+    o[2] = float((c - atybar[j]) / cscale);
+    o[6] = float(dp / fmax(dem_w[j], 1e-12) / 0.2);
+}
+
+__global__ void k_blend_rows(int m, int nd, int nf, const float* __restrict__ tmpl, const double* __restrict__ f,
+                             const double* __restrict__ g, const double* __restrict__ rowlo0,
+                             const double* __restrict__ rowup, const double* __restrict__ axbar,
+                             const double* __restrict__ bscale, const double* __restrict__ row_abs,
+                             const long long* __restrict__ rp, const int* __restrict__ ci,
+                             const double* __restrict__ val, float* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const float* t = tmpl + (size_t)i * nf;
+    float* o = out + (size_t)i * nf;
+    for (int k = 0; k < nf; ++k) o[k] = t[k];
+    const double lo = (i < nd) ? rowlo0[i] * f[i] : rowlo0[i];
+    const double up = rowup[i];
+    double gp = 0.0;
+    for (long long q = rp[i]; q < rp[i + 1]; ++q) gp += val[q] * (g[ci[q]] - 1.0);
+    if (i < nd) o[1] = float((f[i] - 1.0) / 0.2);
+    o[4] = float((isfinite(lo) ? axbar[i] - lo : 0.0) / bscale[i]);
+    o[5] = float((isfinite(up) ? up - axbar[i] : 0.0) / bscale[i]);
+    o[6] = float(gp / fmax(row_abs[i], 1e-12) / 0.1);
+}
+
+}  // namespace
+
+struct nir_blend_features {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int n = 0, m = 0, nd = 0, nf = 0;
+    double cscale = 1.0;
+    std::vector<void*> allocs;
+    float *col_t = nullptr, *row_t = nullptr, *col_out = nullptr, *row_out = nullptr;
+    double *cost0 = nullptr, *atybar = nullptr, *dem_w = nullptr, *dem_val = nullptr;
+    double *rowlo0 = nullptr, *rowup = nullptr, *axbar = nullptr, *bscale = nullptr, *row_abs = nullptr,
+           *abs_val = nullptr;
+    long long *dem_rp = nullptr, *abs_rp = nullptr;
+    int *dem_ci = nullptr, *abs_ci = nullptr;
+    double *f = nullptr, *g = nullptr;
+
+    template <typename T>
+    T* upload(const T* src, size_t count) {
+        void* p = nullptr;
+        MLP_CUDA(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+        allocs.push_back(p);
+        if (src && count) MLP_CUDA(cudaMemcpy(p, src, count * sizeof(T), cudaMemcpyHostToDevice));
+        return static_cast<T*>(p);
+    }
+    ~nir_blend_features() {
+        cudaSetDevice(device);
+        if (stream) cudaStreamSynchronize(stream);
+        for (void* p : allocs) cudaFree(p);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+extern "C" {
+
+int nir_blend_features_create(const nir_blend_feature_data* d, int32_t device, nir_blend_features** out) {
+    if (!d || !out || d->n < 0 || d->m < 0 || d->nd < 0 || d->nd > d->m || d->nf < 7 || !d->col_template ||
+        !d->row_template || !d->cost0 || !d->atybar || !d->dem_w || !d->dem_rp || !d->rowlo0 || !d->rowup ||
+        !d->axbar || !d->bscale || !d->row_abs || !d->abs_rp) {
+        g_err = "invalid blending-feature data";
+        return 2;
+    }
+    *out = nullptr;
+    auto h = std::make_unique<nir_blend_features>();
+    try {
+        const long long dn = d->dem_rp[d->n], an = d->abs_rp[d->m];
+        if (dn < 0 || an < 0 || (dn > 0 && (!d->dem_ci || !d->dem_val)) || (an > 0 && (!d->abs_ci || !d->abs_val)))
+            throw std::invalid_argument("invalid feature operators");
+        for (long long q = 0; q < dn; ++q)
+            if (d->dem_ci[q] < 0 || d->dem_ci[q] >= d->nd) throw std::invalid_argument("demand index out of range");
+        for (long long q = 0; q < an; ++q)
+            if (d->abs_ci[q] < 0 || d->abs_ci[q] >= d->n) throw std::invalid_argument("column index out of range");
+        h->device = device;
+        MLP_CUDA(cudaSetDevice(device));
+        MLP_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+        h->n = d->n;
+        h->m = d->m;
+        h->nd = d->nd;
+        h->nf = d->nf;
+        h->cscale = d->cscale;
+        const size_t n = size_t(d->n), m = size_t(d->m), nf = size_t(d->nf);
+        h->col_t = h->upload(d->col_template, n * nf);
+        h->row_t = h->upload(d->row_template, m * nf);
+        h->col_out = h->upload<float>(nullptr, n * nf);
+        h->row_out = h->upload<float>(nullptr, m * nf);
+        h->cost0 = h->upload(d->cost0, n);
+        h->atybar = h->upload(d->atybar, n);
+        h->dem_w = h->upload(d->dem_w, n);
+        h->rowlo0 = h->upload(d->rowlo0, m);
+        h->rowup = h->upload(d->rowup, m);
+        h->axbar = h->upload(d->axbar, m);
+        h->bscale = h->upload(d->bscale, m);
+        h->row_abs = h->upload(d->row_abs, m);
+        static_assert(sizeof(long long) == sizeof(int64_t), "64-bit offsets");
+        h->dem_rp = h->upload(reinterpret_cast<const long long*>(d->dem_rp), n + 1);
+        h->dem_ci = h->upload(d->dem_ci, size_t(dn));
+        h->dem_val = h->upload(d->dem_val, size_t(dn));
+        h->abs_rp = h->upload(reinterpret_cast<const long long*>(d->abs_rp), m + 1);
+        h->abs_ci = h->upload(d->abs_ci, size_t(an));
+        h->abs_val = h->upload(d->abs_val, size_t(an));
+        h->f = h->upload<double>(nullptr, std::max<size_t>(size_t(d->nd), 1));
+        h->g = h->upload<double>(nullptr, n);
+    } catch (const std::invalid_argument& e) {
+        return fail(e, true);
+    } catch (const std::exception& e) {
+        return fail(e, false);
+    }
+    *out = h.release();
+    return 0;
+}
+
+int nir_blend_features_build(nir_blend_features* h, const double* f, const double* g, const float** col_dev,
+                             const float** row_dev) {
+    if (!h || (!f && h->nd > 0) || (!g && h->n > 0) || !col_dev || !row_dev) {
+        g_err = "invalid arguments";
+        return 2;
+    }
+    try {
+        MLP_CUDA(cudaSetDevice(h->device));
+        cudaStream_t s = h->stream;
+        if (h->nd) MLP_CUDA(cudaMemcpyAsync(h->f, f, size_t(h->nd) * sizeof(double), cudaMemcpyHostToDevice, s));
+        if (h->n) MLP_CUDA(cudaMemcpyAsync(h->g, g, size_t(h->n) * sizeof(double), cudaMemcpyHostToDevice, s));
+        if (h->n)
+            k_blend_cols<<<unsigned((h->n + 255) / 256), 256, 0, s>>>(h->n, h->nf, h->col_t, h->g, h->f, h->cost0,
+                                                                     h->atybar, h->dem_w, h->cscale, h->dem_rp,
+                                                                     h->dem_ci, h->dem_val, h->col_out);
+        if (h->m)
+            k_blend_rows<<<unsigned((h->m + 255) / 256), 256, 0, s>>>(h->m, h->nd, h->nf, h->row_t, h->f, h->g,
+                                                                     h->rowlo0, h->rowup, h->axbar, h->bscale,
+                                                                     h->row_abs, h->abs_rp, h->abs_ci, h->abs_val,
+                                                                     h->row_out);
+        MLP_LAUNCHED();
+        MLP_CUDA(cudaStreamSynchronize(s));
+        *col_dev = h->col_out;
+        *row_dev = h->row_out;
+    } catch (const std::exception& e) {
+        return fail(e, false);
+    }
+    return 0;
+}
+
+void nir_blend_features_free(nir_blend_features* h) { delete h; }
 
 }  // extern "C"

@@ -156,12 +156,17 @@ class WarmStart:
 
         self._dem_t = sp.csr_matrix((b.value[dem], (self.cols[dem], b.row_index[dem])), shape=(fam.n, fam.nd))
         self._abs_a = sp.csr_matrix((np.abs(b.value), (b.row_index, self.cols)), shape=(fam.m, fam.n))
+        self.device = device
+        self._dev = None  # the features on the device (MLP.BlendFeatures), built after a fit
         self.fitted = False
 
     # ---- statistics of the training solutions
     def _stats(self, sol: Solutions):
         fam = self.fam
         self._colF = self._rowF = None
+        if self._dev is not None:
+            self._dev.close()
+            self._dev = None
         ok = sol.status == P.OPTIMAL
         X = sol.x[ok].astype(np.float64)
         Y = sol.y[ok].astype(np.float64)
@@ -260,15 +265,45 @@ class WarmStart:
         self.fitted = True
         return {"col_loss": lc, "row_loss": lr, "col_samples": len(XC), "row_samples": len(XR)}
 
-    def predict(self, f, g):
-        """x0, y0, omega for one instance."""
-        xc = self.col_net.predict(self.col_features(f, g))[:, 0].astype(np.float64)
-        yr = self.row_net.predict(self.row_features(f, g))[:, 0].astype(np.float64)
+    def device_features(self):
+        """The feature builder on the device (the same features as
+        col_features / row_features, include/nir_mlp.h), created on first
+        use after a fit; None when the sizes are not multiples of 8 (the
+        networks take whole groups of 8 samples from the device)."""
+        fam = self.fam
+        if fam.n % 8 or fam.m % 8:
+            return None
+        if self._dev is None:
+            b = fam.base
+            dt, aa = self._dem_t, self._abs_a
+            self._dev = MLP.BlendFeatures(dict(
+                n=fam.n, m=fam.m, nd=fam.nd, nf=COL_FEATURES, col_template=self._col_base(),
+                row_template=self._row_base(), cost0=fam.cost0, atybar=self.atybar, dem_w=self.dem_w,
+                cscale=self.cscale, dem_rp=dt.indptr.astype(np.int64), dem_ci=dt.indices, dem_val=dt.data,
+                rowlo0=fam.rowlo0, rowup=b.rowup, axbar=self.axbar, bscale=self.bscale, row_abs=self.row_abs,
+                abs_rp=aa.indptr.astype(np.int64), abs_ci=aa.indices, abs_val=aa.data), self.device)
+        return self._dev
+
+    def predict(self, f, g, on_device: bool = True):
+        """x0, y0, omega for one instance: the features built on the device
+        (or, with on_device False or sizes the device path does not take,
+        on the host), then one pass of each network."""
+        dev = self.device_features() if on_device else None
+        if dev is not None:
+            col, row = dev.build(f, g)
+            xc = self.col_net.predict_device(col, self.fam.n)[:, 0].astype(np.float64)
+            yr = self.row_net.predict_device(row, self.fam.m)[:, 0].astype(np.float64)
+        else:
+            xc = self.col_net.predict(self.col_features(f, g))[:, 0].astype(np.float64)
+            yr = self.row_net.predict(self.row_features(f, g))[:, 0].astype(np.float64)
         x = np.clip(xc, 0.0, 1.0) * self.u
         y = self.ybar + self.ysd * yr
         return x, y, float(np.exp(self.log_omega))
 
     def close(self):
+        if self._dev is not None:
+            self._dev.close()
+            self._dev = None
         self.col_net.close()
         self.row_net.close()
 

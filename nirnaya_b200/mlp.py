@@ -13,14 +13,27 @@ LIB_PATH = os.path.join(_HERE, "libnir_mlp.so")
 EXPORTED = [
     "nir_mlp_create", "nir_mlp_free", "nir_mlp_last_error", "nir_mlp_param_count", "nir_mlp_get_params",
     "nir_mlp_set_params", "nir_mlp_set_output_weights", "nir_mlp_set_data", "nir_mlp_train", "nir_mlp_predict",
-    "nir_mlp_gradients", "nir_mlp_gemm_check", "nir_mlp_gemm_time", "nir_mlp_step_stats",
+    "nir_mlp_gradients", "nir_mlp_gemm_check", "nir_mlp_gemm_time", "nir_mlp_step_stats", "nir_mlp_predict_device",
 ]
+BLEND_EXPORTED = ["nir_blend_features_create", "nir_blend_features_build", "nir_blend_features_free"]
 
 
 class Config(C.Structure):
     _fields_ = [("d_in", C.c_int32), ("width", C.c_int32), ("depth", C.c_int32), ("d_out", C.c_int32),
                 ("seed", C.c_uint64), ("lr", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float),
                 ("eps", C.c_float)]
+
+
+class BlendFeatureData(C.Structure):
+    """nir_blend_feature_data (include/nir_mlp.h)."""
+    _fields_ = [("n", C.c_int32), ("m", C.c_int32), ("nd", C.c_int32), ("nf", C.c_int32),
+                ("col_template", C.POINTER(C.c_float)), ("row_template", C.POINTER(C.c_float)),
+                ("cost0", C.POINTER(C.c_double)), ("atybar", C.POINTER(C.c_double)),
+                ("dem_w", C.POINTER(C.c_double)), ("cscale", C.c_double),
+                ("dem_rp", C.POINTER(C.c_int64)), ("dem_ci", C.POINTER(C.c_int32)), ("dem_val", C.POINTER(C.c_double)),
+                ("rowlo0", C.POINTER(C.c_double)), ("rowup", C.POINTER(C.c_double)), ("axbar", C.POINTER(C.c_double)),
+                ("bscale", C.POINTER(C.c_double)), ("row_abs", C.POINTER(C.c_double)),
+                ("abs_rp", C.POINTER(C.c_int64)), ("abs_ci", C.POINTER(C.c_int32)), ("abs_val", C.POINTER(C.c_double))]
 
 
 _lib = None
@@ -51,6 +64,11 @@ def lib():
                                          C.c_int32, F]
         L.nir_mlp_step_stats.argtypes = [VP, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.nir_mlp_gemm_time.argtypes = [VP, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_double)]
+        L.nir_mlp_predict_device.argtypes = [VP, VP, C.c_int32, F]
+        L.nir_blend_features_create.argtypes = [C.POINTER(BlendFeatureData), C.c_int32, C.POINTER(VP)]
+        L.nir_blend_features_build.argtypes = [VP, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(VP),
+                                               C.POINTER(VP)]
+        L.nir_blend_features_free.argtypes = [VP]
         _lib = L
     return _lib
 
@@ -132,6 +150,13 @@ class Mlp:
         self._check(lib().nir_mlp_predict(self._h, _f(X), X.shape[0], _f(Y)), "predict")
         return Y[:n]
 
+    def predict_device(self, x_dev: int, n: int) -> np.ndarray:
+        """Forward pass of n FP32 samples already on the device (the address
+        x_dev, n x d_in row-major; n a multiple of 8)."""
+        Y = np.zeros((n, self.dims[-1]), np.float32)
+        self._check(lib().nir_mlp_predict_device(self._h, C.c_void_p(x_dev), n, _f(Y)), "predict_device")
+        return Y
+
     def gradients(self, X, T):
         X, T = _c32(X), _c32(T)
         g = np.zeros(self.param_count(), np.float32)
@@ -156,3 +181,59 @@ class Mlp:
         us, fl = C.c_double(), C.c_double()
         lib().nir_mlp_step_stats(self._h, C.byref(us), C.byref(fl))
         return us.value, fl.value
+
+
+class BlendFeatures:
+    """The blending family's per-variable features built on the device
+    (nir_blend_features_*): the family's data is copied once, and each
+    instance uploads only its factors (f, g)."""
+
+    def __init__(self, data: dict, device: int = 0):
+        self._keep = []
+
+        def arr(a, dt):
+            a = np.ascontiguousarray(a, dt)
+            self._keep.append(a)
+            return a.ctypes.data_as(C.POINTER(np.ctypeslib.as_ctypes_type(dt)))
+
+        d = BlendFeatureData()
+        d.n, d.m, d.nd, d.nf = data["n"], data["m"], data["nd"], data["nf"]
+        d.col_template = arr(data["col_template"], np.float32)
+        d.row_template = arr(data["row_template"], np.float32)
+        for k in ("cost0", "atybar", "dem_w", "dem_val", "rowlo0", "rowup", "axbar", "bscale", "row_abs", "abs_val"):
+            setattr(d, k, arr(data[k], np.float64))
+        d.cscale = float(data["cscale"])
+        d.dem_rp = arr(data["dem_rp"], np.int64)
+        d.abs_rp = arr(data["abs_rp"], np.int64)
+        d.dem_ci = arr(data["dem_ci"], np.int32)
+        d.abs_ci = arr(data["abs_ci"], np.int32)
+        h = C.c_void_p()
+        rc = lib().nir_blend_features_create(C.byref(d), device, C.byref(h))
+        self._keep = []  # the library has copied everything
+        if rc != 0:
+            raise RuntimeError(f"nir_blend_features_create failed ({rc}): {lib().nir_mlp_last_error().decode()}")
+        self._h = h
+        self.n, self.m, self.nf = d.n, d.m, d.nf
+
+    def build(self, f, g):
+        """Device addresses (col, row) of instance (f, g)'s features, valid
+        until the next build."""
+        f = np.ascontiguousarray(f, np.float64)
+        g = np.ascontiguousarray(g, np.float64)
+        col, row = C.c_void_p(), C.c_void_p()
+        rc = lib().nir_blend_features_build(self._h, f.ctypes.data_as(C.POINTER(C.c_double)),
+                                            g.ctypes.data_as(C.POINTER(C.c_double)), C.byref(col), C.byref(row))
+        if rc != 0:
+            raise RuntimeError(f"nir_blend_features_build failed ({rc}): {lib().nir_mlp_last_error().decode()}")
+        return col.value, row.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().nir_blend_features_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

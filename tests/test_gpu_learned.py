@@ -43,3 +43,35 @@ def test_warm_start_reaches_the_same_tolerance_in_fewer_iterations():
     # restarted PDLP's iteration count depends only logarithmically on the
     # starting distance: the gain is real but modest (about 8% measured)
     assert s["warm_iterations_mean"] <= 0.97 * s["cold_iterations_mean"], s
+
+
+def test_device_features_are_the_host_features():
+    # the warm start builds its network inputs on the device from the
+    # instance's factors alone; they are the host features up to the last
+    # bit of FP32 rounding, and so are the predictions made from them
+    fam = LW.BlendFamily(m=2000, n=5000, nnz=40000, family_seed=0)
+    p = pdhg.default_params(tol=1e-6, max_iters=200000, spmv_block_nnz=256)
+    with pdhg.Engine(fam.base) as eng:
+        train = LW.solve_family(fam, range(1000, 1064), p, engine=eng)
+    model = LW.WarmStart(fam, width=64, depth=2, seed=0, lr=1e-3)
+    model.fit(train, epochs=2, batch=8192)
+    try:
+        dev = model.device_features()
+        assert dev is not None
+        for seed in (5000, 5001):
+            f, g = fam.factors(seed)
+            col, row = dev.build(f, g)
+            hc, hr = model.col_features(f, g).copy(), model.row_features(f, g).copy()
+            xc_dev = model.col_net.predict_device(col, fam.n)
+            yr_dev = model.row_net.predict_device(row, fam.m)
+            xc_host = model.col_net.predict(hc)
+            yr_host = model.row_net.predict(hr)
+            np.testing.assert_allclose(xc_dev, xc_host, rtol=1e-2, atol=1e-3)
+            np.testing.assert_allclose(yr_dev, yr_host, rtol=1e-2, atol=1e-3)
+            x_d, y_d, w_d = model.predict(f, g)
+            x_h, y_h, w_h = model.predict(f, g, on_device=False)
+            assert w_d == w_h
+            np.testing.assert_allclose(x_d, x_h, rtol=1e-2, atol=1e-3 * np.abs(x_h).max())
+            np.testing.assert_allclose(y_d, y_h, rtol=1e-2, atol=1e-3 * np.abs(y_h).max())
+    finally:
+        model.close()

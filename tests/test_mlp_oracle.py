@@ -49,9 +49,29 @@ def test_mlp_library_exports_every_declared_symbol():
     header = open(os.path.join(ROOT, "include", "nir_mlp.h")).read()
     declared = set(re.findall(r"\b(nir_mlp_\w+)\s*\(", header))
     assert declared == set(mlp.EXPORTED)
+    blend = set(re.findall(r"\b(nir_blend_features_\w+)\s*\(", header))
+    assert blend == set(mlp.BLEND_EXPORTED)
     lib = C.CDLL(mlp.LIB_PATH)
-    for name in declared:
+    for name in declared | blend:
         assert hasattr(lib, name), name
+
+
+def test_blend_feature_data_layout_matches_the_c_compiler(tmp_path):
+    import subprocess
+
+    from nirnaya_b200 import mlp
+
+    src = tmp_path / "b.c"
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "nir_mlp.h"', 'int main(void){',
+             'printf("%zu\\n", sizeof(nir_blend_feature_data));']
+    lines += [f'printf("%zu\\n", offsetof(nir_blend_feature_data, {f}));' for f, _ in mlp.BlendFeatureData._fields_]
+    lines += ["return 0;}"]
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "b"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    vals = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()]
+    assert vals[0] == C.sizeof(mlp.BlendFeatureData)
+    assert vals[1:] == [getattr(mlp.BlendFeatureData, f).offset for f, _ in mlp.BlendFeatureData._fields_]
 
 
 def test_mlp_config_layout_matches_the_c_compiler(tmp_path):
