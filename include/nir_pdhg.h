@@ -89,7 +89,7 @@ typedef struct nir_pdhg_params {
     double primal_weight_smoothing; /* theta of the log-space weight update      (0.5)   */
     double step_factor;           /* eta = step_factor / ||A||_2 estimate        (0.998) */
     int32_t power_iters;          /* power-iteration rounds for ||A||_2          (64)    */
-    int32_t polish_stall_checks;  /* MIXED: FP64 polish once KKT <= 100 tol has not
+    int32_t polish_stall_checks;  /* MIXED: FP64 polish once KKT <= 30 tol has not
                                      improved 0.8x for this many checks and half
                                      of the checks so far                         (40)   */
     double polish_switch_kkt;     /* MIXED: ... or as soon as KKT <= this        (0)     */

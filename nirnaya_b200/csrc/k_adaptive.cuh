@@ -587,15 +587,20 @@ __device__ void control_update(const CtlArgs& a, DevState* st, const CtlSums& su
         } else {
             st->stall += 1;
         }
-        // a plateau counts as a stall only once it has lasted polish_stall
-        // checks and half of the checks so far, and only within a factor
-        // 100 of the tolerance: PDLP's own plateaus grow with its restart
-        // lengths (an artificial restart at 0.36 of the iterations so far)
-        // and sit at any KKT level, while the rounding of the FP32 matrix
-        // values (2^-24 relative) shows only near the tolerance; a
-        // hand-over earlier only slows the solve down
-        const long long window = max((long long)a.polish_stall, (it / max(a.K, 1)) / 2);
-        if ((st->stall >= window && kkt <= 100.0 * a.tol) || kkt <= a.polish_switch) {
+        // a plateau counts as a stall once it has lasted polish_stall
+        // checks and half of the checks so far, within a factor 30 of the
+        // tolerance: PDLP's own plateaus grow with its restart lengths (an
+        // artificial restart at 0.36 of the iterations so far) and sit at
+        // any KKT level, while the rounding of the FP32 matrix values
+        // (2^-24 relative) shows only near the tolerance.  A hand-over
+        // inside an ordinary plateau only slows the solve down: on the
+        // power-law LP the FP32-value phase converges by itself in the same
+        // iterations, and a rule that also handed over after a plateau of
+        // three quarters of the run at any level fired there at 19,000 of
+        // 155,000 iterations.
+        const long long checks = it / max(a.K, 1);
+        const bool near = st->stall >= max((long long)a.polish_stall, checks / 2) && kkt <= 30.0 * a.tol;
+        if (near || kkt <= a.polish_switch) {
             st->switch_request = 1;
             st->phase = 1;
             return;
