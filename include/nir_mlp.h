@@ -79,6 +79,22 @@ int nir_mlp_predict(nir_mlp* h, const float* x, int32_t n, float* y);
  * finished, e.g. nir_blend_features_build); y on the host. */
 int nir_mlp_predict_device(nir_mlp* h, const float* x_dev, int32_t n, float* y);
 
+/* The output map of nir_mlp_predict_device_affine, for n samples:
+ *   out[i] = shift[i] + scale[i] * min(max(pred[i][col], lo), hi)   (FP64)
+ * scale and shift are host arrays of n doubles, copied to the device here
+ * (NULL scale = 1, NULL shift = 0).  It turns a network's standardised
+ * output into a starting point (a box-scaled x, or a de-standardised y)
+ * without a trip through the host. */
+int nir_mlp_set_affine(nir_mlp* h, int32_t n, int32_t col, double lo, double hi, const double* scale,
+                       const double* shift);
+
+/* The forward pass of nir_mlp_predict_device followed by the output map
+ * set by nir_mlp_set_affine (for the same n): *out_dev receives the device
+ * address of the n FP64 results, owned by the handle, valid until its next
+ * call and complete when this returns (nir_pdhg_params.x_init / y_init
+ * take it as is). */
+int nir_mlp_predict_device_affine(nir_mlp* h, const float* x_dev, int32_t n, const double** out_dev);
+
 /* Loss and gradients of one minibatch (n a multiple of 8, at most 4096)
  * without updating the weights: grads in the flat parameter layout. */
 int nir_mlp_gradients(nir_mlp* h, const float* x, const float* targets, int32_t n, float* loss, float* grads);

@@ -106,7 +106,12 @@ typedef struct nir_pdhg_params {
                                      FP64 solve from the last FP32 point with the initial
                                      weight, 0 = as 1 but keeping the weight     (2)    */
     const double* x_init;         /* warm start in original space, ncol, or NULL          */
-    const double* y_init;         /* warm start duals, nrow, or NULL                      */
+    const double* y_init;         /* warm start duals, nrow, or NULL.  Either may be host
+                                     memory or device memory (unified addressing): a
+                                     device-resident start is copied on the device, with
+                                     no trip through the host except where the engine
+                                     remaps it (its row order, parallel columns); it must
+                                     be complete before the call                          */
     double omega_init;            /* warm-start primal weight; <= 0 = default             */
     double primal_weight_decades; /* the weight stays within this many decades of
                                      its initial value                           (1.0)   */

@@ -464,6 +464,26 @@ nir_lp_view reorder_rows(const nir_lp_view* lp, const std::vector<int>& row_orig
     return v;
 }
 
+// True when p is device (or managed) memory, as a starting point given by
+// its device address is; false for host memory, pinned or pageable.
+bool device_resident(const void* p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// A starting vector that the host must read (to remap it): a device-resident
+// one is copied into buf first.
+const double* host_readable(const double* p, size_t len, std::vector<double>& buf) {
+    if (!p || !device_resident(p)) return p;
+    buf.resize(len);
+    NIR_CUDA(cudaMemcpy(buf.data(), p, len * sizeof(double), cudaMemcpyDefault));
+    return buf.data();
+}
+
 // A row-indexed vector of the caller's into the engine's order, and back.
 void rows_in(const nir_pdhg* h, const double* src, std::vector<double>& dst) {
     dst.resize(size_t(h->m));
@@ -1634,12 +1654,13 @@ int solve_fast(nir_pdhg* h, const nir_pdhg_params& p, int (*poll)(void*), void* 
     // starting point
     double* d_xin = nullptr;
     double* d_yin = nullptr;
+    // host or device memory (a device-resident start is copied on the device)
     if (p.x_init) {
-        NIR_CUDA(cudaMemcpyAsync(h->out_x, p.x_init, n * sizeof(double), cudaMemcpyHostToDevice, s));
+        NIR_CUDA(cudaMemcpyAsync(h->out_x, p.x_init, n * sizeof(double), cudaMemcpyDefault, s));
         d_xin = h->out_x;
     }
     if (p.y_init) {
-        NIR_CUDA(cudaMemcpyAsync(h->out_y, p.y_init, m * sizeof(double), cudaMemcpyHostToDevice, s));
+        NIR_CUDA(cudaMemcpyAsync(h->out_y, p.y_init, m * sizeof(double), cudaMemcpyDefault, s));
         d_yin = h->out_y;
     }
     if (!pdlp && !p.x_init) {
@@ -1911,7 +1932,10 @@ int nir_pdhg_solve(nir_pdhg* h, const nir_pdhg_params* p_in, int (*poll)(void*),
         h->last_x = nullptr;  // out_x and x64 serve as scratch until the solve's end
         // the caller's row order <-> the engine's (row_order)
         const bool mapped = !h->row_orig.empty();
-        std::vector<double> yin, yres;
+        std::vector<double> yin, yres, xdev, ydev;
+        // the row order and the parallel columns remap a start on the host
+        if (h->inner) p.x_init = host_readable(p.x_init, size_t(h->n), xdev);
+        if (mapped || h->inner) p.y_init = host_readable(p.y_init, size_t(h->m), ydev);
         if (mapped && p.y_init) {
             rows_in(h, p.y_init, yin);
             p.y_init = yin.data();

@@ -251,6 +251,23 @@ __global__ void k_to_bf16(size_t n, const float* __restrict__ a, bf16* __restric
         b[i] = __float2bfloat16_rn(a[i]);
 }
 
+// out[i] = shift[i] + scale[i] * clamp(pred[i * ld + col], lo, hi), FP64
+// (r0 = the first sample of this chunk; pred holds the chunk's rows).  The
+// product and the sum are rounded separately (no fused multiply-add), the
+// clamp passes a NaN through, and a missing scale or shift is no operation,
+// so the result is the host's numpy expression bit for bit.
+__global__ void k_affine_out(int rows, int r0, const float* __restrict__ pred, int ld, int col, double lo, double hi,
+                             const double* __restrict__ scale, const double* __restrict__ shift,
+                             double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= rows) return;
+    const int g = r0 + i;
+    double p = double(pred[(size_t)i * ld + col]);
+    p = (p < lo) ? lo : ((p > hi) ? hi : p);
+    const double v = scale ? __dmul_rn(scale[g], p) : p;
+    out[g] = shift ? __dadd_rn(shift[g], v) : v;
+}
+
 template <typename T>
 __global__ void k_gather_rows(const int* __restrict__ idx, int rows, int cols, const T* __restrict__ src,
                               T* __restrict__ dst) {
@@ -397,6 +414,10 @@ struct nir_mlp {
     double us_per_step = 0.0, flops_per_step = 0.0;
     float* stage = nullptr;  // FP32 staging of uploaded rows, grown on demand
     size_t stage_len = 0;
+    // output map of nir_mlp_predict_device_affine
+    int aff_n = 0, aff_col = 0;
+    double aff_lo = 0.0, aff_hi = 0.0;
+    double *aff_scale = nullptr, *aff_shift = nullptr, *aff_out = nullptr;
     std::vector<void*> allocs;
 
     template <typename T>
@@ -873,6 +894,69 @@ int nir_mlp_predict_device(nir_mlp* h, const float* x_dev, int32_t n, float* y) 
                                      cudaMemcpyDeviceToHost, h->stream));
             MLP_CUDA(cudaStreamSynchronize(h->stream));
         }
+    } catch (const std::exception& e) {
+        return fail(e, false);
+    }
+    return 0;
+}
+
+int nir_mlp_set_affine(nir_mlp* h, int32_t n, int32_t col, double lo, double hi, const double* scale,
+                       const double* shift) {
+    if (!h || n < 8 || n % 8 != 0 || col < 0 || col >= h->cfg.d_out || !(lo <= hi)) {
+        g_err = "invalid arguments (n a positive multiple of 8, 0 <= col < d_out, lo <= hi)";
+        return 2;
+    }
+    try {
+        MLP_CUDA(cudaSetDevice(h->device));
+        for (double** q : {&h->aff_scale, &h->aff_shift, &h->aff_out}) {
+            if (*q) h->release(*q);
+            *q = nullptr;
+        }
+        h->aff_out = h->alloc<double>(size_t(n));
+        if (scale) {
+            h->aff_scale = h->alloc<double>(size_t(n));
+            MLP_CUDA(cudaMemcpyAsync(h->aff_scale, scale, size_t(n) * sizeof(double), cudaMemcpyHostToDevice,
+                                     h->stream));
+        }
+        if (shift) {
+            h->aff_shift = h->alloc<double>(size_t(n));
+            MLP_CUDA(cudaMemcpyAsync(h->aff_shift, shift, size_t(n) * sizeof(double), cudaMemcpyHostToDevice,
+                                     h->stream));
+        }
+        MLP_CUDA(cudaStreamSynchronize(h->stream));
+        h->aff_n = n;
+        h->aff_col = col;
+        h->aff_lo = lo;
+        h->aff_hi = hi;
+    } catch (const std::exception& e) {
+        h->aff_n = 0;
+        return fail(e, false);
+    }
+    return 0;
+}
+
+int nir_mlp_predict_device_affine(nir_mlp* h, const float* x_dev, int32_t n, const double** out_dev) {
+    if (!h || !x_dev || !out_dev || n < 8 || n % 8 != 0 || n != h->aff_n) {
+        g_err = "invalid arguments (n must be the n of nir_mlp_set_affine)";
+        return 2;
+    }
+    try {
+        MLP_CUDA(cudaSetDevice(h->device));
+        const int chunk = std::min(n, 65536);
+        ensure_rows(h, chunk);
+        for (int r = 0; r < n; r += chunk) {
+            const int k = std::min(chunk, n - r);
+            const size_t len = (size_t)k * h->cfg.d_in;
+            k_to_bf16<<<grid1d(len), 256, 0, h->stream>>>(len, x_dev + (size_t)r * h->cfg.d_in, h->x);
+            MLP_LAUNCHED();
+            forward(h, k);
+            k_affine_out<<<unsigned((k + 255) / 256), 256, 0, h->stream>>>(k, r, h->pred, h->cfg.d_out, h->aff_col,
+                                                                          h->aff_lo, h->aff_hi, h->aff_scale,
+                                                                          h->aff_shift, h->aff_out);
+            MLP_LAUNCHED();
+        }
+        MLP_CUDA(cudaStreamSynchronize(h->stream));
+        *out_dev = h->aff_out;
     } catch (const std::exception& e) {
         return fail(e, false);
     }

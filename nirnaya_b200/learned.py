@@ -158,12 +158,14 @@ class WarmStart:
         self._abs_a = sp.csr_matrix((np.abs(b.value), (b.row_index, self.cols)), shape=(fam.m, fam.n))
         self.device = device
         self._dev = None  # the features on the device (MLP.BlendFeatures), built after a fit
+        self._affine = False  # the networks' output maps for device_out are set
         self.fitted = False
 
     # ---- statistics of the training solutions
     def _stats(self, sol: Solutions):
         fam = self.fam
         self._colF = self._rowF = None
+        self._affine = False
         if self._dev is not None:
             self._dev.close()
             self._dev = None
@@ -284,11 +286,28 @@ class WarmStart:
                 abs_rp=aa.indptr.astype(np.int64), abs_ci=aa.indices, abs_val=aa.data), self.device)
         return self._dev
 
-    def predict(self, f, g, on_device: bool = True):
+    def predict(self, f, g, on_device: bool = True, device_out: bool = False):
         """x0, y0, omega for one instance: the features built on the device
         (or, with on_device False or sizes the device path does not take,
-        on the host), then one pass of each network."""
-        dev = self.device_features() if on_device else None
+        on the host), then one pass of each network.
+
+        With device_out, x0 and y0 are the device addresses (int) of FP64
+        vectors owned by the networks, valid until their next prediction,
+        which Engine.solve takes as its start with no trip through the host;
+        their values are those of the host form bit for bit."""
+        dev = self.device_features() if (on_device or device_out) else None
+        if device_out:
+            if dev is None:
+                raise ValueError("device_out needs the device features (n and m multiples of 8)")
+            if not self._affine:
+                # x0 = u * clip(p, 0, 1); y0 = ybar + ysd * p
+                self.col_net.set_affine(self.fam.n, 0, 0.0, 1.0, scale=self.u)
+                self.row_net.set_affine(self.fam.m, 0, scale=self.ysd, shift=self.ybar)
+                self._affine = True
+            col, row = dev.build(f, g)
+            x0 = self.col_net.predict_device_affine(col, self.fam.n)
+            y0 = self.row_net.predict_device_affine(row, self.fam.m)
+            return x0, y0, float(np.exp(self.log_omega))
         if dev is not None:
             col, row = dev.build(f, g)
             xc = self.col_net.predict_device(col, self.fam.n)[:, 0].astype(np.float64)
@@ -350,16 +369,18 @@ def evaluate(fam: BlendFamily, model: WarmStart, seeds, params: P.Params | None 
     N = len(seeds)
     ev = Evaluation(np.zeros(N, np.int64), np.zeros(N, np.int64), np.zeros(N), np.zeros(N), 0.0,
                     np.zeros(N, bool), np.zeros(N), np.zeros(N))
+    # the start stays on the device from features to solve where it can
+    dev_out = model.device_features() is not None
     if N:
         # one untimed prediction: the networks' first call sizes their
         # device buffers, a one-off cost of the handle, not of an instance
-        model.predict(*fam.factors(seeds[0]))
+        model.predict(*fam.factors(seeds[0]), device_out=dev_out)
     try:
         for i, s in enumerate(seeds):
             f, g = fam.factors(s)
             rowlo, cost = fam.vectors(f, g)
             t0 = time.perf_counter()
-            x0, y0, w0 = model.predict(f, g)
+            x0, y0, w0 = model.predict(f, g, device_out=dev_out)
             ev.predict_seconds += time.perf_counter() - t0
             eng.update_vectors(cost=cost, rowlo=rowlo)
             t0 = time.perf_counter()

@@ -14,6 +14,7 @@ EXPORTED = [
     "nir_mlp_create", "nir_mlp_free", "nir_mlp_last_error", "nir_mlp_param_count", "nir_mlp_get_params",
     "nir_mlp_set_params", "nir_mlp_set_output_weights", "nir_mlp_set_data", "nir_mlp_train", "nir_mlp_predict",
     "nir_mlp_gradients", "nir_mlp_gemm_check", "nir_mlp_gemm_time", "nir_mlp_step_stats", "nir_mlp_predict_device",
+    "nir_mlp_set_affine", "nir_mlp_predict_device_affine",
 ]
 BLEND_EXPORTED = ["nir_blend_features_create", "nir_blend_features_build", "nir_blend_features_free"]
 
@@ -65,6 +66,9 @@ def lib():
         L.nir_mlp_step_stats.argtypes = [VP, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.nir_mlp_gemm_time.argtypes = [VP, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_double)]
         L.nir_mlp_predict_device.argtypes = [VP, VP, C.c_int32, F]
+        D = C.POINTER(C.c_double)
+        L.nir_mlp_set_affine.argtypes = [VP, C.c_int32, C.c_int32, C.c_double, C.c_double, D, D]
+        L.nir_mlp_predict_device_affine.argtypes = [VP, VP, C.c_int32, C.POINTER(VP)]
         L.nir_blend_features_create.argtypes = [C.POINTER(BlendFeatureData), C.c_int32, C.POINTER(VP)]
         L.nir_blend_features_build.argtypes = [VP, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(VP),
                                                C.POINTER(VP)]
@@ -156,6 +160,23 @@ class Mlp:
         Y = np.zeros((n, self.dims[-1]), np.float32)
         self._check(lib().nir_mlp_predict_device(self._h, C.c_void_p(x_dev), n, _f(Y)), "predict_device")
         return Y
+
+    def set_affine(self, n: int, col: int = 0, lo: float = -np.inf, hi: float = np.inf, scale=None, shift=None):
+        """The map of predict_device_affine: shift + scale * clamp(pred[:, col], lo, hi)."""
+        keep = [None if v is None else np.ascontiguousarray(v, np.float64) for v in (scale, shift)]
+        for v in keep:
+            assert v is None or v.shape == (n,)
+        ptr = [None if v is None else v.ctypes.data_as(C.POINTER(C.c_double)) for v in keep]
+        self._check(lib().nir_mlp_set_affine(self._h, int(n), int(col), float(lo), float(hi), ptr[0], ptr[1]),
+                    "set_affine")
+
+    def predict_device_affine(self, x_dev: int, n: int) -> int:
+        """Forward pass of n FP32 samples on the device and the set_affine map:
+        the device address of n FP64 results, valid until the next call."""
+        out = C.c_void_p()
+        self._check(lib().nir_mlp_predict_device_affine(self._h, C.c_void_p(x_dev), int(n), C.byref(out)),
+                    "predict_device_affine")
+        return int(out.value)
 
     def gradients(self, X, T):
         X, T = _c32(X), _c32(T)

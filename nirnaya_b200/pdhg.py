@@ -162,6 +162,16 @@ def _dptr(a):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
+def _start_ptr(v, keep):
+    """A starting vector for nir_pdhg_solve: a device address (int) as is,
+    else a contiguous FP64 host copy kept alive in keep."""
+    if isinstance(v, (int, np.integer)) and not isinstance(v, bool):
+        return C.cast(C.c_void_p(int(v)), C.POINTER(C.c_double))
+    a = np.ascontiguousarray(v, np.float64)
+    keep.append(a)
+    return _dptr(a)
+
+
 class Engine:
     """One LP resident on one GPU (nir_pdhg_create ... nir_pdhg_free)."""
 
@@ -201,17 +211,15 @@ class Engine:
         self.lp._view = None
 
     def solve(self, params: Params | None = None, poll=None, x_init=None, y_init=None, omega_init=None):
+        """x_init / y_init: host arrays, or device addresses (int) of FP64
+        vectors on this handle's device, complete before the call."""
         # a copy: the warm-start pointers must not outlive this call in the caller's params
         p = Params.from_buffer_copy(params) if params is not None else default_params()
         keep = []
         if x_init is not None:
-            xa = np.ascontiguousarray(x_init, np.float64)
-            keep.append(xa)
-            p.x_init = _dptr(xa)
+            p.x_init = _start_ptr(x_init, keep)
         if y_init is not None:
-            ya = np.ascontiguousarray(y_init, np.float64)
-            keep.append(ya)
-            p.y_init = _dptr(ya)
+            p.y_init = _start_ptr(y_init, keep)
         if omega_init is not None:
             p.omega_init = float(omega_init)
         x = np.zeros(self.lp.ncol)
