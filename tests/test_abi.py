@@ -134,3 +134,24 @@ def test_verify_entry_points_reject_bad_arguments_before_any_device_call():
     assert pdhg.last_error() == "null handle"
     assert lib.nir_pdhg_batch_verify(None, None, None, None, 1e-6, None) == pdhg.INPUT_ERROR
     assert pdhg.last_error() == "null report"
+
+
+def test_a_start_is_a_device_address_as_is_or_a_kept_host_copy():
+    # Engine.solve hands x_init / y_init to nir_pdhg_solve: an int is a device
+    # address passed through unchanged; anything else becomes a contiguous
+    # FP64 host copy that lives as long as the call's keep list
+    import numpy as np
+
+    from nirnaya_b200 import pdhg
+
+    keep = []
+    p = pdhg._start_ptr(0x7F0012345600, keep)
+    assert C.cast(p, C.c_void_p).value == 0x7F0012345600 and keep == []
+    p = pdhg._start_ptr(np.int64(4096), keep)
+    assert C.cast(p, C.c_void_p).value == 4096 and keep == []
+    p = pdhg._start_ptr([1, 2, 3], keep)
+    assert len(keep) == 1 and keep[0].dtype == np.float64 and keep[0].flags.c_contiguous
+    assert [p[i] for i in range(3)] == [1.0, 2.0, 3.0]
+    strided = np.arange(10.0)[::2]
+    p = pdhg._start_ptr(strided, keep)
+    assert len(keep) == 2 and [p[i] for i in range(5)] == [0.0, 2.0, 4.0, 6.0, 8.0]
