@@ -23,6 +23,12 @@ about 12 minutes):
 
     python tests/golden/make_optima.py [name ...]
 
+With --confirm, each named entry is solved again by HiGHS's dual simplex
+(method "highs-ds"), a second algorithm, and the entry records that
+objective beside the first; the two must agree to 1e-9 relative:
+
+    python tests/golden/make_optima.py --confirm c5_badly_scaled_5000x12000
+
 Objectives are stored as hex strings (exact) and as decimals (readable).
 Several runs may fill the file at once: each merges its entry into it.
 """
@@ -64,8 +70,9 @@ def instances():
     return d
 
 
-def highs_optimum(lp):
-    """Optimal objective (with the LP's offset) by HiGHS IPM + crossover."""
+def highs_optimum(lp, method="highs-ipm"):
+    """Optimal objective (with the LP's offset) by HiGHS: IPM + crossover,
+    or the dual simplex with method "highs-ds"."""
     import scipy
     import scipy.sparse as sp
     from scipy.optimize import linprog
@@ -81,10 +88,10 @@ def highs_optimum(lp):
     t0 = time.time()
     r = linprog(lp.cost, A_ub=A_ub if A_ub.shape[0] else None, b_ub=b_ub if A_ub.shape[0] else None,
                 A_eq=A[eq] if eq.any() else None, b_eq=rl[eq] if eq.any() else None, bounds=bounds,
-                method="highs-ipm", options={"presolve": True})
+                method=method, options={"presolve": True})
     if r.status != 0:
         raise RuntimeError(f"HiGHS did not solve the LP: {r.message}")
-    return float(r.fun) + float(lp.obj_offset), time.time() - t0, f"scipy {scipy.__version__} linprog highs-ipm"
+    return float(r.fun) + float(lp.obj_offset), time.time() - t0, f"scipy {scipy.__version__} linprog {method}"
 
 
 def main():
@@ -92,11 +99,28 @@ def main():
     from nirnaya_b200 import lp as L
 
     build.build_lpgen()
-    want = set(sys.argv[1:])
+    args = sys.argv[1:]
+    confirm = "--confirm" in args
+    want = set(a for a in args if a != "--confirm")
     for name, (kind, seed, kw) in instances().items():
         if want and name not in want:
             continue
         lp = L.generate(kind, seed, **kw)
+        if confirm:
+            out = json.load(open(OUT))
+            e = out[name]
+            obj, secs, how = highs_optimum(lp, "highs-ds")
+            ref = float.fromhex(e["objective_hex"])
+            rel = abs(obj - ref) / (1.0 + abs(ref))
+            if rel > 1e-9:
+                raise RuntimeError(f"{name}: the dual simplex gives {obj!r}, the fixture {ref!r} (rel {rel:.2e})")
+            out = json.load(open(OUT))  # merged: several runs may fill it
+            out[name]["confirmed"] = {"solver": how, "objective_hex": obj.hex(), "rel_diff": rel,
+                                      "solver_seconds": round(secs, 1)}
+            print(name, "confirmed", obj, f"rel {rel:.1e}", f"{secs:.1f}s", flush=True)
+            with open(OUT, "w") as f:
+                json.dump(out, f, indent=1, sort_keys=True)
+            continue
         obj, secs, how = highs_optimum(lp)
         out = json.load(open(OUT)) if os.path.exists(OUT) else {}  # merged: several runs may fill it
         out[name] = {"kind": kind, "seed": seed, "kw": kw, "nrow": lp.nrow, "ncol": lp.ncol, "nnz": int(lp.nnz),
