@@ -1,7 +1,7 @@
 // The CLI's program entry for the drop-in build of `sovsolve`.
 //
 // The reference's README advertises `--method=auto|simplex|ipm|pdhg`
-// (README.md:27), but its argument loop only takes the two-token form
+// (its README.md:27), but its argument loop only takes the two-token form
 // `--method pdhg` (src/driver/cli_main.cpp:51-52) and silently skips any
 // other dash argument (:77), so `--method=pdhg` ran the dual simplex.
 // This entry splits every `--<option>=<value>` of an option that takes a

@@ -272,7 +272,7 @@ def test_dropin_cli_cpu_methods_match_the_reference_cli(tmp_path, model, method)
 
 @pytest.mark.parametrize("method", ["dual", "ipm"])
 def test_dropin_cli_accepts_the_method_equals_form(tmp_path, method):
-    """`--method=<m>` (README.md:27) selects the method as `--method <m>`
+    """`--method=<m>` (the reference's README.md:27) selects the method as `--method <m>`
     does; the reference's own loop drops that form (cli_main.cpp:77)."""
     model = os.path.join(REFINERY, "MRPL_Crude_Blending_LP.mps")
     if not os.path.exists(model):

@@ -38,7 +38,7 @@ def test_warm_start_reaches_the_same_tolerance_in_fewer_iterations():
     s = ev.summary()
     assert s["accepted"] == s["instances"], s
     assert info.status == pdhg.OPTIMAL and ffi.rel_kkt(lp, x, y).rel_kkt <= 1.05e-6
-    # warm and cold objectives agree to the north-star's 1e-6 relative
+    # warm and cold objectives agree to 1e-6 relative, the required objective tolerance
     assert s["max_rel_objective_gap"] <= 1e-6, s
     # restarted PDLP's iteration count depends only logarithmically on the
     # starting distance: the gain is real but modest (about 8% measured)

@@ -168,7 +168,7 @@ def test_pdlp_reaches_tolerance(name, make, prec):
     # the objective is the dd_real evaluation of c'x, and it is near the optimum
     assert info.objective == ffi.eval_objective(lp, x)
     opt = _optimum(lp)
-    # the relative objective error of src/io/sol_io.hpp:96-102, at the north-star 1e-6
+    # the relative objective error of src/io/sol_io.hpp:96-102, within the required 1e-6
     assert abs(info.objective - opt) / (1 + abs(opt)) <= 1e-6, (info.objective, opt)
     if prec == pdhg.PREC_FP64:
         assert info.iterations_fp64 == info.iterations
