@@ -669,7 +669,7 @@ struct LaunchCfg {
 // Shared-memory carveout preference of the SpMV kernels, in percent of the
 // maximum, set before their occupancy query: 28 % (64 KB) holds the 2-4
 // resident CTAs' shared memory and leaves the rest of the 256 KB to L1 for
-// the gathers (C2's A' y 2-3 % faster than the driver's 100 KB choice; 0 %,
+// the gathers (C2's A' y 2-3 % faster than the CUDA driver's 100 KB choice; 0 %,
 // "prefer L1", cut the resident CTAs and made the iteration 35 % slower).
 #ifndef NIR_SMEM_CARVEOUT
 #define NIR_SMEM_CARVEOUT 28
