@@ -1268,7 +1268,8 @@ def run_arm(args, wl, rank, world, local):
     wl = WORKLOADS[args.workload]
     dom_family = "cta" if (r["lay"].block_nnz_at if "primal" in dom_name else r["lay"].block_nnz) > 256 else "warp"
     traffic = committed_traffic(f"{dom_name}[{dom_family}]:{wl['label']}")
-    cpu = cpu_baseline(lp, wl["label"], seconds=args.cpu_seconds)
+    # the reference on the host cores: rank 0 at N=1 only
+    cpu = cpu_baseline(lp, wl["label"], seconds=args.cpu_seconds) if world == 1 else None
     fp64 = r["fp64"]
     if cpu and fp64 and fp64["iterations"]:
         # seconds per iteration: the reference on the host cores vs the FP64 GPU solve
